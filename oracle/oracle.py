@@ -1,0 +1,214 @@
+"""ctypes bindings of the CPU checkers (test infrastructure only).
+
+Imported by tests/, __graft_entry__.smoke() and bench.py's CPU baseline; the
+product never imports this module.
+
+    run_oracle(...)     double-precision restatement of tests/reference.py
+                        (tcoh_oracle.c), optionally with the reference
+                        kernel's float SHP statistics
+    run_reference(...)  the reference kernel tcoh.cl itself, compiled as C
+                        (oracle/_ref, built by oracle/Makefile from the
+                        reference checkout; present only where it was built)
+"""
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+TESTS = {"ks": 0, "ad": 1, "tlog": 2}
+
+
+def build(reference_dir=None):
+    """Compile liboracle.so, and oracle/_ref when the reference is present."""
+    cmd = ["make", "-s", "-C", HERE]
+    if reference_dir:
+        cmd.append("REF=" + reference_dir)
+    subprocess.run(cmd, check=True)
+
+
+class _Settings(ctypes.Structure):
+    _fields_ = [
+        ("ndates", ctypes.c_int),
+        ("win_az", ctypes.c_int),
+        ("win_rg", ctypes.c_int),
+        ("test", ctypes.c_int),
+        ("alpha", ctypes.c_double),
+        ("emi", ctypes.c_int),
+        ("bias", ctypes.c_int),
+        ("min_looks", ctypes.c_int),
+        ("npairs", ctypes.c_int),
+        ("pairs_all", ctypes.c_int),
+        ("shp_fp32", ctypes.c_int),
+    ]
+
+
+class _KernelConstants(ctypes.Structure):
+    _fields_ = [
+        ("ks_max", ctypes.c_int),
+        ("ad_norm", ctypes.c_float),
+        ("ad_sigma", ctypes.c_float),
+        ("ad_crit", ctypes.c_float),
+        ("tlog_crit", ctypes.c_float),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        _lib = ctypes.CDLL(path)
+        _lib.orc_strip.restype = ctypes.c_int
+        _lib.orc_ad_statistic.restype = ctypes.c_double
+        _lib.orc_ad_sigma_of.restype = ctypes.c_double
+        _lib.orc_ad_critical.restype = ctypes.c_double
+        _lib.orc_normal_quantile.restype = ctypes.c_double
+        _lib.orc_ad_critical.argtypes = [ctypes.c_double]
+        _lib.orc_normal_quantile.argtypes = [ctypes.c_double]
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def _settings(n, window, shp_test, alpha, estimator, bias, min_shp, npairs, pairs_all, shp_fp32):
+    return _Settings(
+        n, window[0], window[1], TESTS[shp_test], alpha, int(estimator == "emi"),
+        int(bias), max(int(min_shp), n), npairs, int(pairs_all), int(shp_fp32),
+    )
+
+
+def kernel_constants(n, shp_test="ks", alpha=0.05):
+    """The float constants that the reference kernel is built with."""
+    s = _settings(n, (21, 7), shp_test, alpha, "evd", False, n, 0, False, True)
+    k = _KernelConstants()
+    lib().orc_kernel_constants_for(ctypes.byref(s), ctypes.byref(k))
+    return k
+
+
+def run_oracle(slc, amp, valid, rows, cols, window=(21, 7), shp_test="ks", alpha=0.05,
+               min_shp=20, estimator="evd", bias=False, npairs=0, pairs_all=False,
+               shp_fp32=False, want_phases=False, want_mask=False, threads=0):
+    """Oracle over a padded strip (layouts of ocl_run). Returns a dict with
+    coh (float64), count (int32), and pairs / phases / mask when asked."""
+    slc = np.ascontiguousarray(slc, np.float32)
+    amp = np.ascontiguousarray(amp, np.float32)
+    valid = np.ascontiguousarray(valid, np.uint8)
+    prow, pcol, n = amp.shape
+    s = _settings(n, window, shp_test, alpha, estimator, bias, min_shp, npairs, pairs_all, shp_fp32)
+    coh = np.empty((rows, cols), np.float64)
+    count = np.empty((rows, cols), np.int32)
+    pairs = np.empty((npairs, rows, cols), np.float64) if npairs else None
+    phases = np.empty((rows, cols, n), np.float64) if want_phases else None
+    words = (window[0] * window[1] + 31) // 32
+    mask = np.empty((rows, cols, words), np.uint32) if want_mask else None
+    rc = lib().orc_strip(
+        ctypes.byref(s), _ptr(slc), _ptr(amp), _ptr(valid), prow, pcol, rows, cols,
+        _ptr(coh), _ptr(count), _ptr(pairs), _ptr(phases), _ptr(mask), int(threads),
+    )
+    if rc != 0:
+        raise ValueError("oracle rejected the strip shape or settings")
+    out = {"coh": coh, "count": count}
+    if npairs:
+        out["pairs"] = pairs
+    if want_phases:
+        out["phases"] = phases
+    if want_mask:
+        out["mask"] = mask
+    return out
+
+
+def ad_statistic(a, b):
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    return lib().orc_ad_statistic(_ptr(a), _ptr(b), len(a))
+
+
+def ks_accept(a, b, alpha):
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    return bool(lib().orc_ks_accept(_ptr(a), _ptr(b), len(a), ctypes.c_double(alpha)))
+
+
+def ad_sigma(n):
+    return lib().orc_ad_sigma_of(n)
+
+
+def ad_critical(alpha):
+    return lib().orc_ad_critical(alpha)
+
+
+def hermitian_eigen(m):
+    """Eigenvalues and eigenvectors of a Hermitian matrix by the oracle's
+    double-precision Jacobi solver (unsorted)."""
+    m = np.asarray(m, np.complex128)
+    n = m.shape[0]
+    ar = np.ascontiguousarray(m.real)
+    ai = np.ascontiguousarray(m.imag)
+    vr = np.zeros((n, n))
+    vi = np.zeros((n, n))
+    lib().orc_hermitian_eigen(n, _ptr(ar), _ptr(ai), _ptr(vr), _ptr(vi))
+    return np.diag(ar).copy(), vr + 1j * vi
+
+
+# ---------------------------------------------------------------------------
+# The reference kernel compiled as C.
+
+_ref = {}
+
+
+def reference_available():
+    return os.path.exists(os.path.join(HERE, "_ref", "libtcoh_ref.so"))
+
+
+def _ref_lib(pairs):
+    name = "libtcoh_ref_pairs.so" if pairs else "libtcoh_ref.so"
+    if name not in _ref:
+        path = os.path.join(HERE, "_ref", name)
+        if not os.path.exists(path):
+            raise FileNotFoundError(path + " (build with: make -C oracle)")
+        lib_ = ctypes.CDLL(path)
+        lib_.ref_run.restype = ctypes.c_int
+        lib_.ref_run.argtypes = [ctypes.c_int] * 8 + [ctypes.c_float] * 4 + [ctypes.c_int] + [
+            ctypes.c_void_p] * 3 + [ctypes.c_int] * 4 + [ctypes.c_void_p] * 3 + [ctypes.c_int]
+        lib_.ref_threads.restype = ctypes.c_int
+        _ref[name] = lib_
+    return _ref[name]
+
+
+def reference_threads():
+    return _ref_lib(False).ref_threads()
+
+
+def run_reference(slc, amp, valid, rows, cols, window=(21, 7), shp_test="ks", alpha=0.05,
+                  min_shp=20, estimator="evd", bias=False, npairs=0, pairs_all=False,
+                  threads=0):
+    """The reference kernel (tcoh.cl compiled as C) over a padded strip."""
+    slc = np.ascontiguousarray(slc, np.float32)
+    amp = np.ascontiguousarray(amp, np.float32)
+    valid = np.ascontiguousarray(valid, np.uint8)
+    prow, pcol, n = amp.shape
+    k = kernel_constants(n, shp_test, alpha)
+    coh = np.empty((rows, cols), np.float32)
+    count = np.empty((rows, cols), np.int32)
+    pairs = np.empty((max(npairs, 1), rows, cols), np.float32)
+    rc = _ref_lib(npairs > 0).ref_run(
+        n, window[0], window[1], TESTS[shp_test], int(estimator == "emi"), int(bias),
+        max(int(min_shp), n), k.ks_max, k.ad_norm, k.ad_sigma, k.ad_crit, k.tlog_crit,
+        int(pairs_all), _ptr(slc), _ptr(amp), _ptr(valid), prow, pcol, rows, cols,
+        _ptr(coh), _ptr(count), _ptr(pairs), int(threads),
+    )
+    if rc != 0:
+        raise ValueError("reference runner rejected the strip shape")
+    out = {"coh": coh, "count": count}
+    if npairs:
+        out["pairs"] = pairs
+    return out
