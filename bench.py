@@ -1,0 +1,453 @@
+#!/usr/bin/env python
+"""Throughput of the phase-linking temporal coherence path on B200.
+
+Metric: Mpixel/s of temporal coherence at N = 30 dates, 21 x 7 window,
+within 1e-4 of the FP64 oracle. Workload (one step = one pass of the path
+over one strip): a 4096 x 4096 stack of 30 complex64 dates, 32 Voronoi
+regions with coherence up to 0.99, shp_test=ad, estimator=emi, -b (the
+precision-form configuration of the reference's published settings),
+seeded synthetic data.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+* value: device-resident strips, K steps timed with CUDA events on the
+  launching stream (inputs of 6 GB, far above the 126 MB L2: no flush);
+* e2e: the same metric through the C-ABI with host buffers (tc_run_ex, the
+  ocl_run path): page-locked strip in, outputs out, copies inside the
+  timed region;
+* roofline of the dominant kernel from per-launch CUDA events;
+* cpu_baseline: the reference kernel (tcoh.cl compiled as C, oracle/_ref)
+  on all host cores over a crop of the same workload;
+* accuracy: max / RMS |coh - oracle| on a crop (FP64 oracle, float SHP
+  decisions), and the SHP decision flips of the float tests against the
+  FP64 ones.
+
+With N > 1 (torchrun), every rank processes its own full workload (weak
+scaling, no collective on the data path); time is the max over ranks.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = dict(n=30, rows=4096, cols=4096, window=(21, 7), shp_test="ad", alpha=0.05,
+                min_shp=20, estimator="emi", bias=True, nregions=32, g0_max=0.99, spacing=12.0)
+METRIC = "Mpixel/s temporal coherence at N=30, 21x7 window, <=1e-4 vs FP64"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--rows", type=int, default=WORKLOAD["rows"])
+    p.add_argument("--cols", type=int, default=WORKLOAD["cols"])
+    p.add_argument("--gram", default="tensor", choices=["tensor", "fp32"],
+                   help="arithmetic of the coherence matrices (the tensor cores, else plain FP32)")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the e2e, plain-FP32, CPU and accuracy legs")
+    return p.parse_args()
+
+
+def workload_name(rows, cols):
+    w = WORKLOAD
+    return "N=%d %dx%d %s/%s%s window %dx%d, %d regions, coherence <= %.2f" % (
+        w["n"], rows, cols, w["shp_test"], w["estimator"], "/-b" if w["bias"] else "",
+        w["window"][0], w["window"][1], w["nregions"], w["g0_max"])
+
+
+# ---------------------------------------------------------------------------
+# Inputs.
+
+def device_strip(torch, stack, ha, hr):
+    """Padded strip buffers (main.c:52-127 layout) built on the device."""
+    n, rows, cols = stack.shape
+    re, im = stack.real.contiguous(), stack.imag.contiguous()
+    bad = torch.isnan(re) | torch.isnan(im) | ((re == 0) & (im == 0))
+    valid = ~bad.any(dim=0)
+    re = torch.where(valid[None], re, torch.zeros_like(re))
+    im = torch.where(valid[None], im, torch.zeros_like(im))
+    amp = torch.sqrt(re * re + im * im)
+    amp, _ = torch.sort(amp, dim=0)
+    P, Q = rows + 2 * ha, cols + 2 * hr
+    dev = stack.device
+    slc = torch.zeros((P, Q, n, 2), dtype=torch.float32, device=dev)
+    slc[ha:ha + rows, hr:hr + cols, :, 0] = re.permute(1, 2, 0)
+    slc[ha:ha + rows, hr:hr + cols, :, 1] = im.permute(1, 2, 0)
+    del re, im
+    a = torch.zeros((P, Q, n), dtype=torch.float32, device=dev)
+    a[ha:ha + rows, hr:hr + cols] = amp.permute(1, 2, 0)
+    del amp
+    v = torch.zeros((P, Q), dtype=torch.uint8, device=dev)
+    v[ha:ha + rows, hr:hr + cols] = valid.to(torch.uint8)
+    return slc, a, v
+
+
+# ---------------------------------------------------------------------------
+# Clocks during the timed region.
+
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.close()
+        rows = [r.split(", ") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        if not rows:
+            return None
+        import statistics
+
+        sm = [float(r[1]) for r in rows if len(r) > 1 and r[1].strip().replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if len(r) > 2 and r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].strip() == "Active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# Algorithmic work per pixel (fixed by formula; extra work of an
+# implementation does not count).
+
+def flops_per_pixel(n, looks, emi):
+    gram = 8.0 * looks * n * (n + 1) / 2
+    norm_gamma = 10.0 * n * (n - 1) / 2 + 20.0 * n * (n - 1) / 2
+    evd = 16.0 * n ** 3 / 3 + 8.0 * n ** 2 + 64 * 5 * n
+    link = norm_gamma + evd + ((n ** 3 + 2.0 * n ** 2) if emi else 0.0)
+    return gram, link
+
+
+def shp_ops_per_pixel(n, test, area):
+    if test == "ks":
+        return area * 2.0 * n
+    if test == "ad":
+        return area * (2.0 * n - 1) * 7
+    return area * 6.0 + n
+
+
+# ---------------------------------------------------------------------------
+# CPU legs.
+
+def cpu_crop(slc, amp, valid, rows, cols, r0, nrows, ncols, ha, hr):
+    """Sub-strip for output rows r0 .. r0+nrows-1, columns 0 .. ncols-1."""
+    import numpy as np
+
+    sl = slice(r0, r0 + nrows + 2 * ha)
+    cs = slice(0, ncols + 2 * hr)
+    return (np.ascontiguousarray(slc[sl, cs]), np.ascontiguousarray(amp[sl, cs]),
+            np.ascontiguousarray(valid[sl, cs]))
+
+
+def reference_rate(slc, amp, valid, rows, cols, kw, target_s=10.0, threads=0):
+    """Mpixel/s of the reference kernel (tcoh.cl as C) on the host cores,
+    on crops of the workload sized for about target_s seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    ha, hr = kw["window"][0] // 2, kw["window"][1] // 2
+    kind = "reference" if oracle.reference_available() else "port"
+    run = oracle.run_reference if kind == "reference" else oracle.run_oracle
+    ccols = min(cols, 512)
+    # calibration on 4 rows
+    crop = cpu_crop(slc, amp, valid, rows, cols, rows // 2, 4, ccols, ha, hr)
+    t = time.perf_counter()
+    run(*crop, 4, ccols, threads=threads, **kw)
+    rate = 4 * ccols / max(time.perf_counter() - t, 1e-6)
+    nrows = int(max(4, min(rows // 2, rate * target_s / ccols)))
+    crop = cpu_crop(slc, amp, valid, rows, cols, rows // 4, nrows, ccols, ha, hr)
+    t = time.perf_counter()
+    run(*crop, nrows, ccols, threads=threads, **kw)
+    dt = time.perf_counter() - t
+    cores = oracle.reference_threads() if kind == "reference" else (threads or os.cpu_count())
+    return {"value": nrows * ccols / dt / 1e6, "unit": "Mpixel/s", "cores": cores, "kind": kind,
+            "sample": "%d x %d output pixels of the workload (rows %d.., %.1f s)" % (
+                nrows, ccols, rows // 4, dt)}
+
+
+def accuracy(slc, amp, valid, coh_gpu, count_gpu, rows, cols, kw, size=48):
+    """|coh - FP64 oracle| on a centred crop (oracle with the float SHP
+    decisions, so that both use the same masks), plus SHP decision flips of
+    the float statistics against the FP64 ones."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    ha, hr = kw["window"][0] // 2, kw["window"][1] // 2
+    r0, c0 = rows // 2, cols // 2
+    sl = slice(r0, r0 + size + 2 * ha)
+    cs = slice(c0, c0 + size + 2 * hr)
+    crop = (np.ascontiguousarray(slc[sl, cs]), np.ascontiguousarray(amp[sl, cs]),
+            np.ascontiguousarray(valid[sl, cs]))
+    o32 = oracle.run_oracle(*crop, size, size, shp_fp32=True, **kw)
+    o64 = oracle.run_oracle(*crop, size, size, shp_fp32=False, **kw)
+    g = coh_gpu[r0:r0 + size, c0:c0 + size].astype(np.float64)
+    cnt = count_gpu[r0:r0 + size, c0:c0 + size]
+    m = ~np.isnan(o32["coh"]) & ~np.isnan(g)
+    err = np.abs(g[m] - o32["coh"][m])
+    return {
+        "pixels": int(size * size),
+        "max_abs": float(err.max()) if err.size else None,
+        "rms": float(np.sqrt(np.mean(err ** 2))) if err.size else None,
+        "count_mismatch": int((cnt != o32["count"]).sum()),
+        "null_mask_mismatch": int((np.isnan(g) != np.isnan(o32["coh"])).sum()),
+        "shp_count_flips_float_vs_fp64": int((o32["count"] != o64["count"]).sum()),
+    }
+
+
+# ---------------------------------------------------------------------------
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    w = dict(WORKLOAD)
+    rows, cols = args.rows, args.cols
+    ha, hr = w["window"][0] // 2, w["window"][1] // 2
+    kw = dict(window=w["window"], shp_test=w["shp_test"], alpha=w["alpha"], min_shp=w["min_shp"],
+              estimator=w["estimator"], bias=w["bias"])
+
+    import numpy as np
+    import torch
+
+    import tcoh_b200
+    import tcoh_b200.synthetic as syn
+
+    if args.impl == "reference" and world > 1 and rank != 0:
+        return
+    dist = None
+    if world > 1 and args.impl != "reference":
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    stack = syn.generate(w["n"], rows, cols, nregions=w["nregions"], g0_max=w["g0_max"],
+                         spacing=w["spacing"], seed=1 + rank, device=dev)
+    slc, amp, valid = device_strip(torch, stack, ha, hr)
+    del stack
+    torch.cuda.synchronize()
+    P, Q = slc.shape[0], slc.shape[1]
+
+    if args.impl == "reference":
+        slc_h, amp_h, valid_h = slc.cpu().numpy(), amp.cpu().numpy(), valid.cpu().numpy()
+        vals = []
+        for i in range(args.warmup + args.steps):
+            r = reference_rate(slc_h, amp_h, valid_h, rows, cols, kw, target_s=5.0)
+            if i >= args.warmup:
+                vals.append(r["value"])
+        v = float(np.mean(vals))
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mpixel/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": workload_name(rows, cols), "parallelism": "host cores"},
+                "cpu_baseline": dict(r, value=v),
+                "e2e": {"value": v, "unit": "Mpixel/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    s = tcoh_b200.make_settings(w["n"], **kw)
+    try:
+        be = tcoh_b200.Backend(s, Q, device=local, gram=args.gram)
+    except tcoh_b200.BackendError:
+        if args.gram != "tensor":
+            raise
+        args.gram = "fp32"
+        be = tcoh_b200.Backend(s, Q, device=local, gram=args.gram)
+    coh = torch.empty((rows, cols), dtype=torch.float32, device=dev)
+    count = torch.empty((rows, cols), dtype=torch.int32, device=dev)
+    stream = torch.cuda.Stream(dev)
+
+    def step(b=be):
+        b.run_device(slc, amp, valid, rows, cols, coh, count, stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+
+    # Per-stage device time of one more step (events around every launch).
+    be.set_timing(True)
+    step()
+    torch.cuda.synchronize()
+    stages = be.stage_stats()
+    be.set_timing(False)
+    launches = sum(v[1] for k, v in stages.items() if k != "copy")
+
+    npix = rows * cols
+    value = world * npix / (ms * 1e-3) / 1e6
+    cnt = count.cpu().numpy()
+    coh_h = coh.cpu().numpy()
+    validpix = cnt >= 0
+    estimated = cnt >= s.min_looks
+    lbar = float(cnt[validpix].mean()) if validpix.any() else 0.0
+    f_gram, f_link = flops_per_pixel(w["n"], lbar, w["estimator"] == "emi")
+    fp32_peak = tcoh_b200.fp32_peak_tflops(local)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    bf16_peak = peaks.get("bf16_tflops", 1590.0)
+    work = {
+        "shp": (shp_ops_per_pixel(w["n"], w["shp_test"], w["window"][0] * w["window"][1]) *
+                validpix.sum(), "fp32", fp32_peak),
+        "gram": (f_gram * validpix.sum(), "tensor" if args.gram == "tensor" else "fp32",
+                 bf16_peak if args.gram == "tensor" else fp32_peak),
+        "link": (f_link * estimated.sum(), "fp32", fp32_peak),
+    }
+    kernels = {}
+    for name, (flops, bound, peak) in work.items():
+        t_ms, nl = stages[name]
+        if t_ms <= 0 or nl == 0:
+            continue
+        per_launch_ms = t_ms / nl
+        achieved = flops / nl / (per_launch_ms * 1e-3) / 1e12
+        kernels[name] = {"ms_per_step": t_ms, "launches": nl, "achieved_tflops": achieved,
+                         "bound": bound, "peak_tflops": peak, "frac": achieved / peak}
+    dom = max(kernels, key=lambda k: kernels[k]["ms_per_step"])
+    d = kernels[dom]
+    roofline = {"kernel": dom, "bound": d["bound"], "achieved": d["achieved_tflops"],
+                "peak": d["peak_tflops"], "unit": "TFLOP/s",
+                "frac": d["frac"], "traffic": None,
+                "peak_source": ("measured FP32 FMA microbenchmark (tc_fp32_peak)"
+                                if d["bound"] == "fp32" else "MEASURED_PEAKS.json bf16_tflops")}
+
+    line = {"metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": workload_name(rows, cols), "gram": args.gram,
+                       "pixels_per_step": npix, "parallelism": "dp%d (independent strips)" % world,
+                       "l2": "inputs %.1f GB per step > 126 MB L2, no flush" % (
+                           (slc.numel() * 4 + amp.numel() * 4 + valid.numel()) / 1e9)},
+            "gpu_launches": launches * args.steps,
+            "roofline": roofline,
+            "stages": kernels,
+            "mean_shp_count": lbar,
+            "estimated_fraction": float(estimated.mean()),
+            "mean_coherence": float(np.nanmean(coh_h)) if np.isfinite(coh_h).any() else None,
+            "clocks": ck}
+
+    if not args.no_extras and rank == 0:
+        # Plain FP32 form of the Gram on the same strip.
+        if args.gram == "tensor":
+            try:
+                be32 = tcoh_b200.Backend(s, Q, device=local, gram="fp32")
+                c32 = torch.empty_like(coh)
+                n32 = torch.empty_like(count)
+
+                def step32():
+                    be32.run_device(slc, amp, valid, rows, cols, c32, n32, stream=stream)
+
+                step32()
+                torch.cuda.synchronize()
+                e0.record(stream)
+                for _ in range(3):
+                    step32()
+                e1.record(stream)
+                e1.synchronize()
+                ms32 = e0.elapsed_time(e1) / 3
+                line["plain_fp32"] = {"value": npix / (ms32 * 1e-3) / 1e6, "ms_per_step": ms32,
+                                      "tensor_over_plain": ms32 / ms}
+                be32.close()
+            except tcoh_b200.BackendError as e:
+                line["plain_fp32"] = {"error": str(e)}
+        # End to end through the C-ABI with page-locked host buffers.
+        slc_h = torch.empty(slc.shape, dtype=torch.float32, pin_memory=True)
+        amp_h = torch.empty(amp.shape, dtype=torch.float32, pin_memory=True)
+        valid_h = torch.empty(valid.shape, dtype=torch.uint8, pin_memory=True)
+        slc_h.copy_(slc)
+        amp_h.copy_(amp)
+        valid_h.copy_(valid)
+        out = {"coh": torch.empty((rows, cols), dtype=torch.float32, pin_memory=True).numpy(),
+               "count": torch.empty((rows, cols), dtype=torch.int32, pin_memory=True).numpy()}
+        sn, an, vn = slc_h.numpy(), amp_h.numpy(), valid_h.numpy()
+        be.run(sn, an, vn, rows, cols, out=out)
+        ke = max(1, min(3, args.steps))
+        t = time.perf_counter()
+        for _ in range(ke):
+            be.run(sn, an, vn, rows, cols, out=out)
+        dt = (time.perf_counter() - t) / ke
+        line["e2e"] = {"value": npix / dt / 1e6, "unit": "Mpixel/s",
+                       "h2d_bytes_per_step": int(sn.nbytes + an.nbytes + vn.nbytes),
+                       "d2h_bytes_per_step": int(out["coh"].nbytes + out["count"].nbytes),
+                       "ms_per_step": dt * 1e3, "api": "tc_run_ex (the ocl_run path)"}
+        # CPU baseline and accuracy on crops.
+        line["cpu_baseline"] = reference_rate(sn, an, vn, rows, cols, kw, target_s=12.0)
+        line["accuracy"] = accuracy(sn, an, vn, coh_h, cnt, rows, cols, kw)
+    be.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

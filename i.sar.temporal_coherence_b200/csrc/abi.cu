@@ -1,0 +1,750 @@
+/* C-ABI of the B200 backend: the ocl_* drop-in for ocl.c and the tc_*
+ * extensions (include/tcoh_b200.h).
+ *
+ * A context owns one CUDA stream and device buffers that grow on demand, as
+ * ocl.c's ensure_buffer does (ocl.c:265-277). A run processes the padded
+ * strip in chunks of output rows (a whole number of 16-row tile rows, all
+ * columns), each chunk being three launches on the context's stream:
+ * SHP selection -> masked coherence matrices -> phase linking. Chunks
+ * bound the intermediate matrices to a few hundred MB and keep every launch
+ * far below any watchdog limit, the role of ocl.c's 0.5 s chunks
+ * (ocl.c:22-23, 329-363).
+ */
+#include "../../include/tcoh_b200.h"
+#include "tcoh_internal.h"
+
+#include <dlfcn.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define TC_API extern "C" __attribute__((visibility("default")))
+
+/* ------------------------------------------------------------------ */
+/* Errors.                                                             */
+/* ------------------------------------------------------------------ */
+
+static thread_local char g_error[512];
+static void (*g_fatal)(const char *) = nullptr;
+
+static int set_error(int code, const char *fmt, ...)
+{
+    va_list ap;
+
+    va_start(ap, fmt);
+    vsnprintf(g_error, sizeof(g_error), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+#define CK(call)                                                                     \
+    do {                                                                             \
+        cudaError_t e_ = (call);                                                     \
+        if (e_ != cudaSuccess)                                                       \
+            return set_error(e_ == cudaErrorMemoryAllocation ? TC_ERR_MEMORY         \
+                                                              : TC_ERR_CUDA,         \
+                             "CUDA error %d (%s) in %s", (int)e_,                    \
+                             cudaGetErrorString(e_), #call);                         \
+    } while (0)
+
+typedef void (*grass_fatal_fn)(const char *, ...);
+
+/* ocl.c:44-48 reports through G_fatal_error, which never returns. */
+static void fatal(const char *what)
+{
+    char msg[700];
+
+    snprintf(msg, sizeof(msg), "%s: %s", what, g_error);
+    if (g_fatal) {
+        g_fatal(msg);
+    }
+    else {
+        grass_fatal_fn gf = (grass_fatal_fn)dlsym(RTLD_DEFAULT, "G_fatal_error");
+
+        if (gf)
+            gf("%s", msg);
+        fprintf(stderr, "ERROR: %s\n", msg);
+    }
+    exit(EXIT_FAILURE);
+}
+
+static void message(const char *fmt, ...)
+{
+    char msg[512];
+    va_list ap;
+    grass_fatal_fn gm = (grass_fatal_fn)dlsym(RTLD_DEFAULT, "G_message");
+
+    va_start(ap, fmt);
+    vsnprintf(msg, sizeof(msg), fmt, ap);
+    va_end(ap);
+    if (gm)
+        gm("%s", msg);
+    else if (getenv("TCOH_VERBOSE"))
+        fprintf(stderr, "%s\n", msg);
+}
+
+TC_API const char *tc_last_error(void) { return g_error; }
+
+TC_API void tc_set_fatal_handler(void (*handler)(const char *message)) { g_fatal = handler; }
+
+/* ------------------------------------------------------------------ */
+/* SHP constants (stats.c:61-95) and their float literals.             */
+/* ------------------------------------------------------------------ */
+
+static const double ad_alpha_tab[7] = {0.25, 0.10, 0.05, 0.025, 0.01, 0.005, 0.001};
+static const double ad_crit_tab[7] = {0.325, 1.226, 1.961, 2.718, 3.752, 4.592, 6.546};
+
+/* Standard deviation of the two-sample A2 under the null (Scholz and
+   Stephens 1987, eq. 4), samples of sizes na and nb. */
+static double ad_sigma_of(int na, int nb)
+{
+    const int k = 2, total = na + nb;
+    const double big_h = 1.0 / na + 1.0 / nb;
+    double h = 0.0, g = 0.0;
+
+    if (total <= 3)
+        return 1.0;
+    for (int j = 1; j < total; j++)
+        h += 1.0 / j;
+    for (int i = 1; i <= total - 2; i++)
+        for (int j = i + 1; j <= total - 1; j++)
+            g += 1.0 / ((double)(total - i) * j);
+    const double a = (4 * g - 6) * (k - 1) + (10 - 6 * g) * big_h;
+    const double b = (2 * g - 4) * k * k + 8 * h * k + (2 * g - 14 * h - 4) * big_h - 8 * h +
+                     4 * g - 6;
+    const double c = (6 * h + 2 * g - 2) * k * k + (4 * h - 4 * g + 6) * k +
+                     (2 * h - 6) * big_h + 4 * h;
+    const double d = (2 * h + 6) * k * k - 4 * h * k;
+    const double var = (a * pow(total, 3) + b * (double)total * total + c * total + d) /
+                       ((total - 1.0) * (total - 2.0) * (total - 3.0));
+
+    return var > 0 ? sqrt(var) : 1.0;
+}
+
+/* Two-sided standard normal quantile by bisection on erfc. */
+static double normal_quantile(double alpha)
+{
+    double lo = 0.0, hi = 40.0;
+
+    for (int i = 0; i < 200; i++) {
+        const double mid = 0.5 * (lo + hi);
+
+        if (erfc(mid / sqrt(2.0)) > alpha)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return 0.5 * (lo + hi);
+}
+
+TC_API int tc_shp_constants(struct settings *s)
+{
+    const int n = s->ndates;
+
+    if (!s || n < 2 || !(s->alpha > 0 && s->alpha < 1))
+        return set_error(TC_ERR_ARG, "invalid dates or alpha");
+    s->ks_max = (int)floor(sqrt(-0.5 * log(s->alpha / 2.0)) * sqrt(2.0 / n) * n);
+    s->ad_norm = 1.0 / (2.0 * n) * (2.0 / n);
+    s->ad_sigma = ad_sigma_of(n, n);
+    s->ad_crit = 0.0;
+    if (s->test == SHP_AD) {
+        int i;
+
+        if (s->alpha > ad_alpha_tab[0] || s->alpha < ad_alpha_tab[6])
+            return set_error(TC_ERR_ARG,
+                             "Anderson-Darling test: alpha must be between %g and %g",
+                             ad_alpha_tab[6], ad_alpha_tab[0]);
+        for (i = 0; i < 6; i++)
+            if (s->alpha >= ad_alpha_tab[i + 1])
+                break;
+        if (i == 6)
+            i = 5;
+        const double f = (log(s->alpha) - log(ad_alpha_tab[i])) /
+                         (log(ad_alpha_tab[i + 1]) - log(ad_alpha_tab[i]));
+
+        s->ad_crit = ad_crit_tab[i] + f * (ad_crit_tab[i + 1] - ad_crit_tab[i]);
+    }
+    s->tlog_crit = normal_quantile(s->alpha);
+    return TC_OK;
+}
+
+/* The float value of a constant written as "%.9ef" into the OpenCL build
+   options (ocl.c:222-229). */
+static float float_literal(double v)
+{
+    char buf[64];
+
+    snprintf(buf, sizeof(buf), "%.9e", v);
+    return strtof(buf, nullptr);
+}
+
+/* ------------------------------------------------------------------ */
+/* Context.                                                            */
+/* ------------------------------------------------------------------ */
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t size = 0;
+};
+
+static cudaError_t ensure(DevBuf &b, size_t size)
+{
+    if (b.p && b.size >= size)
+        return cudaSuccess;
+    if (b.p)
+        cudaFree(b.p);
+    b.p = nullptr;
+    b.size = 0;
+    cudaError_t e = cudaMalloc(&b.p, size ? size : 16);
+
+    if (e == cudaSuccess)
+        b.size = size;
+    return e;
+}
+
+enum { ST_PREP, ST_SHP, ST_GRAM, ST_LINK, ST_COPY, ST_COUNT };
+
+struct ocl {
+    int device;
+    int sms;
+    int n, wa, wr, test, emi, bias, min_looks, npairs, pairs_all;
+    TcShpConst shp;
+    int padded_cols;
+    tc_options opt;
+    int gram_block;
+    cudaStream_t stream;
+    DevBuf slc, amp, valid, coh, count, pairs, phases, status;
+    DevBuf soa, logstat, mask, gram, upper_tab, pair_tab, link_scratch;
+    bool timing;
+    float stage_ms[ST_COUNT];
+    int stage_launches[ST_COUNT];
+};
+
+static int check_settings(const struct settings *s, int padded_cols)
+{
+    if (!s)
+        return set_error(TC_ERR_ARG, "no settings");
+    if (s->ndates < 2 || s->ndates > TC_MAX_DATES)
+        return set_error(TC_ERR_ARG, "%d dates: 2 to %d are supported", s->ndates,
+                         TC_MAX_DATES);
+    if (s->win_az < 1 || s->win_rg < 1 || !(s->win_az & 1) || !(s->win_rg & 1))
+        return set_error(TC_ERR_ARG, "Window sizes must be odd, got %d,%d", s->win_az,
+                         s->win_rg);
+    if (s->win_az * s->win_rg > 32 * TC_MAX_MASK_WORDS)
+        return set_error(TC_ERR_ARG, "window of %d candidates: at most %d are supported",
+                         s->win_az * s->win_rg, 32 * TC_MAX_MASK_WORDS);
+    if ((int)s->test < 0 || (int)s->test > 2)
+        return set_error(TC_ERR_ARG, "unknown SHP test %d", (int)s->test);
+    if (s->npairs != 0 &&
+        s->npairs != (s->pairs_all ? s->ndates * (s->ndates - 1) / 2 : s->ndates - 1))
+        return set_error(TC_ERR_ARG, "%d pair planes for %d dates (%s pairs)", s->npairs,
+                         s->ndates, s->pairs_all ? "all" : "consecutive");
+    if (padded_cols < s->win_rg)
+        return set_error(TC_ERR_ARG, "padded strip of %d columns for a window of %d",
+                         padded_cols, s->win_rg);
+    return TC_OK;
+}
+
+TC_API int tc_device_count(void)
+{
+    int c = 0;
+
+    if (cudaGetDeviceCount(&c) != cudaSuccess)
+        return 0;
+    return c;
+}
+
+TC_API void ocl_list_devices(void)
+{
+    const int c = tc_device_count();
+
+    fprintf(stdout, "platform|device|type|name|version|compute_units|global_memory_mb\n");
+    for (int d = 0; d < c; d++) {
+        cudaDeviceProp p;
+
+        if (cudaGetDeviceProperties(&p, d) != cudaSuccess)
+            continue;
+        fprintf(stdout, "0|%d|GPU|%s|CUDA sm_%d%d|%d|%lu\n", d, p.name, p.major, p.minor,
+                p.multiProcessorCount, (unsigned long)(p.totalGlobalMem / (1024 * 1024)));
+    }
+    fflush(stdout);
+}
+
+static void free_bufs(struct ocl *o)
+{
+    DevBuf *b[] = {&o->slc, &o->amp, &o->valid, &o->coh, &o->count, &o->pairs,
+                   &o->phases, &o->status, &o->soa, &o->logstat, &o->mask, &o->gram,
+                   &o->upper_tab, &o->pair_tab, &o->link_scratch};
+
+    for (size_t i = 0; i < sizeof(b) / sizeof(b[0]); i++)
+        if (b[i]->p) {
+            cudaFree(b[i]->p);
+            b[i]->p = nullptr;
+            b[i]->size = 0;
+        }
+}
+
+TC_API int tc_open(int device, const struct settings *s, int padded_cols,
+                   const struct tc_options *opt, struct ocl **out, size_t *max_alloc)
+{
+    int rc, count = 0;
+
+    if (!out)
+        return set_error(TC_ERR_ARG, "no output handle");
+    *out = nullptr;
+    if ((rc = check_settings(s, padded_cols)) != TC_OK)
+        return rc;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+        return set_error(TC_ERR_DEVICE, "No CUDA device found");
+    if (device < 0)
+        device = 0;
+    if (device >= count)
+        return set_error(TC_ERR_DEVICE, "CUDA device %d not found (%d devices, see -l)",
+                         device, count);
+    cudaDeviceProp prop;
+
+    CK(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10)
+        return set_error(TC_ERR_DEVICE,
+                         "CUDA device %d (%s, sm_%d%d) is not an sm_100 GPU; this build "
+                         "targets sm_100a only",
+                         device, prop.name, prop.major, prop.minor);
+    CK(cudaSetDevice(device));
+
+    struct ocl *o = new ocl();
+
+    o->device = device;
+    o->sms = prop.multiProcessorCount;
+    o->n = s->ndates;
+    o->wa = s->win_az;
+    o->wr = s->win_rg;
+    o->test = (int)s->test;
+    o->emi = s->emi;
+    o->bias = s->bias;
+    o->min_looks = s->min_looks;
+    o->npairs = s->npairs;
+    o->pairs_all = s->pairs_all;
+    o->padded_cols = padded_cols;
+    o->shp.test = (int)s->test;
+    o->shp.ks_max = s->ks_max;
+    o->shp.ad_norm = float_literal(s->ad_norm);
+    o->shp.ad_sigma = float_literal(s->ad_sigma);
+    o->shp.ad_crit = float_literal(s->ad_crit);
+    o->shp.tlog_crit = float_literal(s->tlog_crit);
+    o->opt.gram = tc_gram_tensor_supported(TcStrip{o->n}) ? TC_GRAM_TENSOR : TC_GRAM_FP32;
+    o->opt.split_terms = 3;
+    o->opt.chunk_pixels = 0;
+    if (opt) {
+        const int dflt = o->opt.gram;
+
+        o->opt = *opt;
+        if (o->opt.gram < 0)
+            o->opt.gram = dflt;
+    }
+    if (o->opt.split_terms != 2 && o->opt.split_terms != 3)
+        o->opt.split_terms = 3;
+    if (o->opt.gram != TC_GRAM_FP32 && o->opt.gram != TC_GRAM_TENSOR) {
+        delete o;
+        return set_error(TC_ERR_ARG, "unknown Gram arithmetic %d", opt->gram);
+    }
+    if (o->opt.gram == TC_GRAM_TENSOR && !tc_gram_tensor_supported(TcStrip{o->n})) {
+        delete o;
+        return set_error(TC_ERR_ARG, "tensor-core Gram not available for %d dates", s->ndates);
+    }
+    o->gram_block = tc_gram_block_for(o->n);
+    o->timing = false;
+    memset(o->stage_ms, 0, sizeof(o->stage_ms));
+    memset(o->stage_launches, 0, sizeof(o->stage_launches));
+
+    cudaError_t e = cudaStreamCreateWithFlags(&o->stream, cudaStreamNonBlocking);
+
+    if (e != cudaSuccess) {
+        delete o;
+        return set_error(TC_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+    }
+    /* Date pairs of the packed upper triangle and of the pair planes. */
+    {
+        const int n = o->n, npu = tc_npu(n);
+        unsigned short *up = (unsigned short *)malloc(sizeof(unsigned short) * npu);
+        unsigned short *pt = (unsigned short *)malloc(sizeof(unsigned short) * (n * n + 1));
+        int q = 0;
+
+        for (int i = 0; i < n; i++)
+            for (int j = i; j < n; j++)
+                up[q++] = (unsigned short)(i << 8 | j);
+        q = 0;
+        for (int i = 0; i < n - 1; i++)
+            for (int j = i + 1; j < (o->pairs_all ? n : i + 2); j++)
+                pt[q++] = (unsigned short)(i << 8 | j);
+        e = ensure(o->upper_tab, sizeof(unsigned short) * npu);
+        if (e == cudaSuccess)
+            e = ensure(o->pair_tab, sizeof(unsigned short) * (q ? q : 1));
+        if (e == cudaSuccess)
+            e = cudaMemcpy(o->upper_tab.p, up, sizeof(unsigned short) * npu,
+                           cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && q)
+            e = cudaMemcpy(o->pair_tab.p, pt, sizeof(unsigned short) * q,
+                           cudaMemcpyHostToDevice);
+        free(up);
+        free(pt);
+        if (e != cudaSuccess) {
+            free_bufs(o);
+            cudaStreamDestroy(o->stream);
+            delete o;
+            return set_error(TC_ERR_CUDA, "table upload: %s", cudaGetErrorString(e));
+        }
+    }
+    if (max_alloc) {
+        size_t fr = 0, tot = 0;
+
+        cudaMemGetInfo(&fr, &tot);
+        /* The strip (slc + amp, 12 N bytes per pixel), the outputs and the
+           internal chunk buffers must fit together. */
+        *max_alloc = fr / 3;
+    }
+    message("CUDA device: %s (NVIDIA CUDA, %d SMs)", prop.name, o->sms);
+    *out = o;
+    return TC_OK;
+}
+
+TC_API int tc_close(struct ocl *o)
+{
+    if (!o)
+        return TC_OK;
+    cudaSetDevice(o->device);
+    cudaStreamSynchronize(o->stream);
+    free_bufs(o);
+    cudaStreamDestroy(o->stream);
+    delete o;
+    return TC_OK;
+}
+
+TC_API int tc_set_timing(struct ocl *o, int on)
+{
+    if (!o)
+        return set_error(TC_ERR_ARG, "no context");
+    o->timing = on != 0;
+    return TC_OK;
+}
+
+TC_API int tc_stage_stats(const struct ocl *o, float *ms, int *launches, int n)
+{
+    if (!o)
+        return 0;
+    if (n > ST_COUNT)
+        n = ST_COUNT;
+    for (int i = 0; i < n; i++) {
+        if (ms)
+            ms[i] = o->stage_ms[i];
+        if (launches)
+            launches[i] = o->stage_launches[i];
+    }
+    return n;
+}
+
+/* ------------------------------------------------------------------ */
+/* Runs.                                                               */
+/* ------------------------------------------------------------------ */
+
+/* Event pairs around launches when timing is on. */
+struct Timer {
+    struct ocl *o;
+    cudaStream_t st;
+    cudaEvent_t ev[2 * 1024];
+    int stage[1024];
+    int used = 0;
+
+    Timer(struct ocl *o_, cudaStream_t s) : o(o_), st(s) {}
+    int begin(int stg)
+    {
+        if (!o->timing || used >= 1024)
+            return -1;
+        const int i = used++;
+
+        cudaEventCreate(&ev[2 * i]);
+        cudaEventCreate(&ev[2 * i + 1]);
+        stage[i] = stg;
+        cudaEventRecord(ev[2 * i], st);
+        return i;
+    }
+    void end(int i)
+    {
+        if (i >= 0)
+            cudaEventRecord(ev[2 * i + 1], st);
+    }
+    /* After a synchronize: sum per stage. */
+    void collect()
+    {
+        for (int i = 0; i < used; i++) {
+            float ms = 0.f;
+
+            cudaEventSynchronize(ev[2 * i + 1]);
+            cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]);
+            o->stage_ms[stage[i]] += ms;
+            if (stage[i] != ST_COPY)
+                o->stage_launches[stage[i]]++;
+            cudaEventDestroy(ev[2 * i]);
+            cudaEventDestroy(ev[2 * i + 1]);
+        }
+        used = 0;
+    }
+};
+
+static int chunk_rows_for(const struct ocl *o, int rows, int cols)
+{
+    const int tiles_x = (cols + TC_TILE_W - 1) / TC_TILE_W;
+    const long long per_tile_row = (long long)tiles_x * TC_TILE_PIX;
+    long long target = o->opt.chunk_pixels;
+
+    if (target <= 0) {
+        /* About 256 MB of coherence matrices per chunk. */
+        target = (256ll << 20) / ((long long)tc_npu(o->n) * 8);
+    }
+    long long trows = target / per_tile_row;
+
+    if (trows < 1)
+        trows = 1;
+    long long r = trows * TC_TILE_H;
+
+    if (r > rows)
+        r = (rows + TC_TILE_H - 1) / TC_TILE_H * TC_TILE_H;
+    return (int)r;
+}
+
+/* The computation on device buffers (asynchronous on st). */
+static int run_device(struct ocl *o, const float *slc, const float *amp,
+                      const unsigned char *valid, int padded_rows, int rows, int cols,
+                      float *coh, int *count, float *pairs, float *phases,
+                      unsigned char *status, cudaStream_t st, Timer &tm)
+{
+    if (rows < 1 || cols < 1)
+        return set_error(TC_ERR_ARG, "empty strip (%d x %d)", rows, cols);
+    if (cols + o->wr - 1 != o->padded_cols)
+        return set_error(TC_ERR_ARG, "%d columns do not match the padded width %d", cols,
+                         o->padded_cols);
+    if (padded_rows != rows + o->wa - 1)
+        return set_error(TC_ERR_ARG, "%d padded rows for %d rows and a %d-line window",
+                         padded_rows, rows, o->wa);
+    if (o->npairs && !pairs)
+        return set_error(TC_ERR_ARG, "no pair buffer for %d pair planes", o->npairs);
+    if (o->opt.gram == TC_GRAM_TENSOR && !tc_gram_tensor_supported(TcStrip{o->n}))
+        return set_error(TC_ERR_ARG, "tensor-core Gram not available for %d dates", o->n);
+
+    TcStrip s;
+
+    s.n = o->n;
+    s.wa = o->wa;
+    s.wr = o->wr;
+    s.area = o->wa * o->wr;
+    s.mask_words = (s.area + 31) / 32;
+    s.W = o->padded_cols;
+    s.padded_rows = padded_rows;
+    s.rows = rows;
+    s.cols = cols;
+    s.npad = (long long)padded_rows * o->padded_cols;
+    s.planes = (o->n + o->gram_block - 1) / o->gram_block * o->gram_block;
+
+    const int crows = chunk_rows_for(o, rows, cols);
+    const int tiles_x = (cols + TC_TILE_W - 1) / TC_TILE_W;
+    const long long max_npix = (long long)(crows / TC_TILE_H) * tiles_x * TC_TILE_PIX;
+
+    CK(ensure(o->mask, sizeof(uint32_t) * s.mask_words * max_npix));
+    CK(ensure(o->gram, sizeof(float2) * tc_npu(o->n) * max_npix));
+    CK(ensure(o->link_scratch, tc_link_scratch_bytes(o->n, o->sms)));
+    if (o->opt.gram == TC_GRAM_FP32)
+        CK(ensure(o->soa, sizeof(float2) * s.planes * s.npad));
+    if (o->test == SHP_TLOG)
+        CK(ensure(o->logstat, sizeof(float2) * s.npad));
+
+    int t;
+
+    if (o->opt.gram == TC_GRAM_FP32) {
+        t = tm.begin(ST_PREP);
+        CK(tc_launch_prep(s, slc, (float2 *)o->soa.p, st));
+        tm.end(t);
+    }
+    if (o->test == SHP_TLOG) {
+        t = tm.begin(ST_PREP);
+        CK(tc_launch_logstats(s, amp, valid, (float2 *)o->logstat.p, st));
+        tm.end(t);
+    }
+    TcLinkConst lk;
+
+    lk.emi = o->emi;
+    lk.bias = o->bias;
+    lk.min_looks = o->min_looks;
+    lk.npairs = o->npairs;
+    lk.pairs_all = o->pairs_all;
+    for (int row0 = 0; row0 < rows; row0 += crows) {
+        TcChunk c;
+
+        c.row0 = row0;
+        c.nrows = rows - row0 < crows ? rows - row0 : crows;
+        c.tiles_x = tiles_x;
+        c.tiles_y = (c.nrows + TC_TILE_H - 1) / TC_TILE_H;
+        c.npix = c.tiles_x * c.tiles_y * TC_TILE_PIX;
+
+        t = tm.begin(ST_SHP);
+        CK(tc_launch_shp(s, c, o->shp, amp, valid, (const float2 *)o->logstat.p,
+                         (uint32_t *)o->mask.p, count, o->sms, st));
+        tm.end(t);
+        t = tm.begin(ST_GRAM);
+        if (o->opt.gram == TC_GRAM_FP32)
+            CK(tc_launch_gram_fp32(s, c, o->gram_block, (const float2 *)o->soa.p,
+                                   (const uint32_t *)o->mask.p, (float2 *)o->gram.p, st));
+        else
+            CK(tc_launch_gram_tensor(s, c, o->opt.split_terms, slc, (const uint32_t *)o->mask.p,
+                                     (float2 *)o->gram.p, st));
+        tm.end(t);
+        t = tm.begin(ST_LINK);
+        CK(tc_launch_link(s, c, lk, (const float2 *)o->gram.p, count,
+                          (const unsigned short *)o->upper_tab.p,
+                          (const unsigned short *)o->pair_tab.p, (double *)o->link_scratch.p,
+                          coh, pairs, phases, status, o->sms, st));
+        tm.end(t);
+    }
+    return TC_OK;
+}
+
+TC_API int tc_run_device(struct ocl *o, const float *slc, const float *amp,
+                         const unsigned char *valid, int padded_rows, int rows, int cols,
+                         float *coh, int *count, float *pairs, float *phases,
+                         unsigned char *status, void *stream)
+{
+    if (!o)
+        return set_error(TC_ERR_ARG, "no context");
+    CK(cudaSetDevice(o->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    Timer tm(o, st);
+
+    memset(o->stage_ms, 0, sizeof(o->stage_ms));
+    memset(o->stage_launches, 0, sizeof(o->stage_launches));
+    int rc = run_device(o, slc, amp, valid, padded_rows, rows, cols, coh, count, pairs,
+                        phases, status, st, tm);
+
+    if (o->timing) {
+        cudaStreamSynchronize(st);
+        tm.collect();
+    }
+    return rc;
+}
+
+TC_API int tc_run_ex(struct ocl *o, const float *slc, const float *amp,
+                     const unsigned char *valid, int padded_rows, int rows, int cols,
+                     float *coh, int *count, float *pairs, float *phases,
+                     unsigned char *status)
+{
+    if (!o)
+        return set_error(TC_ERR_ARG, "no context");
+    if (!slc || !amp || !valid || !coh || !count)
+        return set_error(TC_ERR_ARG, "missing strip or output buffer");
+    if (rows < 1 || cols < 1 || padded_rows != rows + o->wa - 1 ||
+        cols + o->wr - 1 != o->padded_cols)
+        return set_error(TC_ERR_ARG, "strip of %d x %d (padded %d x %d) does not match "
+                         "the window %d x %d",
+                         rows, cols, padded_rows, o->padded_cols, o->wa, o->wr);
+    CK(cudaSetDevice(o->device));
+    const size_t npad = (size_t)padded_rows * o->padded_cols;
+    const size_t nout = (size_t)rows * cols;
+    const size_t n = o->n;
+    cudaStream_t st = o->stream;
+    Timer tm(o, st);
+
+    memset(o->stage_ms, 0, sizeof(o->stage_ms));
+    memset(o->stage_launches, 0, sizeof(o->stage_launches));
+    CK(ensure(o->slc, npad * n * 2 * sizeof(float)));
+    CK(ensure(o->amp, npad * n * sizeof(float)));
+    CK(ensure(o->valid, npad));
+    CK(ensure(o->coh, nout * sizeof(float)));
+    CK(ensure(o->count, nout * sizeof(int)));
+    if (o->npairs)
+        CK(ensure(o->pairs, o->npairs * nout * sizeof(float)));
+    if (phases)
+        CK(ensure(o->phases, nout * n * sizeof(float)));
+    if (status)
+        CK(ensure(o->status, nout));
+
+    int t = tm.begin(ST_COPY);
+
+    CK(cudaMemcpyAsync(o->slc.p, slc, npad * n * 2 * sizeof(float), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(o->amp.p, amp, npad * n * sizeof(float), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(o->valid.p, valid, npad, cudaMemcpyHostToDevice, st));
+    tm.end(t);
+    int rc = run_device(o, (const float *)o->slc.p, (const float *)o->amp.p,
+                        (const unsigned char *)o->valid.p, padded_rows, rows, cols,
+                        (float *)o->coh.p, (int *)o->count.p,
+                        o->npairs ? (float *)o->pairs.p : nullptr,
+                        phases ? (float *)o->phases.p : nullptr,
+                        status ? (unsigned char *)o->status.p : nullptr, st, tm);
+
+    if (rc != TC_OK) {
+        cudaStreamSynchronize(st);
+        tm.collect();
+        return rc;
+    }
+    t = tm.begin(ST_COPY);
+    CK(cudaMemcpyAsync(coh, o->coh.p, nout * sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(count, o->count.p, nout * sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (o->npairs && pairs)
+        CK(cudaMemcpyAsync(pairs, o->pairs.p, o->npairs * nout * sizeof(float),
+                           cudaMemcpyDeviceToHost, st));
+    if (phases)
+        CK(cudaMemcpyAsync(phases, o->phases.p, nout * n * sizeof(float),
+                           cudaMemcpyDeviceToHost, st));
+    if (status)
+        CK(cudaMemcpyAsync(status, o->status.p, nout, cudaMemcpyDeviceToHost, st));
+    tm.end(t);
+    CK(cudaStreamSynchronize(st));
+    tm.collect();
+    return TC_OK;
+}
+
+/* ------------------------------------------------------------------ */
+/* ocl_* drop-in.                                                      */
+/* ------------------------------------------------------------------ */
+
+TC_API struct ocl *ocl_open(int platform, int device, const struct settings *s,
+                            int padded_cols, size_t *max_alloc)
+{
+    struct ocl *o = nullptr;
+    tc_options opt;
+    const char *env;
+
+    if (platform < 0 && device >= 0) {
+        set_error(TC_ERR_ARG, "Option device requires option platform");
+        fatal("CUDA backend");
+    }
+    if (platform > 0) {
+        set_error(TC_ERR_DEVICE, "platform %d not found (1 platform, see -l)", platform);
+        fatal("CUDA backend");
+    }
+    opt.gram = tc_gram_tensor_supported(TcStrip{s ? s->ndates : 0}) ? TC_GRAM_TENSOR
+                                                                     : TC_GRAM_FP32;
+    opt.split_terms = 3;
+    opt.chunk_pixels = 0;
+    if ((env = getenv("TCOH_GRAM")) && !strcmp(env, "fp32"))
+        opt.gram = TC_GRAM_FP32;
+    if ((env = getenv("TCOH_SPLIT_TERMS")))
+        opt.split_terms = atoi(env);
+    if ((env = getenv("TCOH_CHUNK_PIXELS")))
+        opt.chunk_pixels = atoi(env);
+    if (tc_open(device, s, padded_cols, &opt, &o, max_alloc) != TC_OK)
+        fatal("CUDA backend");
+    return o;
+}
+
+TC_API void ocl_run(struct ocl *o, const float *slc, const float *amp,
+                    const unsigned char *valid, int padded_rows, int rows, int cols,
+                    float *coh, int *count, float *pairs)
+{
+    if (tc_run_ex(o, slc, amp, valid, padded_rows, rows, cols, coh, count, pairs, nullptr,
+                  nullptr) != TC_OK)
+        fatal("CUDA backend");
+}
+
+TC_API void ocl_close(struct ocl *o)
+{
+    tc_close(o);
+}

@@ -1,0 +1,1299 @@
+/* Phase linking and temporal coherence for stacks of up to 32 dates: two
+ * pixels per warp, one per 16-lane half.
+ *
+ * Lane l of a half owns rows l and l + 16 of its pixel's matrices, in
+ * registers. The stages and their numerics are those of kernels_link.cu
+ * (see there for the reference lines); this layout exists for speed: each
+ * Householder step is gated by reductions and shared-memory round trips,
+ * and with two pixels per warp (two rows per lane) every such latency and
+ * every serial scalar computation serves two pixels, while the rank-2
+ * updates of two rows per lane give the schedulers independent work.
+ *
+ * The Householder reduction runs in float. At step k the pivot column k of
+ * a row sits in r[0] and its trailing columns k+1 .. n-1 in r[1 ..]; the
+ * rank-2 update writes column j into r[j - 1], so register indices stay
+ * static while k is a run-time loop (the code stays small). The Householder
+ * vectors are parked in the lower triangle of T, which only mirrors the
+ * upper one.
+ *
+ * EMI: |T| is inverted in double (Gauss-Jordan when every pivot exceeds
+ * 1e-5; through |T|^2 when |T| is indefinite; Jacobi pseudo-inverse with the
+ * absolute floor 1e-9 of tests/reference.py:151-156 when it is close to
+ * singular). M = |T|^-1 o T is reduced in float, and the eigenvector of its
+ * smallest eigenvalue is then refined in double: the residual
+ * r = M x - mu x (M and mu in double) is mapped by the float Householder
+ * basis Q onto the tridiagonal, the correction solves (tri - mu) t = Q^H r
+ * off the eigen-direction, and x -= Q t; two such steps give double
+ * accuracy whenever the float rounding of M is small against the gap of its
+ * two smallest eigenvalues.
+ */
+#include "tcoh_internal.h"
+
+#include <math.h>
+
+#define FULL 0xffffffffu
+
+namespace {
+
+struct Grp {
+    int lane, gl, base;
+    unsigned mask;
+};
+
+__device__ __forceinline__ Grp make_grp(int lane)
+{
+    Grp g;
+
+    g.lane = lane;
+    g.gl = lane & 15;
+    g.base = lane & 16;
+    g.mask = 0xFFFFu << g.base;
+    return g;
+}
+
+template <typename T>
+__device__ __forceinline__ T gsum(T v, const Grp &g)
+{
+#pragma unroll
+    for (int o = 8; o; o >>= 1)
+        v += __shfl_xor_sync(g.mask, v, o);
+    return v;
+}
+
+__device__ __forceinline__ float gmaxf(float v, const Grp &g)
+{
+#pragma unroll
+    for (int o = 8; o; o >>= 1)
+        v = fmaxf(v, __shfl_xor_sync(g.mask, v, o));
+    return v;
+}
+
+__device__ __forceinline__ float gminf(float v, const Grp &g)
+{
+#pragma unroll
+    for (int o = 8; o; o >>= 1)
+        v = fminf(v, __shfl_xor_sync(g.mask, v, o));
+    return v;
+}
+
+__device__ __forceinline__ double gmaxd(double v, const Grp &g)
+{
+#pragma unroll
+    for (int o = 8; o; o >>= 1)
+        v = fmax(v, __shfl_xor_sync(g.mask, v, o));
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T gbcast(T v, int row, const Grp &g)
+{
+    return __shfl_sync(g.mask, v, g.base | (row & 15));
+}
+
+__device__ __forceinline__ void gsync(const Grp &g) { __syncwarp(g.mask); }
+
+/* Per-group shared workspace (byte offsets, 16-byte aligned). */
+struct HalfLayout {
+    int n, ld;
+    int off_T, off_G, off_vw, off_lu, off_tau, off_d, off_e, off_df, off_e2f, off_y,
+        off_nrm, off_zs, off_rs, off_lam, off_x;
+    int per_group;
+};
+
+struct HWs {
+    float2 *T;
+    double *G;
+    float4 *vw;
+    float4 *lu;
+    float2 *tau;
+    float *d, *e, *df, *e2f, *y, *nrm;
+    float2 *zs;
+    double *rs, *lam;
+    double2 *x; /* double vectors of the refinement (2 x 32) */
+};
+
+__device__ __forceinline__ HWs hws(unsigned char *base, const HalfLayout &L)
+{
+    HWs w;
+
+    w.T = (float2 *)(base + L.off_T);
+    w.G = (double *)(base + L.off_G);
+    w.vw = (float4 *)(base + L.off_vw);
+    w.lu = (float4 *)(base + L.off_lu);
+    w.tau = (float2 *)(base + L.off_tau);
+    w.d = (float *)(base + L.off_d);
+    w.e = (float *)(base + L.off_e);
+    w.df = (float *)(base + L.off_df);
+    w.e2f = (float *)(base + L.off_e2f);
+    w.y = (float *)(base + L.off_y);
+    w.nrm = (float *)(base + L.off_nrm);
+    w.zs = (float2 *)(base + L.off_zs);
+    w.rs = (double *)(base + L.off_rs);
+    w.lam = (double *)(base + L.off_lam);
+    w.x = (double2 *)(base + L.off_x);
+    return w;
+}
+
+/* ------------------------------------------------------------------ */
+/* Householder reduction of the group's matrix (rows in r0, r1).       */
+/* ------------------------------------------------------------------ */
+
+__device__ void householder(float2 (&r0)[32], float2 (&r1)[32], int n, const HWs &w, int ld,
+                            const Grp &g)
+{
+    const int i0 = g.gl, i1 = g.gl + 16;
+
+    for (int k = 0; k < n - 1; k++) {
+        const int len = n - 1 - k;
+        const float2 c0 = r0[0], c1 = r1[0];
+        float xn2 = (i0 >= k + 2 && i0 < n ? c0.x * c0.x + c0.y * c0.y : 0.f) +
+                    (i1 >= k + 2 && i1 < n ? c1.x * c1.x + c1.y * c1.y : 0.f);
+
+        xn2 = gsum(xn2, g);
+        const float2 sa = k + 1 < 16 ? c0 : c1;
+        const float2 alpha = make_float2(gbcast(sa.x, k + 1, g), gbcast(sa.y, k + 1, g));
+        const float dk = gbcast(k < 16 ? c0.x : c1.x, k, g);
+        float beta, tr = 0.f, ti = 0.f, sr = 0.f, si = 0.f;
+
+        if (xn2 == 0.f && alpha.y == 0.f)
+            beta = alpha.x;
+        else {
+            beta = -copysignf(sqrtf(alpha.x * alpha.x + alpha.y * alpha.y + xn2), alpha.x);
+            const float ib = __frcp_rn(beta);
+
+            tr = (beta - alpha.x) * ib;
+            ti = -alpha.y * ib;
+            const float dr = alpha.x - beta, di = alpha.y;
+            const float iden = __frcp_rn(dr * dr + di * di);
+
+            sr = dr * iden;
+            si = -di * iden;
+        }
+        const bool refl = !(tr == 0.f && ti == 0.f);
+        float2 v0 = make_float2(0.f, 0.f), v1 = make_float2(0.f, 0.f);
+
+        if (i0 == k + 1)
+            v0 = make_float2(1.f, 0.f);
+        else if (i0 > k + 1 && i0 < n)
+            v0 = refl ? make_float2(c0.x * sr - c0.y * si, c0.x * si + c0.y * sr) : c0;
+        if (i1 == k + 1)
+            v1 = make_float2(1.f, 0.f);
+        else if (i1 > k + 1 && i1 < n)
+            v1 = refl ? make_float2(c1.x * sr - c1.y * si, c1.x * si + c1.y * sr) : c1;
+        if (i0 > k && i0 < n)
+            w.T[i0 * ld + k] = v0;
+        if (i1 > k && i1 < n)
+            w.T[i1 * ld + k] = v1;
+        if (g.gl == 0) {
+            w.d[k] = dk;
+            w.e[k] = beta;
+            w.tau[k] = make_float2(tr, ti);
+        }
+        /* With tau = 0 the update below is exact zero: only the shift. */
+        ((float2 *)w.vw)[2 * i0] = v0;
+        ((float2 *)w.vw)[2 * i1] = v1;
+        gsync(g);
+        float2 p0a = make_float2(0.f, 0.f), p0b = p0a, p1a = p0a, p1b = p0a;
+
+#pragma unroll
+        for (int jb = 1; jb < 32; jb += 4) {
+            if (jb > len)
+                break;
+#pragma unroll
+            for (int jj = jb; jj < jb + 4 && jj < 32; jj++) {
+                if (jj <= len) {
+                    const float2 vj = ((const float2 *)w.vw)[2 * (k + jj)];
+                    float2 &q0 = (jj & 1) ? p0b : p0a;
+                    float2 &q1 = (jj & 1) ? p1b : p1a;
+
+                    q0.x = fmaf(r0[jj].x, vj.x, fmaf(-r0[jj].y, vj.y, q0.x));
+                    q0.y = fmaf(r0[jj].x, vj.y, fmaf(r0[jj].y, vj.x, q0.y));
+                    q1.x = fmaf(r1[jj].x, vj.x, fmaf(-r1[jj].y, vj.y, q1.x));
+                    q1.y = fmaf(r1[jj].x, vj.y, fmaf(r1[jj].y, vj.x, q1.y));
+                }
+            }
+        }
+        const float2 p0 = make_float2(p0a.x + p0b.x, p0a.y + p0b.y);
+        const float2 p1 = make_float2(p1a.x + p1b.x, p1a.y + p1b.y);
+        float2 w0 = make_float2(tr * p0.x - ti * p0.y, tr * p0.y + ti * p0.x);
+        float2 w1 = make_float2(tr * p1.x - ti * p1.y, tr * p1.y + ti * p1.x);
+        float pr = (i0 > k ? w0.x * v0.x + w0.y * v0.y : 0.f) + (i1 > k ? w1.x * v1.x + w1.y * v1.y : 0.f);
+        float pi = (i0 > k ? w0.x * v0.y - w0.y * v0.x : 0.f) + (i1 > k ? w1.x * v1.y - w1.y * v1.x : 0.f);
+
+        pr = gsum(pr, g);
+        pi = gsum(pi, g);
+        const float hr = -0.5f * (tr * pr - ti * pi), hi = -0.5f * (tr * pi + ti * pr);
+
+        w0.x += hr * v0.x - hi * v0.y;
+        w0.y += hr * v0.y + hi * v0.x;
+        w1.x += hr * v1.x - hi * v1.y;
+        w1.y += hr * v1.y + hi * v1.x;
+        if (i0 <= k)
+            w0 = make_float2(0.f, 0.f);
+        if (i1 <= k)
+            w1 = make_float2(0.f, 0.f);
+        ((float2 *)w.vw)[2 * i0 + 1] = w0;
+        ((float2 *)w.vw)[2 * i1 + 1] = w1;
+        gsync(g);
+#pragma unroll
+        for (int jb = 1; jb < 32; jb += 4) {
+            if (jb > len)
+                break;
+#pragma unroll
+            for (int jj = jb; jj < jb + 4 && jj < 32; jj++) {
+                if (jj <= len) {
+                    const float4 q = w.vw[k + jj]; /* v_j (xy), w_j (zw) */
+                    float2 t0 = r0[jj], t1 = r1[jj];
+
+                    t0.x -= v0.x * q.z + v0.y * q.w + w0.x * q.x + w0.y * q.y;
+                    t0.y -= v0.y * q.z - v0.x * q.w + w0.y * q.x - w0.x * q.y;
+                    t1.x -= v1.x * q.z + v1.y * q.w + w1.x * q.x + w1.y * q.y;
+                    t1.y -= v1.y * q.z - v1.x * q.w + w1.y * q.x - w1.x * q.y;
+                    r0[jj - 1] = t0;
+                    r1[jj - 1] = t1;
+                }
+            }
+        }
+        gsync(g);
+    }
+    {
+        const float dl = gbcast(n - 1 < 16 ? r0[0].x : r1[0].x, n - 1, g);
+
+        if (g.gl == 0)
+            w.d[n - 1] = dl;
+    }
+    gsync(g);
+}
+
+/* ------------------------------------------------------------------ */
+/* Tridiagonal eigenvector.                                            */
+/* ------------------------------------------------------------------ */
+
+__device__ __forceinline__ int sturm16(const float *d, const float *e2, int n, float x,
+                                       float pivmin)
+{
+    float q = d[0] - x;
+    int c = q < 0.f;
+
+    for (int i = 1; i < n; i++) {
+        if (fabsf(q) < pivmin)
+            q = -pivmin;
+        q = d[i] - x - __fdividef(e2[i - 1], q);
+        c += q < 0.f;
+    }
+    return c;
+}
+
+/* Eigenvalue of rank `index` of the group's tridiagonal (w.d, w.e), by
+   17-way multisection of its Gershgorin interval. */
+__device__ float tri_eigenvalue(int n, int index, const HWs &w, const Grp &g, float &norm,
+                                unsigned &status)
+{
+    const int i0 = g.gl, i1 = g.gl + 16;
+    float lo = INFINITY, hi = -INFINITY;
+
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+        const int r = t ? i1 : i0;
+
+        if (r < n) {
+            const float rad = (r > 0 ? fabsf(w.e[r - 1]) : 0.f) + (r < n - 1 ? fabsf(w.e[r]) : 0.f);
+
+            lo = fminf(lo, w.d[r] - rad);
+            hi = fmaxf(hi, w.d[r] + rad);
+            if (r < n - 1)
+                w.e2f[r] = w.e[r] * w.e[r];
+        }
+    }
+    lo = gminf(lo, g);
+    hi = gmaxf(hi, g);
+    norm = fmaxf(fabsf(lo), fabsf(hi));
+    lo -= 1.0e-6f * norm + 1.0e-30f;
+    hi += 1.0e-6f * norm + 1.0e-30f;
+    gsync(g);
+    const float pivmin = 1.0e-30f + 1.0e-14f * norm;
+    int round = 0;
+
+    for (; round < 20; round++) {
+        const float xq = lo + (hi - lo) * ((float)(g.gl + 1) * (1.0f / 17.0f));
+        const int cnt = sturm16(w.d, w.e2f, n, xq, pivmin);
+        const unsigned gt = (__ballot_sync(g.mask, cnt > index) >> g.base) & 0xFFFFu;
+        float nlo, nhi;
+
+        if (gt == 0u) {
+            nlo = gbcast(xq, 15, g);
+            nhi = hi;
+        }
+        else {
+            const int f = __ffs(gt) - 1;
+
+            nhi = gbcast(xq, f, g);
+            nlo = gbcast(xq, f > 0 ? f - 1 : 0, g);
+            if (f == 0)
+                nlo = lo;
+        }
+        nlo = fmaxf(nlo, lo);
+        nhi = fminf(nhi, hi);
+        if (!(nlo > lo || nhi < hi))
+            break;
+        lo = nlo;
+        hi = nhi;
+    }
+    if (round == 20)
+        status |= TC_STATUS_ITER_CAP;
+    return 0.5f * (lo + hi);
+}
+
+/* Partially pivoted LU of tri - lambda I, into w.lu (written by the first
+   lane of the group); returns the pivot bits. Every lane computes it. */
+template <typename R>
+__device__ unsigned long long tri_lu(int n, R lambda, R tiny, const HWs &w, const Grp &g)
+{
+    R dd = (R)w.d[0] - lambda, s1 = n > 1 ? (R)w.e[0] : (R)0;
+    unsigned long long piv = 0ull;
+
+    for (int k = 0; k < n - 1; k++) {
+        const R sub = w.e[k], nd = (R)w.d[k + 1] - lambda;
+        const R ns = k + 1 < n - 1 ? (R)w.e[k + 1] : (R)0;
+        float4 f;
+
+        if (fabs(dd) >= fabs(sub)) {
+            if (fabs(dd) < tiny)
+                dd = dd < (R)0 ? -tiny : tiny;
+            const R rd = (R)1 / dd, l = sub * rd;
+
+            f = make_float4((float)rd, (float)s1, 0.f, (float)l);
+            dd = nd - l * s1;
+            s1 = ns;
+        }
+        else {
+            const R rs = (R)1 / sub, l = dd * rs;
+
+            piv |= 1ull << k;
+            f = make_float4((float)rs, (float)nd, (float)ns, (float)l);
+            dd = s1 - l * nd;
+            s1 = -l * ns;
+        }
+        if (g.gl == 0)
+            w.lu[k] = f;
+    }
+    if (fabs(dd) < tiny)
+        dd = dd < (R)0 ? -tiny : tiny;
+    if (g.gl == 0)
+        w.lu[n - 1] = make_float4((float)((R)1 / dd), 0.f, 0.f, 0.f);
+    gsync(g);
+    return piv;
+}
+
+/* Solve (tri - lambda) with the LU of tri_lu, in place on yr (every lane,
+   same values). */
+__device__ __forceinline__ void tri_solve(float (&yr)[32], int n, unsigned long long piv,
+                                          const HWs &w)
+{
+#pragma unroll
+    for (int k = 0; k < 31; k++) {
+        if (k >= n - 1)
+            break;
+        if ((piv >> k) & 1ull) {
+            const float t = yr[k];
+
+            yr[k] = yr[k + 1];
+            yr[k + 1] = t;
+        }
+        yr[k + 1] -= w.lu[k].w * yr[k];
+    }
+#pragma unroll
+    for (int k = 31; k >= 0; k--) {
+        if (k > n - 1)
+            continue;
+        const float4 u = w.lu[k];
+        float v = yr[k];
+
+        if (k + 1 < n)
+            v -= u.y * yr[k + 1];
+        if (k + 2 < n)
+            v -= u.z * yr[k + 2];
+        yr[k] = v * u.x;
+    }
+}
+
+/* The eigenvector of rank `index` of the reduced matrix, back-transformed:
+   returns the components of rows i0, i1 in z0, z1; y (tridiagonal vector)
+   is left in yr. */
+__device__ unsigned eigvec(int n, int index, const HWs &w, int ld, const Grp &g, float2 &z0,
+                           float2 &z1, float (&yr)[32], float &lambda, float &norm)
+{
+    unsigned status = 0;
+
+    lambda = tri_eigenvalue(n, index, w, g, norm, status);
+    const float tiny = 1.0e-6f * fmaxf(norm, 1.0e-30f);
+    const unsigned long long piv = tri_lu<float>(n, lambda, tiny, w, g);
+
+#pragma unroll
+    for (int k = 0; k < 32; k++)
+        yr[k] = 1.f;
+    for (int it = 0; it < 3; it++) {
+        tri_solve(yr, n, piv, w);
+        float nrm = 0.f;
+
+#pragma unroll
+        for (int k = 0; k < 32; k++)
+            if (k < n)
+                nrm = fmaxf(nrm, fabsf(yr[k]));
+        const float inv = __frcp_rn(nrm);
+
+#pragma unroll
+        for (int k = 0; k < 32; k++)
+            yr[k] *= inv;
+    }
+    const int i0 = g.gl, i1 = g.gl + 16;
+    float y0 = 0.f, y1 = 0.f;
+
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+        if (k == i0)
+            y0 = yr[k];
+        if (k == i1)
+            y1 = yr[k];
+    }
+    z0 = make_float2(i0 < n ? y0 : 0.f, 0.f);
+    z1 = make_float2(i1 < n ? y1 : 0.f, 0.f);
+    /* z = H_0 .. H_{n-2} y */
+    for (int k = n - 2; k >= 0; k--) {
+        const float2 ta = w.tau[k];
+
+        if (ta.x == 0.f && ta.y == 0.f)
+            continue;
+        const float2 v0 = i0 > k && i0 < n ? w.T[i0 * ld + k] : make_float2(0.f, 0.f);
+        const float2 v1 = i1 > k && i1 < n ? w.T[i1 * ld + k] : make_float2(0.f, 0.f);
+        float sr = v0.x * z0.x + v0.y * z0.y + v1.x * z1.x + v1.y * z1.y;
+        float si = v0.x * z0.y - v0.y * z0.x + v1.x * z1.y - v1.y * z1.x;
+
+        sr = gsum(sr, g);
+        si = gsum(si, g);
+        const float hr = ta.x * sr - ta.y * si, hi = ta.x * si + ta.y * sr;
+
+        z0.x -= v0.x * hr - v0.y * hi;
+        z0.y -= v0.x * hi + v0.y * hr;
+        z1.x -= v1.x * hr - v1.y * hi;
+        z1.y -= v1.x * hi + v1.y * hr;
+    }
+    return status;
+}
+
+/* ------------------------------------------------------------------ */
+/* EMI: |T|^-1 in double.                                              */
+/* ------------------------------------------------------------------ */
+
+/* Gauss-Jordan without pivoting on the group's symmetric matrix (rows
+   i0, i1 in g0, g1; rows and columns >= n zero), in place. False when a
+   pivot is not above `floor`. */
+__device__ bool gj16(double (&g0)[32], double (&g1)[32], int n, double floor, const HWs &w,
+                     const Grp &g)
+{
+    const int i0 = g.gl, i1 = g.gl + 16;
+
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+        if (k >= n)
+            break;
+        const double p = gbcast(k < 16 ? g0[k] : g1[k], k, g);
+
+        if (!(p > floor))
+            return false;
+        const double ip = 1.0 / p;
+
+        if (g.gl == (k & 15)) {
+#pragma unroll
+            for (int j = 0; j < 32; j += 2) {
+                const double a = k < 16 ? g0[j] : g1[j], b = k < 16 ? g0[j + 1] : g1[j + 1];
+
+                *(double2 *)&w.rs[j] = make_double2(a * ip, b * ip);
+            }
+        }
+        gsync(g);
+        const double gk0 = g0[k], gk1 = g1[k];
+        const double f0 = i0 == k ? p - 1.0 : gk0, f1 = i1 == k ? p - 1.0 : gk1;
+
+#pragma unroll
+        for (int j = 0; j < 32; j += 2) {
+            const double2 r2 = *(const double2 *)&w.rs[j];
+
+            if (j != k) {
+                g0[j] = fma(-f0, r2.x, g0[j]);
+                g1[j] = fma(-f1, r2.x, g1[j]);
+            }
+            if (j + 1 != k) {
+                g0[j + 1] = fma(-f0, r2.y, g0[j + 1]);
+                g1[j + 1] = fma(-f1, r2.y, g1[j + 1]);
+            }
+        }
+        g0[k] = i0 == k ? ip : -gk0 * ip;
+        g1[k] = i1 == k ? ip : -gk1 * ip;
+        gsync(g);
+    }
+    return true;
+}
+
+/* (o0, o1) = rows i0, i1 of A times B; A and B n x ld (memory). */
+__device__ void rows_times(const double *A, const double *B, int ld, int n, int i0, int i1,
+                           double (&o0)[32], double (&o1)[32])
+{
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+        o0[j] = 0.0;
+        o1[j] = 0.0;
+    }
+    for (int k = 0; k < n; k++) {
+        const double *row = B + k * ld;
+        const double x0 = i0 < n ? A[i0 * ld + k] : 0.0, x1 = i1 < n ? A[i1 * ld + k] : 0.0;
+
+#pragma unroll
+        for (int j = 0; j < 32; j++)
+            if (j < n) {
+                const double b = row[j];
+
+                o0[j] = fma(x0, b, o0[j]);
+                o1[j] = fma(x1, b, o1[j]);
+            }
+    }
+}
+
+/* Jacobi pseudo-inverse of G (n x ld double, shared) in place, V (n x ld)
+   workspace; eigenvalues |l| < 1e-9 dropped (tests/reference.py:151-156). */
+__device__ unsigned jacobi_pinv16(int n, int ld, double *G, double *V, double *lam,
+                                  const Grp &g)
+{
+    unsigned status = TC_STATUS_ITER_CAP;
+
+    for (int r = g.gl; r < n; r += 16)
+        for (int j = 0; j < n; j++)
+            V[r * ld + j] = r == j ? 1.0 : 0.0;
+    gsync(g);
+    for (int sweep = 0; sweep < 60; sweep++) {
+        double off = 0.0, dg = 0.0;
+
+        for (int r = g.gl; r < n; r += 16)
+            for (int j = 0; j < n; j++) {
+                const double x = G[r * ld + j];
+
+                if (j == r)
+                    dg += x * x;
+                else
+                    off += x * x;
+            }
+        off = gsum(off, g);
+        dg = gsum(dg, g);
+        if (off <= 1.0e-30 * dg) {
+            status = 0;
+            break;
+        }
+        for (int p = 0; p < n - 1; p++)
+            for (int q = p + 1; q < n; q++) {
+                const double apq = G[p * ld + q];
+
+                if (apq == 0.0)
+                    continue;
+                const double app = G[p * ld + p], aqq = G[q * ld + q];
+                const double theta = (aqq - app) / (2.0 * apq);
+                const double t = (theta >= 0.0 ? 1.0 : -1.0) /
+                                 (fabs(theta) + sqrt(theta * theta + 1.0));
+                const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+
+                gsync(g);
+                for (int r = g.gl; r < n; r += 16) {
+                    if (r != p && r != q) {
+                        const double akp = G[r * ld + p], akq = G[r * ld + q];
+
+                        G[r * ld + p] = c * akp - s * akq;
+                        G[r * ld + q] = s * akp + c * akq;
+                    }
+                    const double vkp = V[r * ld + p], vkq = V[r * ld + q];
+
+                    V[r * ld + p] = c * vkp - s * vkq;
+                    V[r * ld + q] = s * vkp + c * vkq;
+                }
+                gsync(g);
+                for (int r = g.gl; r < n; r += 16)
+                    if (r != p && r != q) {
+                        G[p * ld + r] = G[r * ld + p];
+                        G[q * ld + r] = G[r * ld + q];
+                    }
+                if (g.gl == 0) {
+                    G[p * ld + p] = app - t * apq;
+                    G[q * ld + q] = aqq + t * apq;
+                    G[p * ld + q] = 0.0;
+                    G[q * ld + p] = 0.0;
+                }
+                gsync(g);
+            }
+    }
+    for (int r = g.gl; r < n; r += 16)
+        lam[r] = G[r * ld + r];
+    gsync(g);
+    for (int i = g.gl; i < n; i += 16)
+        for (int j = 0; j < n; j++) {
+            double s = 0.0;
+
+            for (int k = 0; k < n; k++) {
+                const double l = lam[k];
+
+                if (fabs(l) >= 1.0e-9)
+                    s += V[i * ld + k] * V[j * ld + k] / l;
+            }
+            G[i * ld + j] = s;
+        }
+    gsync(g);
+    return status;
+}
+
+/* |T|^-1 into G (shared, double), from |T| in G. Returns status bits. */
+__device__ unsigned emi_inverse(int n, int ld, const HWs &w, double *V, const Grp &g)
+{
+    const int i0 = g.gl, i1 = g.gl + 16;
+    double g0[32], g1[32];
+    unsigned st = 0;
+
+#pragma unroll
+    for (int j = 0; j < 32; j++) {
+        g0[j] = (i0 < n && j < n) ? w.G[i0 * ld + j] : 0.0;
+        g1[j] = (i1 < n && j < n) ? w.G[i1 * ld + j] : 0.0;
+    }
+    bool ok = gj16(g0, g1, n, 1.0e-5, w, g);
+
+    if (!ok) {
+        /* |T| not safely positive definite: (|T|^2)^-1 |T|, with the
+           intermediate inverse in V. */
+        st |= TC_STATUS_EMI_PINV;
+        gsync(g);
+        rows_times(w.G, w.G, ld, n, i0, i1, g0, g1);
+        ok = gj16(g0, g1, n, 1.0e-300, w, g);
+        if (ok) {
+#pragma unroll
+            for (int j = 0; j < 32; j++)
+                if (j < n) {
+                    if (i0 < n)
+                        V[i0 * ld + j] = g0[j];
+                    if (i1 < n)
+                        V[i1 * ld + j] = g1[j];
+                }
+            gsync(g);
+            rows_times(V, w.G, ld, n, i0, i1, g0, g1);
+        }
+    }
+    if (ok) {
+        /* every |eigenvalue| of |T| above 1e-9, where the pseudo-inverse of
+           reference.py is the inverse: n max|inv_ij| < 1e8 ensures it. */
+        double mx = 0.0;
+
+#pragma unroll
+        for (int j = 0; j < 32; j++)
+            mx = fmax(mx, fmax(fabs(g0[j]), fabs(g1[j])));
+        mx = gmaxd(mx, g);
+        ok = mx == mx && n * mx < 1.0e8;
+    }
+    gsync(g);
+    if (ok) {
+#pragma unroll
+        for (int j = 0; j < 32; j++)
+            if (j < n) {
+                if (i0 < n)
+                    w.G[i0 * ld + j] = g0[j];
+                if (i1 < n)
+                    w.G[i1 * ld + j] = g1[j];
+            }
+    }
+    else {
+        /* G still holds |T| (only registers were changed). */
+        st |= TC_STATUS_EMI_PINV | jacobi_pinv16(n, ld, w.G, V, w.lam, g);
+    }
+    gsync(g);
+    return st;
+}
+
+/* M_ij = inv_ij T_ij (double) */
+__device__ __forceinline__ double2 mval(const HWs &w, int ld, int i, int j)
+{
+    const double gg = w.G[i * ld + j];
+    const float2 t = w.T[i < j ? i * ld + j : j * ld + i];
+
+    return make_double2(gg * (double)t.x, i < j ? gg * (double)t.y : -gg * (double)t.y);
+}
+
+/* One refinement step of the eigenpair of M for the eigenvector (z0, z1)
+   of rows (i0, i1): see the file comment. tri and Q are the float
+   reduction of M; y is the tridiagonal eigenvector. */
+__device__ void refine(int n, int ld, const HWs &w, const Grp &g, double2 &x0, double2 &x1,
+                       const float (&yr)[32], unsigned long long piv, bool do_solve)
+{
+    const int i0 = g.gl, i1 = g.gl + 16;
+
+    /* normalize, publish x */
+    double nn = x0.x * x0.x + x0.y * x0.y + x1.x * x1.x + x1.y * x1.y;
+
+    nn = gsum(nn, g);
+    const double inrm = 1.0 / sqrt(nn);
+
+    x0.x *= inrm;
+    x0.y *= inrm;
+    x1.x *= inrm;
+    x1.y *= inrm;
+    w.x[i0] = x0;
+    w.x[i1] = x1;
+    gsync(g);
+    /* u = M x (rows i0, i1), mu = x^H u */
+    double2 u0 = make_double2(0.0, 0.0), u1 = u0;
+
+    for (int j = 0; j < n; j++) {
+        const double2 xj = w.x[j];
+
+        if (i0 < n) {
+            const double2 m = mval(w, ld, i0, j);
+
+            u0.x += m.x * xj.x - m.y * xj.y;
+            u0.y += m.x * xj.y + m.y * xj.x;
+        }
+        if (i1 < n) {
+            const double2 m = mval(w, ld, i1, j);
+
+            u1.x += m.x * xj.x - m.y * xj.y;
+            u1.y += m.x * xj.y + m.y * xj.x;
+        }
+    }
+    double mu = x0.x * u0.x + x0.y * u0.y + x1.x * u1.x + x1.y * u1.y;
+
+    mu = gsum(mu, g);
+    if (!do_solve)
+        return;
+    /* r = u - mu x; b = Q^H r = H_{n-2} .. H_0 r */
+    double2 b0 = make_double2(u0.x - mu * x0.x, u0.y - mu * x0.y);
+    double2 b1 = make_double2(u1.x - mu * x1.x, u1.y - mu * x1.y);
+
+    if (i0 >= n)
+        b0 = make_double2(0.0, 0.0);
+    if (i1 >= n)
+        b1 = make_double2(0.0, 0.0);
+    for (int k = 0; k < n - 1; k++) {
+        const float2 ta = w.tau[k];
+
+        if (ta.x == 0.f && ta.y == 0.f)
+            continue;
+        const float2 v0 = i0 > k && i0 < n ? w.T[i0 * ld + k] : make_float2(0.f, 0.f);
+        const float2 v1 = i1 > k && i1 < n ? w.T[i1 * ld + k] : make_float2(0.f, 0.f);
+        double sr = (double)v0.x * b0.x + (double)v0.y * b0.y + (double)v1.x * b1.x +
+                    (double)v1.y * b1.y;
+        double si = (double)v0.x * b0.y - (double)v0.y * b0.x + (double)v1.x * b1.y -
+                    (double)v1.y * b1.x;
+
+        sr = gsum(sr, g);
+        si = gsum(si, g);
+        /* H^H b = b - conj(tau) v (v^H b) */
+        const double hr = (double)ta.x * sr + (double)ta.y * si;
+        const double hi = (double)ta.x * si - (double)ta.y * sr;
+
+        b0.x -= (double)v0.x * hr - (double)v0.y * hi;
+        b0.y -= (double)v0.x * hi + (double)v0.y * hr;
+        b1.x -= (double)v1.x * hr - (double)v1.y * hi;
+        b1.y -= (double)v1.x * hi + (double)v1.y * hr;
+    }
+    /* b is real-tridiagonal space but complex-valued: solve the real and
+       imaginary parts with the float LU of (tri - lambda), off y. */
+    w.x[i0] = b0;
+    w.x[i1] = b1;
+    gsync(g);
+    float tr_[32], ti_[32];
+    double ynrm = 0.0, cr = 0.0, ci = 0.0;
+
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+        const double2 bk = k < n ? w.x[k] : make_double2(0.0, 0.0);
+
+        ynrm += (double)yr[k] * yr[k];
+        cr += (double)yr[k] * bk.x;
+        ci += (double)yr[k] * bk.y;
+        tr_[k] = (float)bk.x;
+        ti_[k] = (float)bk.y;
+    }
+    cr /= ynrm;
+    ci /= ynrm;
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+        tr_[k] -= (float)(cr * yr[k]);
+        ti_[k] -= (float)(ci * yr[k]);
+    }
+    tri_solve(tr_, n, piv, w);
+    tri_solve(ti_, n, piv, w);
+    double dr = 0.0, di = 0.0;
+
+#pragma unroll
+    for (int k = 0; k < 32; k++)
+        if (k < n) {
+            dr += (double)yr[k] * tr_[k];
+            di += (double)yr[k] * ti_[k];
+        }
+    dr /= ynrm;
+    di /= ynrm;
+    double2 t0 = make_double2(0.0, 0.0), t1 = t0;
+
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+        if (k == i0 && k < n)
+            t0 = make_double2(tr_[k] - dr * yr[k], ti_[k] - di * yr[k]);
+        if (k == i1 && k < n)
+            t1 = make_double2(tr_[k] - dr * yr[k], ti_[k] - di * yr[k]);
+    }
+    /* d = Q t = H_0 .. H_{n-2} t; x -= d */
+    for (int k = n - 2; k >= 0; k--) {
+        const float2 ta = w.tau[k];
+
+        if (ta.x == 0.f && ta.y == 0.f)
+            continue;
+        const float2 v0 = i0 > k && i0 < n ? w.T[i0 * ld + k] : make_float2(0.f, 0.f);
+        const float2 v1 = i1 > k && i1 < n ? w.T[i1 * ld + k] : make_float2(0.f, 0.f);
+        double sr = (double)v0.x * t0.x + (double)v0.y * t0.y + (double)v1.x * t1.x +
+                    (double)v1.y * t1.y;
+        double si = (double)v0.x * t0.y - (double)v0.y * t0.x + (double)v1.x * t1.y -
+                    (double)v1.y * t1.x;
+
+        sr = gsum(sr, g);
+        si = gsum(si, g);
+        const double hr = (double)ta.x * sr - (double)ta.y * si;
+        const double hi = (double)ta.x * si + (double)ta.y * sr;
+
+        t0.x -= (double)v0.x * hr - (double)v0.y * hi;
+        t0.y -= (double)v0.x * hi + (double)v0.y * hr;
+        t1.x -= (double)v1.x * hr - (double)v1.y * hi;
+        t1.y -= (double)v1.x * hi + (double)v1.y * hr;
+    }
+    x0.x -= t0.x;
+    x0.y -= t0.y;
+    x1.x -= t1.x;
+    x1.y -= t1.y;
+    gsync(g);
+}
+
+/* ------------------------------------------------------------------ */
+/* Common stages.                                                      */
+/* ------------------------------------------------------------------ */
+
+/* T of the group's pixel from its packed Gram sums (tcoh.cl:611-636);
+   identity for an inactive group. The group's 16 lanes first issue all
+   their loads. */
+__device__ void load_T(const TcStrip &s, const TcChunk &c, const TcLinkConst &k, int p, bool active,
+                       int looks, const float2 *__restrict__ gram,
+                       const unsigned short *__restrict__ upper_tab, const HWs &w, int ld,
+                       const Grp &g)
+{
+    const int n = s.n, npu = tc_npu(n);
+    float2 gv[33];
+
+#pragma unroll
+    for (int t = 0; t < 33; t++) {
+        const int q = g.gl + 16 * t;
+
+        gv[t] = (active && q < npu) ? gram[(long long)q * c.npix + p] : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int t = 0; t < 33; t++) {
+        const int q = g.gl + 16 * t;
+
+        if (q < npu) {
+            const int i = upper_tab[q] >> 8, j = upper_tab[q] & 255;
+
+            if (i == j)
+                w.nrm[i] = __fsqrt_rn(gv[t].x);
+        }
+    }
+    gsync(g);
+    const float fl = (float)looks;
+
+#pragma unroll
+    for (int t = 0; t < 33; t++) {
+        const int q = g.gl + 16 * t;
+
+        if (q >= npu)
+            continue;
+        const int i = upper_tab[q] >> 8, j = upper_tab[q] & 255;
+
+        if (i == j) {
+            w.T[i * ld + i] = make_float2(1.f, 0.f);
+            continue;
+        }
+        float re = 0.f, im = 0.f;
+
+        if (active) {
+            const float2 gq = gv[t];
+            const float dd = __fmul_rn(w.nrm[i], w.nrm[j]);
+
+            if (dd > 0.f) {
+                re = __fdiv_rn(gq.x, dd);
+                im = __fdiv_rn(gq.y, dd);
+                if (k.bias && looks > 1) {
+                    const float m2 = __fadd_rn(__fmul_rn(re, re), __fmul_rn(im, im));
+                    const float m2c =
+                        __fdiv_rn(__fsub_rn(__fmul_rn(fl, m2), 1.0f), __fsub_rn(fl, 1.0f));
+                    const float f =
+                        (m2 > 0.f && m2c > 0.f) ? __fsqrt_rn(__fdiv_rn(m2c, m2)) : 0.f;
+
+                    re = __fmul_rn(re, f);
+                    im = __fmul_rn(im, f);
+                }
+            }
+        }
+        w.T[i * ld + j] = make_float2(re, im);
+        w.T[j * ld + i] = make_float2(re, -im);
+    }
+    gsync(g);
+}
+
+/* Whether the non-zero coherences link all dates (n <= 32). */
+__device__ bool linked16(int n, int ld, const float2 *T, const Grp &g)
+{
+    unsigned adj[2] = {0u, 0u};
+
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+        const int r = g.gl + 16 * t;
+
+        if (r < n)
+            for (int j = 0; j < n; j++) {
+                const float2 v = T[r * ld + j];
+
+                if (j != r && (v.x != 0.f || v.y != 0.f))
+                    adj[t] |= 1u << j;
+            }
+    }
+    const unsigned all = n == 32 ? ~0u : (1u << n) - 1u;
+    unsigned reached = 1u, frontier = 1u;
+
+    for (int it = 0; it < n; it++) {
+        unsigned mine = 0u;
+
+        if ((frontier >> g.gl) & 1u)
+            mine |= adj[0];
+        if (g.gl + 16 < n && ((frontier >> (g.gl + 16)) & 1u))
+            mine |= adj[1];
+#pragma unroll
+        for (int o = 8; o; o >>= 1)
+            mine |= __shfl_xor_sync(g.mask, mine, o);
+        const unsigned nw = mine & ~reached;
+
+        if (!nw)
+            break;
+        reached |= nw;
+        frontier = nw;
+    }
+    return reached == all;
+}
+
+/* Unit phasors relative to the median date (tcoh.cl:700-724) into w.zs,
+   then the goodness of fit (tcoh.cl:728-744), pairs spread evenly over the
+   lanes. */
+__device__ float gamma16(int n, int ld, const HWs &w, const Grp &g, double2 z0, double2 z1,
+                         const unsigned short *__restrict__ upper_tab)
+{
+    const int i0 = g.gl, i1 = g.gl + 16;
+    const double m0 = i0 < n ? hypot(z0.x, z0.y) : 0.0, m1 = i1 < n ? hypot(z1.x, z1.y) : 0.0;
+    const double mx = gmaxd(fmax(m0, m1), g);
+    int ref = n / 2;
+    const double mref = gbcast(ref < 16 ? m0 : m1, ref, g);
+
+    if (mref <= 1.0e-3 * mx) {
+        int last = -1;
+
+        if (i0 < n && m0 == mx)
+            last = i0;
+        if (i1 < n && m1 == mx)
+            last = i1;
+#pragma unroll
+        for (int o = 8; o; o >>= 1)
+            last = max(last, __shfl_xor_sync(g.mask, last, o));
+        ref = last;
+    }
+    const double zrx = gbcast(ref < 16 ? z0.x : z1.x, ref, g);
+    const double zry = gbcast(ref < 16 ? z0.y : z1.y, ref, g);
+    const double refm = hypot(zrx, zry);
+    const double refr = zrx / refm, refi = -zry / refm;
+    const double floor_ = mx * 1.0e-3;
+
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+        const int r = t ? i1 : i0;
+        const double2 z = t ? z1 : z0;
+
+        if (r < n) {
+            const double re = z.x * refr - z.y * refi, im = z.x * refi + z.y * refr;
+            const double mm = hypot(re, im);
+
+            w.zs[r] = mm > floor_ ? make_float2((float)(re / mm), (float)(im / mm))
+                                  : make_float2(1.f, 0.f);
+        }
+    }
+    gsync(g);
+    float sr = 0.f, si = 0.f;
+    const int npu = tc_npu(n);
+
+    for (int q = g.gl; q < npu; q += 16) {
+        const int i = upper_tab[q] >> 8, j = upper_tab[q] & 255;
+
+        if (i == j)
+            continue;
+        const float2 tv = w.T[i * ld + j];
+        const float m2 = tv.x * tv.x + tv.y * tv.y;
+        float ur = 1.f, ui = 0.f;
+
+        if (m2 > 0.f) {
+            const float r = rsqrtf(m2);
+
+            ur = tv.x * r;
+            ui = tv.y * r;
+        }
+        const float2 zi = w.zs[i], zj = w.zs[j];
+        const float wr = zi.x * zj.x + zi.y * zj.y;
+        const float wi = zi.x * zj.y - zi.y * zj.x;
+
+        sr += ur * wr - ui * wi;
+        si += ur * wi + ui * wr;
+    }
+    sr = gsum(sr, g);
+    si = gsum(si, g);
+    return hypotf(sr, si) / (0.5f * n * (n - 1));
+}
+
+template <bool EMI>
+__global__ void __launch_bounds__(EMI ? 256 : 384)
+tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
+                    const float2 *__restrict__ gram, const int *__restrict__ count,
+                    const unsigned short *__restrict__ upper_tab,
+                    const unsigned short *__restrict__ pair_tab, double *__restrict__ scratch,
+                    float *__restrict__ coh, float *__restrict__ pairs,
+                    float *__restrict__ phases, unsigned char *__restrict__ status)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wpb = blockDim.x >> 5;
+    const Grp g = make_grp(lane);
+    const int grp = warp * 2 + (lane >> 4);
+    const HWs w = hws(smem + (size_t)grp * L.per_group, L);
+    const int n = s.n, ld = L.ld;
+    const long long plane = (long long)s.rows * s.cols;
+    double *V = scratch + ((size_t)blockIdx.x * wpb * 2 + grp) * (size_t)n * ld;
+    const int i0 = g.gl, i1 = g.gl + 16;
+
+    for (int q = blockIdx.x * wpb + warp; 2 * q < c.npix; q += gridDim.x * wpb) {
+        const int p = 2 * q + (lane >> 4);
+        int y, x;
+
+        tc_pixel_yx(c, p, y, x);
+        const bool inrange = p < c.npix && y < c.row0 + c.nrows && y < s.rows && x < s.cols;
+        const long long out = inrange ? (long long)y * s.cols + x : 0;
+        const int looks = inrange ? count[out] : -1;
+        bool active = inrange && looks >= k.min_looks;
+
+        if (inrange && !active) {
+            if (g.gl == 0)
+                coh[out] = NAN;
+            for (int t = g.gl; t < k.npairs; t += 16)
+                pairs[t * plane + out] = NAN;
+            if (phases)
+                for (int r = g.gl; r < n; r += 16)
+                    phases[out * n + r] = NAN;
+            if (status && g.gl == 0)
+                status[out] = 0;
+        }
+        if (!__any_sync(FULL, active))
+            continue;
+        load_T(s, c, k, p, active, looks, gram, upper_tab, w, ld, g);
+        if (active)
+            for (int t = g.gl; t < k.npairs; t += 16) {
+                const int i = pair_tab[t] >> 8, j = pair_tab[t] & 255;
+                const float2 tv = w.T[i * ld + j];
+
+                pairs[t * plane + out] = hypotf(tv.x, tv.y);
+            }
+        unsigned st = 0;
+
+        if (k.bias && active && !linked16(n, ld, w.T, g)) {
+            if (g.gl == 0)
+                coh[out] = NAN;
+            if (phases)
+                for (int r = g.gl; r < n; r += 16)
+                    phases[out * n + r] = NAN;
+            if (status && g.gl == 0)
+                status[out] = TC_STATUS_UNLINKED;
+            active = false;
+        }
+        gsync(g);
+        if (!active) {
+            /* a well-conditioned stand-in keeps the group in step */
+            for (int r = g.gl; r < n; r += 16)
+                for (int j = 0; j < n; j++)
+                    w.T[r * ld + j] = make_float2(r == j ? 1.f : 0.f, 0.f);
+            gsync(g);
+        }
+        if (!__any_sync(FULL, active))
+            continue;
+
+        float2 r0[32], r1[32];
+        double2 z0, z1;
+
+        if (!EMI) {
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+                r0[j] = (i0 < n && j < n) ? w.T[i0 * ld + j] : make_float2(0.f, 0.f);
+                r1[j] = (i1 < n && j < n) ? w.T[i1 * ld + j] : make_float2(0.f, 0.f);
+            }
+            gsync(g);
+            householder(r0, r1, n, w, ld, g);
+            float yr[32], lambda, norm;
+            float2 f0, f1;
+
+            st |= eigvec(n, n - 1, w, ld, g, f0, f1, yr, lambda, norm);
+            z0 = make_double2(f0.x, f0.y);
+            z1 = make_double2(f1.x, f1.y);
+        }
+        else {
+            for (int r = g.gl; r < n; r += 16)
+                for (int j = 0; j < n; j++) {
+                    const float2 t = w.T[r * ld + j];
+
+                    w.G[r * ld + j] = hypot((double)t.x, (double)t.y);
+                }
+            gsync(g);
+            st |= emi_inverse(n, ld, w, V, g);
+            /* M = |T|^-1 o T in float rows */
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+                r0[j] = make_float2(0.f, 0.f);
+                r1[j] = make_float2(0.f, 0.f);
+                if (j < n) {
+                    if (i0 < n) {
+                        const double2 m = mval(w, ld, i0, j);
+
+                        r0[j] = make_float2((float)m.x, (float)m.y);
+                    }
+                    if (i1 < n) {
+                        const double2 m = mval(w, ld, i1, j);
+
+                        r1[j] = make_float2((float)m.x, (float)m.y);
+                    }
+                }
+            }
+            gsync(g);
+            /* The reduction parks its vectors in T's lower triangle, which
+               mval no longer reads (it takes T_ij from i < j). */
+            householder(r0, r1, n, w, ld, g);
+            float yr[32], lambda, norm;
+            float2 f0, f1;
+
+            st |= eigvec(n, 0, w, ld, g, f0, f1, yr, lambda, norm);
+            const unsigned long long piv =
+                tri_lu<float>(n, lambda, 1.0e-6f * fmaxf(norm, 1.0e-30f), w, g);
+
+            z0 = make_double2(f0.x, f0.y);
+            z1 = make_double2(f1.x, f1.y);
+            refine(n, ld, w, g, z0, z1, yr, piv, true);
+            refine(n, ld, w, g, z0, z1, yr, piv, true);
+        }
+        const float gamma = gamma16(n, ld, w, g, z0, z1, upper_tab);
+
+        if (active) {
+            if (g.gl == 0)
+                coh[out] = gamma;
+            if (phases)
+#pragma unroll
+                for (int t = 0; t < 2; t++) {
+                    const int r = t ? i1 : i0;
+
+                    if (r < n) {
+                        const float2 u = w.zs[r];
+
+                        phases[out * n + r] = atan2f(u.y, u.x);
+                    }
+                }
+            if (status && g.gl == 0)
+                status[out] = (unsigned char)st;
+        }
+        __syncwarp();
+    }
+}
+
+HalfLayout half_layout(int n, int emi)
+{
+    HalfLayout L;
+    int off = 0;
+    auto take = [&](int bytes) {
+        const int o = off;
+
+        off += (bytes + 15) & ~15;
+        return o;
+    };
+
+    L.n = n;
+    L.ld = n | 1;
+    L.off_T = take(8 * n * L.ld);
+    L.off_G = take(emi ? 8 * n * L.ld : 0);
+    L.off_vw = take(16 * 32);
+    L.off_lu = take(16 * 32);
+    L.off_tau = take(8 * 32);
+    L.off_d = take(4 * 32);
+    L.off_e = take(4 * 32);
+    L.off_df = take(4 * 32);
+    L.off_e2f = take(4 * 32);
+    L.off_y = take(4 * 32);
+    L.off_nrm = take(4 * 32);
+    L.off_zs = take(8 * 32);
+    L.off_rs = take(emi ? 8 * 32 : 0);
+    L.off_lam = take(emi ? 8 * 32 : 0);
+    L.off_x = take(emi ? 16 * 32 : 0);
+    L.per_group = off;
+    return L;
+}
+
+} // namespace
+
+size_t tc_link_half_scratch_bytes(int n, int sms)
+{
+    /* Per group (two per warp, at most 12 warps per CTA, one CTA per SM):
+       the Jacobi eigenvectors of |T|. */
+    return (size_t)sms * 24 * n * (n | 1) * sizeof(double);
+}
+
+cudaError_t tc_launch_link_half(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
+                                const float2 *gram, const int *count,
+                                const unsigned short *upper_tab, const unsigned short *pair_tab,
+                                double *scratch, float *coh, float *pairs, float *phases,
+                                unsigned char *status, int sms, cudaStream_t st)
+{
+    const HalfLayout L = half_layout(s.n, k.emi);
+    const size_t per_warp = 2 * (size_t)L.per_group;
+    const int max_warps = k.emi ? 8 : 12;
+    int wpb = (int)((200 * 1024) / per_warp);
+
+    if (wpb > max_warps)
+        wpb = max_warps;
+    if (wpb < 1)
+        return cudaErrorInvalidConfiguration;
+    const size_t smem = per_warp * wpb;
+    const int want = (c.npix / 2 + wpb - 1) / wpb;
+    const int blocks = want < sms ? want : sms;
+    cudaError_t e;
+
+    if (k.emi) {
+        e = cudaFuncSetAttribute(tc_link_half_kernel<true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess)
+            tc_link_half_kernel<true><<<blocks, wpb * 32, smem, st>>>(
+                s, c, k, L, gram, count, upper_tab, pair_tab, scratch, coh, pairs, phases, status);
+    }
+    else {
+        e = cudaFuncSetAttribute(tc_link_half_kernel<false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess)
+            tc_link_half_kernel<false><<<blocks, wpb * 32, smem, st>>>(
+                s, c, k, L, gram, count, upper_tab, pair_tab, scratch, coh, pairs, phases, status);
+    }
+    if (e != cudaSuccess)
+        return e;
+    return cudaGetLastError();
+}

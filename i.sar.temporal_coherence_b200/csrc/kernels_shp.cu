@@ -1,0 +1,265 @@
+/* Strip preparation and statistically homogeneous pixel (SHP) selection.
+ *
+ * The SHP tests reproduce the reference kernel's decisions exactly:
+ *   KS   (tcoh.cl:34-54)  depends only on comparisons of the sorted float
+ *                         amplitudes and the integer KS_MAX;
+ *   AD   (tcoh.cl:56-75)  the float rank statistic, accumulated in the same
+ *                         order, each term fl(num^2 / den) taken from a
+ *                         table of the correctly rounded quotients, and the
+ *                         standardization done with round-to-nearest
+ *                         intrinsics (no contraction);
+ *   tlog (tcoh.cl:77-95)  the float log mean / variance of every pixel,
+ *                         computed once per pixel in the kernel's order
+ *                         (the reference recomputes them per candidate, with
+ *                         identical results), with logs rounded from double
+ *                         so that they are the correctly rounded values.
+ *
+ * Layout of the mask: uint32 [mask_words][npix] per chunk, bit b of word w
+ * set when candidate c = 32 w + b (c = dy * WR + dx of the window) is an SHP.
+ */
+#include "tcoh_internal.h"
+
+#include <math.h>
+
+/* AoS [npad][N] float2 -> SoA [planes][npad] float2, zero planes >= N. */
+__global__ void tc_prep_kernel(TcStrip s, const float2 *__restrict__ aos,
+                               float2 *__restrict__ soa)
+{
+    const long long total = (long long)s.planes * s.npad;
+
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int d = (int)(i / s.npad);
+        const long long p = i - (long long)d * s.npad;
+
+        soa[i] = d < s.n ? aos[p * s.n + d] : make_float2(0.f, 0.f);
+    }
+}
+
+/* Log mean and variance of every valid pixel's amplitudes, in the float
+   order of tcoh.cl:82-90 / 556-564. */
+__global__ void tc_logstats_kernel(TcStrip s, const float *__restrict__ amp,
+                                   const unsigned char *__restrict__ valid,
+                                   float2 *__restrict__ out)
+{
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < s.npad;
+         p += (long long)gridDim.x * blockDim.x) {
+        const float *a = amp + p * s.n;
+        float m = 0.f, v = 0.f;
+
+        if (!valid[p]) {
+            out[p] = make_float2(0.f, 0.f);
+            continue;
+        }
+        for (int k = 0; k < s.n; k++)
+            m = __fadd_rn(m, (float)log((double)a[k]));
+        m = __fdiv_rn(m, (float)s.n);
+        for (int k = 0; k < s.n; k++) {
+            const float d = __fsub_rn((float)log((double)a[k]), m);
+
+            v = __fadd_rn(v, __fmul_rn(d, d));
+        }
+        v = __fdiv_rn(v, (float)(s.n - 1));
+        out[p] = make_float2(m, v);
+    }
+}
+
+/* One warp per output pixel; in each round the 32 lanes test 32 window
+   candidates against the centre. The centre's sorted amplitudes sit in
+   shared memory (every lane reads the same array, so any set of indices is
+   conflict-free for N <= 32); each lane's candidate series is transposed
+   into a per-warp column buffer b[j][lane], also conflict-free. */
+template <int TEST>
+__global__ void __launch_bounds__(256)
+tc_shp_kernel(TcStrip s, TcChunk c, TcShpConst k, const float *__restrict__ amp,
+              const unsigned char *__restrict__ valid, const float2 *__restrict__ logstat,
+              uint32_t *__restrict__ mask, int *__restrict__ count)
+{
+    extern __shared__ float sm[];
+    const int n = s.n;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wpb = blockDim.x >> 5;
+    const int tab_len = TEST == 1 ? (n + 1) * (2 * n - 1) : 0;
+    float *tab = sm;
+    float *wbuf = sm + tab_len + warp * ((n + 1) + (n + 1) * 32);
+    float *a_s = wbuf;          /* n + 1 */
+    float *b_s = wbuf + n + 1;  /* (n + 1) x 32 */
+
+    if (TEST == 1) {
+        /* fl((2Nm - jN)^2 / (j (2N - j))), j = 1 .. 2N-1, m = 0 .. N. */
+        for (int i = threadIdx.x; i < tab_len; i += blockDim.x) {
+            const int m = i % (n + 1), j = i / (n + 1) + 1;
+            const float num = (float)(2 * n * m - j * n);
+
+            tab[i] = __fdiv_rn(__fmul_rn(num, num), (float)(j * (2 * n - j)));
+        }
+        __syncthreads();
+    }
+
+    for (int p = blockIdx.x * wpb + warp; p < c.npix; p += gridDim.x * wpb) {
+        int y, x;
+
+        tc_pixel_yx(c, p, y, x);
+        if (y >= c.row0 + c.nrows || y >= s.rows || x >= s.cols)
+            continue;
+        const long long centre = (long long)(y + s.wa / 2) * s.W + x + s.wr / 2;
+        const long long out = (long long)y * s.cols + x;
+
+        if (!valid[centre]) {
+            for (int w = lane; w < s.mask_words; w += 32)
+                mask[(long long)w * c.npix + p] = 0u;
+            if (lane == 0)
+                count[out] = -1;
+            continue;
+        }
+        float mean_a = 0.f, var_a = 0.f;
+
+        if (TEST == 2) {
+            const float2 st = logstat[centre];
+
+            mean_a = st.x;
+            var_a = st.y;
+        }
+        else {
+            for (int j = lane; j < n; j += 32)
+                a_s[j] = amp[centre * n + j];
+            if (lane == 0)
+                a_s[n] = INFINITY;
+        }
+        __syncwarp();
+
+        int looks = 0;
+
+        for (int w = 0; w < s.mask_words; w++) {
+            const int cand = w * 32 + lane;
+            bool ok = false;
+
+            if (cand < s.area) {
+                const int dy = cand / s.wr, dx = cand - dy * s.wr;
+                const long long q = (long long)(y + dy) * s.W + x + dx;
+
+                if (valid[q]) {
+                    if (TEST == 2) {
+                        /* tcoh.cl:91-94 */
+                        const float2 st = logstat[q];
+                        const float se = __fsqrt_rn(
+                            __fdiv_rn(__fadd_rn(var_a, st.y), (float)n));
+
+                        ok = !(se > 0.f) ||
+                             __fdiv_rn(fabsf(__fsub_rn(mean_a, st.x)), se) <= k.tlog_crit;
+                    }
+                    else {
+                        const float *b = amp + q * n;
+
+                        for (int j = 0; j < n; j++)
+                            b_s[j * 32 + lane] = b[j];
+                        b_s[n * 32 + lane] = INFINITY;
+                        /* Merge walk, centre first on ties: 2N - 1 steps,
+                           branch-free; a side that ran out is never taken. */
+                        int ia = 0, ib = 0;
+
+                        if (TEST == 0) {
+                            int d = 0;
+
+                            for (int st = 0; st < 2 * n - 1; st++) {
+                                const bool take_a =
+                                    ia < n && (ib >= n || a_s[ia] <= b_s[ib * 32 + lane]);
+
+                                ia += take_a;
+                                ib += !take_a;
+                                d = max(d, abs(ia - ib));
+                            }
+                            ok = d <= k.ks_max;
+                        }
+                        else {
+                            float acc = 0.f;
+
+                            for (int j = 1; j < 2 * n; j++) {
+                                const bool take_a =
+                                    ia < n && (ib >= n || a_s[ia] <= b_s[ib * 32 + lane]);
+
+                                ia += take_a;
+                                ib += !take_a;
+                                acc = __fadd_rn(acc, tab[(j - 1) * (n + 1) + ia]);
+                            }
+                            ok = __fdiv_rn(__fsub_rn(__fmul_rn(k.ad_norm, acc), 1.0f),
+                                           k.ad_sigma) <= k.ad_crit;
+                        }
+                    }
+                }
+            }
+            const uint32_t bits = __ballot_sync(0xffffffffu, ok);
+
+            if (lane == 0)
+                mask[(long long)w * c.npix + p] = bits;
+            looks += __popc(bits);
+        }
+        if (lane == 0)
+            count[out] = looks;
+        __syncwarp();
+    }
+}
+
+cudaError_t tc_launch_prep(const TcStrip &s, const float *slc_aos, float2 *soa,
+                           cudaStream_t st)
+{
+    const long long total = (long long)s.planes * s.npad;
+    const int threads = 256;
+    const long long blocks = (total + threads - 1) / threads;
+
+    tc_prep_kernel<<<(unsigned)(blocks < 148 * 64 ? blocks : 148 * 64), threads, 0, st>>>(
+        s, (const float2 *)slc_aos, soa);
+    return cudaGetLastError();
+}
+
+cudaError_t tc_launch_logstats(const TcStrip &s, const float *amp,
+                               const unsigned char *valid, float2 *logstat,
+                               cudaStream_t st)
+{
+    const int threads = 256;
+    const long long blocks = (s.npad + threads - 1) / threads;
+
+    tc_logstats_kernel<<<(unsigned)(blocks < 148 * 32 ? blocks : 148 * 32), threads, 0, st>>>(
+        s, amp, valid, logstat);
+    return cudaGetLastError();
+}
+
+cudaError_t tc_launch_shp(const TcStrip &s, const TcChunk &c, const TcShpConst &k,
+                          const float *amp, const unsigned char *valid,
+                          const float2 *logstat, uint32_t *mask, int *count, int sms,
+                          cudaStream_t st)
+{
+    const int threads = 256, wpb = threads / 32;
+    const int tab = k.test == 1 ? (s.n + 1) * (2 * s.n - 1) : 0;
+    const size_t smem = sizeof(float) * (tab + wpb * ((s.n + 1) + (s.n + 1) * 32));
+    const int want = (c.npix + wpb - 1) / wpb;
+    const int blocks = want < sms * 8 ? want : sms * 8;
+    cudaError_t e;
+
+    switch (k.test) {
+    case 0:
+        e = cudaFuncSetAttribute(tc_shp_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        if (e == cudaSuccess)
+            tc_shp_kernel<0><<<blocks, threads, smem, st>>>(s, c, k, amp, valid, logstat, mask,
+                                                            count);
+        break;
+    case 1:
+        e = cudaFuncSetAttribute(tc_shp_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        if (e == cudaSuccess)
+            tc_shp_kernel<1><<<blocks, threads, smem, st>>>(s, c, k, amp, valid, logstat, mask,
+                                                            count);
+        break;
+    default:
+        e = cudaFuncSetAttribute(tc_shp_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        if (e == cudaSuccess)
+            tc_shp_kernel<2><<<blocks, threads, smem, st>>>(s, c, k, amp, valid, logstat, mask,
+                                                            count);
+        break;
+    }
+    if (e != cudaSuccess)
+        return e;
+    return cudaGetLastError();
+}

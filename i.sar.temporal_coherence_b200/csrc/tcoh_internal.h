@@ -1,0 +1,101 @@
+/* Internal definitions shared by the kernels and the C-ABI layer. */
+#ifndef TCOH_INTERNAL_H
+#define TCOH_INTERNAL_H
+
+#include <cuda_runtime.h>
+
+#include "../../include/tcoh_b200.h"
+#include <stdint.h>
+
+#define TC_MAX_DATES 64
+#define TC_MAX_MASK_WORDS 32 /* SHP windows of up to 1024 candidates */
+
+/* Output pixels are processed in tiles of 16 rows x 8 columns (128 pixels,
+   the M extent of one tensor-core accumulator tile). Within a chunk, pixel
+   p belongs to tile p / 128, row (p % 128) / 8, column p % 8 of the tile;
+   tiles run row-major over the chunk. */
+#define TC_TILE_H 16
+#define TC_TILE_W 8
+#define TC_TILE_PIX (TC_TILE_H * TC_TILE_W)
+
+/* Per-strip constants. */
+struct TcStrip {
+    int n;           /* dates */
+    int wa, wr;      /* window lines, samples */
+    int area;        /* wa * wr candidates */
+    int mask_words;  /* ceil(area / 32) */
+    int W;           /* padded columns */
+    int padded_rows;
+    int rows, cols;  /* output size */
+    long long npad;  /* padded pixels */
+    int planes;      /* SoA date planes (n rounded up to the Gram block) */
+};
+
+/* One chunk: output rows row0 .. row0 + nrows - 1, all columns. */
+struct TcChunk {
+    int row0, nrows;
+    int tiles_x, tiles_y;
+    int npix; /* tiles_x * tiles_y * 128 */
+};
+
+/* Decision constants of the SHP tests, as the float values the reference
+   kernel is built with (ocl.c:222-229). */
+struct TcShpConst {
+    int test, ks_max;
+    float ad_norm, ad_sigma, ad_crit, tlog_crit;
+};
+
+struct TcLinkConst {
+    int emi, bias, min_looks;
+    int npairs, pairs_all;
+};
+
+__host__ __device__ inline int tc_npu(int n) { return n * (n + 1) / 2; }
+
+/* Packed upper-triangle index of (i, j), i <= j. */
+__host__ __device__ inline int tc_pidx(int n, int i, int j)
+{
+    return i * (2 * n - i + 1) / 2 + (j - i);
+}
+
+__host__ __device__ inline void tc_pixel_yx(const TcChunk &c, int p, int &y, int &x)
+{
+    const int t = p >> 7, w = p & 127;
+    const int ty = t / c.tiles_x, tx = t - ty * c.tiles_x;
+
+    y = c.row0 + ty * TC_TILE_H + (w >> 3);
+    x = tx * TC_TILE_W + (w & 7);
+}
+
+/* Kernel launchers (kernels_*.cu); all asynchronous on `st`. */
+cudaError_t tc_launch_prep(const TcStrip &s, const float *slc_aos, float2 *soa,
+                           cudaStream_t st);
+cudaError_t tc_launch_logstats(const TcStrip &s, const float *amp,
+                               const unsigned char *valid, float2 *logstat,
+                               cudaStream_t st);
+cudaError_t tc_launch_shp(const TcStrip &s, const TcChunk &c, const TcShpConst &k,
+                          const float *amp, const unsigned char *valid,
+                          const float2 *logstat, uint32_t *mask, int *count,
+                          int sms, cudaStream_t st);
+cudaError_t tc_launch_gram_fp32(const TcStrip &s, const TcChunk &c, int block,
+                                const float2 *soa, const uint32_t *mask,
+                                float2 *gram, cudaStream_t st);
+cudaError_t tc_launch_gram_tensor(const TcStrip &s, const TcChunk &c, int split_terms,
+                                  const float *slc_aos, const uint32_t *mask,
+                                  float2 *gram, cudaStream_t st);
+bool tc_gram_tensor_supported(const TcStrip &s);
+int tc_gram_block_for(int n);
+cudaError_t tc_launch_link(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
+                           const float2 *gram, const int *count,
+                           const unsigned short *upper_tab, const unsigned short *pair_tab,
+                           double *scratch, float *coh, float *pairs, float *phases,
+                           unsigned char *status, int sms, cudaStream_t st);
+size_t tc_link_scratch_bytes(int n, int sms);
+cudaError_t tc_launch_link_half(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
+                                const float2 *gram, const int *count,
+                                const unsigned short *upper_tab, const unsigned short *pair_tab,
+                                double *scratch, float *coh, float *pairs, float *phases,
+                                unsigned char *status, int sms, cudaStream_t st);
+size_t tc_link_half_scratch_bytes(int n, int sms);
+
+#endif

@@ -1,0 +1,167 @@
+/* B200 (sm_100a) backend of the GRASS module i.sar.temporal_coherence.
+ *
+ * A drop-in replacement for the module's OpenCL backend ocl.c: the four
+ * ocl_* entry points below have the exact prototypes of local_proto.h:104-112
+ * and the behaviour of ocl.c (synchronous ocl_run over one padded strip,
+ * fatal errors through G_fatal_error), so that main.c links against
+ * libtcoh_b200.so instead of ocl.c unchanged. The tc_* entry points extend
+ * it: return codes instead of fatal errors, device-resident strips, per-date
+ * phase output, the choice of Gram arithmetic, stage timings and the
+ * flat-earth / topographic geometry on the GPU.
+ *
+ * Strip layouts (row-major over the padded strip, main.c:28-34, 52-127):
+ *   slc   float [padded_rows][padded_cols][N][2]  re, im, phase removed
+ *   amp   float [padded_rows][padded_cols][N]     amplitudes, ascending
+ *   valid uchar [padded_rows][padded_cols]        every date non-null, != 0
+ * with padded_rows = rows + WA - 1 and padded_cols = cols + WR - 1. Outputs:
+ *   coh   float [rows][cols]          temporal coherence, NaN = NULL
+ *   count int   [rows][cols]          SHP count, -1 = NULL
+ *   pairs float [npairs][rows][cols]  |T_ij|, NaN = NULL
+ *   phases float [rows][cols][N]      phase-linked phases (radians, relative
+ *                                      to the reference date), NaN = NULL
+ */
+#ifndef TCOH_B200_H
+#define TCOH_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#ifndef I_SAR_TEMPORAL_COHERENCE_LOCAL_PROTO_H
+/* Same layout as local_proto.h:12 and 34-49, which main.c passes in. */
+enum shp_test { SHP_KS = 0, SHP_AD = 1, SHP_TLOG = 2 };
+
+struct settings {
+    int ndates;
+    int win_az, win_rg;
+    enum shp_test test;
+    double alpha;
+    int emi;
+    int bias;
+    int min_looks;
+    int ks_max;
+    double ad_norm, ad_sigma, ad_crit;
+    double tlog_crit;
+    int npairs;    /* pair coherence maps to write, 0 for none */
+    int pairs_all; /* all pairs i < j instead of consecutive ones */
+    const char *phase_reference; /* none, ellipsoid or elevation */
+    const char *orbit;           /* orbit source, NULL without phase */
+};
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Drop-in for ocl.c (local_proto.h:104-112).                          */
+/* ------------------------------------------------------------------ */
+
+struct ocl;
+
+/* Replaces ocl.c:105-136: prints platform|device|type|name|version|
+   compute_units|global_memory_mb, one line per CUDA device. */
+void ocl_list_devices(void);
+
+/* Replaces ocl.c:191-254. platform -1 or 0 (the CUDA platform), device -1
+   for the first GPU. *max_alloc receives the largest strip buffer the
+   backend accepts, which main.c:731-742 uses to size the strips. */
+struct ocl *ocl_open(int platform, int device, const struct settings *s,
+                     int padded_cols, size_t *max_alloc);
+
+/* Replaces ocl.c:279-375: copies one padded strip to the GPU, computes
+   every output pixel and copies the outputs back before returning. pairs
+   may be NULL when s->npairs is 0. */
+void ocl_run(struct ocl *o, const float *slc, const float *amp,
+             const unsigned char *valid, int padded_rows, int rows, int cols,
+             float *coh, int *count, float *pairs);
+
+/* Replaces ocl.c:377-391. */
+void ocl_close(struct ocl *o);
+
+/* ------------------------------------------------------------------ */
+/* Extensions.                                                         */
+/* ------------------------------------------------------------------ */
+
+/* Return codes of the tc_* functions. */
+#define TC_OK           0
+#define TC_ERR_ARG      1 /* invalid argument or shape */
+#define TC_ERR_CUDA     2 /* CUDA runtime error, see tc_last_error() */
+#define TC_ERR_MEMORY   3 /* device allocation failed */
+#define TC_ERR_DEVICE   4 /* no such device, or not an sm_100 GPU */
+
+/* Arithmetic of the masked coherence-matrix accumulation. */
+#define TC_GRAM_TENSOR 0 /* tcgen05 tensor cores, split BF16 terms, FP32 sums */
+#define TC_GRAM_FP32   1 /* plain FP32 FMA on the CUDA cores */
+
+struct tc_options {
+    int gram;         /* TC_GRAM_TENSOR or TC_GRAM_FP32; -1 for the default
+                         (the tensor cores where available) */
+    int split_terms;  /* BF16 terms per FP32 product for TC_GRAM_TENSOR:
+                         2 (16 significant bits) or 3 (24, FP32-exact) */
+    int chunk_pixels; /* output pixels per internal launch, 0 = automatic */
+};
+
+/* Status bits per pixel (tc_run_ex). */
+#define TC_STATUS_EMI_PINV   1 /* EMI: |T| not safely positive definite,
+                                  inverted by its eigen-pseudo-inverse */
+#define TC_STATUS_UNLINKED   2 /* bias correction unlinked the dates */
+#define TC_STATUS_ITER_CAP   4 /* an iterative solver reached its cap */
+
+/* Message of the last failed tc_* call of this thread. */
+const char *tc_last_error(void);
+
+/* Handler the ocl_* entry points call on a fatal error (ocl.c:44-48). By
+   default G_fatal_error when the host program provides it, else the
+   message is printed to stderr and the process exits with failure. The
+   handler must not return. */
+void tc_set_fatal_handler(void (*handler)(const char *message));
+
+/* The SHP test constants of stats.c:61-95 (ks_max, ad_norm, ad_sigma,
+   ad_crit, tlog_crit) for s->ndates, s->test and s->alpha, for hosts that
+   do not link stats.c. TC_ERR_ARG when alpha is outside the AD table. */
+int tc_shp_constants(struct settings *s);
+
+/* Number of CUDA devices. */
+int tc_device_count(void);
+
+/* Open a context on CUDA device `device` (-1: the first one) for strips of
+   padded_cols columns. opt may be NULL for the defaults. */
+int tc_open(int device, const struct settings *s, int padded_cols,
+            const struct tc_options *opt, struct ocl **out,
+            size_t *max_alloc);
+
+/* ocl_run with a return code and optional extra outputs: phases
+   float [rows][cols][N] and status unsigned char [rows][cols] (either may
+   be NULL). Host buffers. */
+int tc_run_ex(struct ocl *o, const float *slc, const float *amp,
+              const unsigned char *valid, int padded_rows, int rows, int cols,
+              float *coh, int *count, float *pairs, float *phases,
+              unsigned char *status);
+
+/* The same on device buffers, asynchronously on `stream` (a cudaStream_t;
+   NULL is CUDA's default stream). Every pointer is a device address. */
+int tc_run_device(struct ocl *o, const float *slc, const float *amp,
+                  const unsigned char *valid, int padded_rows, int rows,
+                  int cols, float *coh, int *count, float *pairs,
+                  float *phases, unsigned char *status, void *stream);
+
+/* Stage timing. With timing on, every launch of the following runs is
+   bracketed by CUDA events on its stream, and tc_stage_stats gives, per
+   stage, the device milliseconds summed over the last run and the number
+   of kernel launches: [0] strip preparation, [1] SHP selection,
+   [2] coherence matrices, [3] phase linking and coherence, [4] host<->device
+   copies (ms only). Returns the number of stages written (at most n). */
+int tc_set_timing(struct ocl *o, int on);
+int tc_stage_stats(const struct ocl *o, float *ms, int *launches, int n);
+
+/* Close the context and free its device memory. */
+int tc_close(struct ocl *o);
+
+/* Measured FP32 FMA throughput of device `device` in TFLOP/s (two flops per
+   FMA), the roofline denominator of the kernels on the CUDA cores. */
+int tc_fp32_peak(int device, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,98 @@
+"""The oracle against the reference: golden vectors from tests/reference.py
+(the reference's FP64 oracle) and the reference kernel compiled as C."""
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import GOLDEN, TOLERANCE, Case, golden_names
+
+
+@pytest.mark.parametrize("shp_fp32", [False, True])
+def test_oracle_matches_reference_py(golden_case, shp_fp32):
+    c = golden_case
+    slc, amp, valid = c.strip()
+    npairs = c.n * (c.n - 1) // 2 if c.pairs is not None else 0
+    o = oracle.run_oracle(slc, amp, valid, c.rows, c.cols, npairs=npairs, pairs_all=True,
+                          shp_fp32=shp_fp32, **c.kwargs())
+    assert np.array_equal(o["count"], c.count)
+    assert np.array_equal(np.isnan(o["coh"]), np.isnan(c.coh))
+    m = ~np.isnan(c.coh)
+    # Samples rotated by a geometric phase are rounded to float (main.c:121-122).
+    tol = 1e-7 if c.phase is not None else 1e-12
+    assert np.allclose(o["coh"][m], c.coh[m], rtol=0, atol=tol)
+    if npairs:
+        assert np.array_equal(np.isnan(o["pairs"]), np.isnan(c.pairs))
+        pm = ~np.isnan(c.pairs)
+        assert np.allclose(o["pairs"][pm], c.pairs[pm], rtol=0, atol=tol)
+
+
+def test_statistics_known_answers():
+    # tests/i_sar_temporal_coherence_test.py:30-46 of the reference, whose
+    # statistics reference.py checks against scipy.stats.
+    d = np.load(GOLDEN + "/statistics.npz")
+    for a, b, ad, ks in zip(d["a"], d["b"], d["ad"], d["ks"]):
+        a32, b32 = np.sort(a.astype(np.float32)), np.sort(b.astype(np.float32))
+        assert oracle.ad_statistic(a32, b32) == pytest.approx(ad, rel=1e-6)
+        assert oracle.ks_accept(a32, b32, 0.05) == bool(ks)
+    for n, sigma in zip(range(3, 65), d["ad_sigma"]):
+        assert oracle.ad_sigma(n) == pytest.approx(sigma, rel=1e-12)
+    for alpha, crit in zip((0.001, 0.003, 0.01, 0.05, 0.1, 0.2, 0.25), d["ad_critical"]):
+        assert oracle.ad_critical(alpha) == pytest.approx(crit, rel=1e-12)
+    assert oracle.ad_critical(0.05) == pytest.approx(1.961)
+    assert oracle.ad_critical(0.01) == pytest.approx(3.752)
+
+
+def test_scipy_statistics():
+    stats = pytest.importorskip("scipy.stats")
+    rng = np.random.default_rng(11)
+    for n in (5, 12, 30):
+        for _ in range(10):
+            a = np.sort(rng.rayleigh(size=n)).astype(np.float32)
+            b = np.sort(rng.rayleigh(scale=1.4, size=n)).astype(np.float32)
+            import warnings
+
+            with warnings.catch_warnings():
+                warnings.simplefilter("ignore")
+                want = stats.anderson_ksamp([a.astype(float), b.astype(float)], midrank=False).statistic
+            assert oracle.ad_statistic(a, b) == pytest.approx(want, rel=1e-9)
+
+
+def test_eigensolver():
+    rng = np.random.default_rng(3)
+    for n in (2, 5, 30, 64):
+        x = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+        h = x @ x.conj().T
+        w, v = oracle.hermitian_eigen(h)
+        assert np.allclose(np.sort(w), np.linalg.eigvalsh(h), rtol=1e-12, atol=1e-10)
+        assert np.allclose(h @ v, v * w[None, :], atol=1e-9 * np.abs(w).max())
+
+
+@pytest.mark.skipif(not oracle.reference_available(), reason="oracle/_ref not built")
+def test_reference_kernel_matches_reference_py(golden_case):
+    c = golden_case
+    slc, amp, valid = c.strip()
+    npairs = c.n * (c.n - 1) // 2 if c.pairs is not None else 0
+    r = oracle.run_reference(slc, amp, valid, c.rows, c.cols, npairs=npairs, pairs_all=True,
+                             **c.kwargs())
+    assert np.array_equal(r["count"], c.count)
+    assert np.array_equal(np.isnan(r["coh"]), np.isnan(c.coh))
+    m = ~np.isnan(c.coh)
+    assert np.allclose(r["coh"][m], c.coh[m], rtol=0, atol=TOLERANCE)
+
+
+@pytest.mark.skipif(not oracle.reference_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("n,test,alpha", [(10, "ks", 0.05), (10, "ad", 0.05), (30, "ad", 0.01),
+                                          (12, "tlog", 0.05), (30, "tlog", 0.01)])
+def test_oracle_float_shp_is_the_reference_kernel(n, test, alpha):
+    """The oracle's float SHP statistics decide as the reference kernel."""
+    import tcoh_b200.synthetic as syn
+
+    stack = syn.generate(n, 40, 32, seed=n, g0_max=0.9)
+    import tcoh_b200
+
+    slc, amp, valid = tcoh_b200.read_strip(stack.real, stack.imag, -10, 60, 3)
+    kw = dict(window=(21, 7), shp_test=test, alpha=alpha, min_shp=n, estimator="evd")
+    r = oracle.run_reference(slc, amp, valid, 40, 32, **kw)
+    o = oracle.run_oracle(slc, amp, valid, 40, 32, shp_fp32=True, **kw)
+    assert np.array_equal(r["count"], o["count"])
