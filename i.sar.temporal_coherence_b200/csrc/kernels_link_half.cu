@@ -23,9 +23,9 @@
  * smallest eigenvalue is then refined in double: the residual
  * r = M x - mu x (M and mu in double) is mapped by the float Householder
  * basis Q onto the tridiagonal, the correction solves (tri - mu) t = Q^H r
- * off the eigen-direction, and x -= Q t; two such steps give double
+ * off the eigen-direction, and x -= Q t; this step gives double
  * accuracy whenever the float rounding of M is small against the gap of its
- * two smallest eigenvalues.
+ * two smallest eigenvalues (one step squares the relative error).
  */
 #include "tcoh_internal.h"
 
@@ -138,21 +138,58 @@ __device__ __forceinline__ HWs hws(unsigned char *base, const HalfLayout &L)
 /* Householder reduction of the group's matrix (rows in r0, r1).       */
 /* ------------------------------------------------------------------ */
 
+/* Norm of the sub-pivot part of the pivot column, the sub-diagonal and the
+   diagonal of step k, from the pivot column values c0, c1 of rows i0, i1. */
+struct StepHead {
+    float xn2;
+    float2 alpha;
+    float dk;
+};
+
+__device__ __forceinline__ StepHead step_head(float2 c0, float2 c1, int k, int n, const Grp &g)
+{
+    const int i0 = g.gl, i1 = g.gl + 16;
+    StepHead h;
+    float x = (i0 >= k + 2 && i0 < n ? c0.x * c0.x + c0.y * c0.y : 0.f) +
+              (i1 >= k + 2 && i1 < n ? c1.x * c1.x + c1.y * c1.y : 0.f);
+    const float2 sa = k + 1 < 16 ? c0 : c1;
+
+    h.alpha = make_float2(gbcast(sa.x, k + 1, g), gbcast(sa.y, k + 1, g));
+    h.dk = gbcast(k < 16 ? c0.x : c1.x, k, g);
+    h.xn2 = gsum(x, g);
+    return h;
+}
+
+/* One element of the rank-2 update: t - (v conj(wj) + w conj(vj)), with
+   nv = -v and nw = -w (four FMAs per component). */
+__device__ __forceinline__ float2 r2(float2 t, float2 nv, float2 nw, float4 q)
+{
+    t.x = fmaf(nv.x, q.z, t.x);
+    t.x = fmaf(nv.y, q.w, t.x);
+    t.x = fmaf(nw.x, q.x, t.x);
+    t.x = fmaf(nw.y, q.y, t.x);
+    t.y = fmaf(nv.y, q.z, t.y);
+    t.y = fmaf(-nv.x, q.w, t.y);
+    t.y = fmaf(nw.y, q.x, t.y);
+    t.y = fmaf(-nw.x, q.y, t.y);
+    return t;
+}
+
 __device__ void householder(float2 (&r0)[32], float2 (&r1)[32], int n, const HWs &w, int ld,
                             const Grp &g)
 {
     const int i0 = g.gl, i1 = g.gl + 16;
 
+    /* Entries 32..63 stay zero: whole blocks of 4 columns may run past n. */
+    w.vw[32 + g.gl] = make_float4(0.f, 0.f, 0.f, 0.f);
+    w.vw[48 + g.gl] = make_float4(0.f, 0.f, 0.f, 0.f);
+    StepHead hd = step_head(r0[0], r1[0], 0, n, g);
+
     for (int k = 0; k < n - 1; k++) {
         const int len = n - 1 - k;
         const float2 c0 = r0[0], c1 = r1[0];
-        float xn2 = (i0 >= k + 2 && i0 < n ? c0.x * c0.x + c0.y * c0.y : 0.f) +
-                    (i1 >= k + 2 && i1 < n ? c1.x * c1.x + c1.y * c1.y : 0.f);
-
-        xn2 = gsum(xn2, g);
-        const float2 sa = k + 1 < 16 ? c0 : c1;
-        const float2 alpha = make_float2(gbcast(sa.x, k + 1, g), gbcast(sa.y, k + 1, g));
-        const float dk = gbcast(k < 16 ? c0.x : c1.x, k, g);
+        const float2 alpha = hd.alpha;
+        const float xn2 = hd.xn2;
         float beta, tr = 0.f, ti = 0.f, sr = 0.f, si = 0.f;
 
         if (xn2 == 0.f && alpha.y == 0.f)
@@ -185,14 +222,15 @@ __device__ void householder(float2 (&r0)[32], float2 (&r1)[32], int n, const HWs
         if (i1 > k && i1 < n)
             w.T[i1 * ld + k] = v1;
         if (g.gl == 0) {
-            w.d[k] = dk;
+            w.d[k] = hd.dk;
             w.e[k] = beta;
             w.tau[k] = make_float2(tr, ti);
         }
-        /* With tau = 0 the update below is exact zero: only the shift. */
+        /* With tau = 0 the update below is an exact zero: only the shift. */
         ((float2 *)w.vw)[2 * i0] = v0;
         ((float2 *)w.vw)[2 * i1] = v1;
         gsync(g);
+        const float4 *vwk = w.vw + k;
         float2 p0a = make_float2(0.f, 0.f), p0b = p0a, p1a = p0a, p1b = p0a;
 
 #pragma unroll
@@ -201,24 +239,24 @@ __device__ void householder(float2 (&r0)[32], float2 (&r1)[32], int n, const HWs
                 break;
 #pragma unroll
             for (int jj = jb; jj < jb + 4 && jj < 32; jj++) {
-                if (jj <= len) {
-                    const float2 vj = ((const float2 *)w.vw)[2 * (k + jj)];
-                    float2 &q0 = (jj & 1) ? p0b : p0a;
-                    float2 &q1 = (jj & 1) ? p1b : p1a;
+                const float2 vj = *(const float2 *)&vwk[jj];
+                float2 &q0 = (jj & 1) ? p0b : p0a;
+                float2 &q1 = (jj & 1) ? p1b : p1a;
 
-                    q0.x = fmaf(r0[jj].x, vj.x, fmaf(-r0[jj].y, vj.y, q0.x));
-                    q0.y = fmaf(r0[jj].x, vj.y, fmaf(r0[jj].y, vj.x, q0.y));
-                    q1.x = fmaf(r1[jj].x, vj.x, fmaf(-r1[jj].y, vj.y, q1.x));
-                    q1.y = fmaf(r1[jj].x, vj.y, fmaf(r1[jj].y, vj.x, q1.y));
-                }
+                q0.x = fmaf(r0[jj].x, vj.x, fmaf(-r0[jj].y, vj.y, q0.x));
+                q0.y = fmaf(r0[jj].x, vj.y, fmaf(r0[jj].y, vj.x, q0.y));
+                q1.x = fmaf(r1[jj].x, vj.x, fmaf(-r1[jj].y, vj.y, q1.x));
+                q1.y = fmaf(r1[jj].x, vj.y, fmaf(r1[jj].y, vj.x, q1.y));
             }
         }
         const float2 p0 = make_float2(p0a.x + p0b.x, p0a.y + p0b.y);
         const float2 p1 = make_float2(p1a.x + p1b.x, p1a.y + p1b.y);
         float2 w0 = make_float2(tr * p0.x - ti * p0.y, tr * p0.y + ti * p0.x);
         float2 w1 = make_float2(tr * p1.x - ti * p1.y, tr * p1.y + ti * p1.x);
-        float pr = (i0 > k ? w0.x * v0.x + w0.y * v0.y : 0.f) + (i1 > k ? w1.x * v1.x + w1.y * v1.y : 0.f);
-        float pi = (i0 > k ? w0.x * v0.y - w0.y * v0.x : 0.f) + (i1 > k ? w1.x * v1.y - w1.y * v1.x : 0.f);
+        float pr = (i0 > k ? w0.x * v0.x + w0.y * v0.y : 0.f) +
+                   (i1 > k ? w1.x * v1.x + w1.y * v1.y : 0.f);
+        float pi = (i0 > k ? w0.x * v0.y - w0.y * v0.x : 0.f) +
+                   (i1 > k ? w1.x * v1.y - w1.y * v1.x : 0.f);
 
         pr = gsum(pr, g);
         pi = gsum(pi, g);
@@ -235,23 +273,35 @@ __device__ void householder(float2 (&r0)[32], float2 (&r1)[32], int n, const HWs
         ((float2 *)w.vw)[2 * i0 + 1] = w0;
         ((float2 *)w.vw)[2 * i1 + 1] = w1;
         gsync(g);
+        const float2 nv0 = make_float2(-v0.x, -v0.y), nv1 = make_float2(-v1.x, -v1.y);
+        const float2 nw0 = make_float2(-w0.x, -w0.y), nw1 = make_float2(-w1.x, -w1.y);
+
+        /* Column k + 1 first: it is the next pivot column, so the next
+           step's reductions overlap the rest of this update. */
+        {
+            const float4 q = vwk[1];
+
+            r0[0] = r2(r0[1], nv0, nw0, q);
+            r1[0] = r2(r1[1], nv1, nw1, q);
+        }
+        hd = step_head(r0[0], r1[0], k + 1, n, g); /* unused after the last step */
 #pragma unroll
-        for (int jb = 1; jb < 32; jb += 4) {
+        for (int jj = 2; jj < 6; jj++) {
+            const float4 q = vwk[jj];
+
+            r0[jj - 1] = r2(r0[jj], nv0, nw0, q);
+            r1[jj - 1] = r2(r1[jj], nv1, nw1, q);
+        }
+#pragma unroll
+        for (int jb = 6; jb < 32; jb += 4) {
             if (jb > len)
                 break;
 #pragma unroll
             for (int jj = jb; jj < jb + 4 && jj < 32; jj++) {
-                if (jj <= len) {
-                    const float4 q = w.vw[k + jj]; /* v_j (xy), w_j (zw) */
-                    float2 t0 = r0[jj], t1 = r1[jj];
+                const float4 q = vwk[jj];
 
-                    t0.x -= v0.x * q.z + v0.y * q.w + w0.x * q.x + w0.y * q.y;
-                    t0.y -= v0.y * q.z - v0.x * q.w + w0.y * q.x - w0.x * q.y;
-                    t1.x -= v1.x * q.z + v1.y * q.w + w1.x * q.x + w1.y * q.y;
-                    t1.y -= v1.y * q.z - v1.x * q.w + w1.y * q.x - w1.x * q.y;
-                    r0[jj - 1] = t0;
-                    r1[jj - 1] = t1;
-                }
+                r0[jj - 1] = r2(r0[jj], nv0, nw0, q);
+                r1[jj - 1] = r2(r1[jj], nv1, nw1, q);
             }
         }
         gsync(g);
@@ -344,6 +394,9 @@ __device__ float tri_eigenvalue(int n, int index, const HWs &w, const Grp &g, fl
     return 0.5f * (lo + hi);
 }
 
+__device__ __forceinline__ float rcpx(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double rcpx(double x) { return 1.0 / x; }
+
 /* Partially pivoted LU of tri - lambda I, into w.lu (written by the first
    lane of the group); returns the pivot bits. Every lane computes it. */
 template <typename R>
@@ -360,14 +413,14 @@ __device__ unsigned long long tri_lu(int n, R lambda, R tiny, const HWs &w, cons
         if (fabs(dd) >= fabs(sub)) {
             if (fabs(dd) < tiny)
                 dd = dd < (R)0 ? -tiny : tiny;
-            const R rd = (R)1 / dd, l = sub * rd;
+            const R rd = rcpx(dd), l = sub * rd;
 
             f = make_float4((float)rd, (float)s1, 0.f, (float)l);
             dd = nd - l * s1;
             s1 = ns;
         }
         else {
-            const R rs = (R)1 / sub, l = dd * rs;
+            const R rs = rcpx(sub), l = dd * rs;
 
             piv |= 1ull << k;
             f = make_float4((float)rs, (float)nd, (float)ns, (float)l);
@@ -380,7 +433,7 @@ __device__ unsigned long long tri_lu(int n, R lambda, R tiny, const HWs &w, cons
     if (fabs(dd) < tiny)
         dd = dd < (R)0 ? -tiny : tiny;
     if (g.gl == 0)
-        w.lu[n - 1] = make_float4((float)((R)1 / dd), 0.f, 0.f, 0.f);
+        w.lu[n - 1] = make_float4((float)rcpx(dd), 0.f, 0.f, 0.f);
     gsync(g);
     return piv;
 }
@@ -885,25 +938,22 @@ __device__ void load_T(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
                        const Grp &g)
 {
     const int n = s.n, npu = tc_npu(n);
+    const int i0 = g.gl, i1 = g.gl + 16;
     float2 gv[33];
 
+    /* every load issued before any use */
+    const float d0 = (active && i0 < n) ? gram[(long long)tc_pidx(n, i0, i0) * c.npix + p].x : 1.f;
+    const float d1 = (active && i1 < n) ? gram[(long long)tc_pidx(n, i1, i1) * c.npix + p].x : 1.f;
 #pragma unroll
     for (int t = 0; t < 33; t++) {
         const int q = g.gl + 16 * t;
 
         gv[t] = (active && q < npu) ? gram[(long long)q * c.npix + p] : make_float2(0.f, 0.f);
     }
-#pragma unroll
-    for (int t = 0; t < 33; t++) {
-        const int q = g.gl + 16 * t;
-
-        if (q < npu) {
-            const int i = upper_tab[q] >> 8, j = upper_tab[q] & 255;
-
-            if (i == j)
-                w.nrm[i] = __fsqrt_rn(gv[t].x);
-        }
-    }
+    if (i0 < n)
+        w.nrm[i0] = __fsqrt_rn(d0);
+    if (i1 < n)
+        w.nrm[i1] = __fsqrt_rn(d1);
     gsync(g);
     const float fl = (float)looks;
 
@@ -926,17 +976,17 @@ __device__ void load_T(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
             const float dd = __fmul_rn(w.nrm[i], w.nrm[j]);
 
             if (dd > 0.f) {
-                re = __fdiv_rn(gq.x, dd);
-                im = __fdiv_rn(gq.y, dd);
-                if (k.bias && looks > 1) {
-                    const float m2 = __fadd_rn(__fmul_rn(re, re), __fmul_rn(im, im));
-                    const float m2c =
-                        __fdiv_rn(__fsub_rn(__fmul_rn(fl, m2), 1.0f), __fsub_rn(fl, 1.0f));
-                    const float f =
-                        (m2 > 0.f && m2c > 0.f) ? __fsqrt_rn(__fdiv_rn(m2c, m2)) : 0.f;
+                const float rd = __frcp_rn(dd);
 
-                    re = __fmul_rn(re, f);
-                    im = __fmul_rn(im, f);
+                re = gq.x * rd;
+                im = gq.y * rd;
+                if (k.bias && looks > 1) {
+                    const float m2 = re * re + im * im;
+                    const float m2c = (fl * m2 - 1.0f) * __frcp_rn(fl - 1.0f);
+                    const float f = (m2 > 0.f && m2c > 0.f) ? sqrtf(m2c * __frcp_rn(m2)) : 0.f;
+
+                    re *= f;
+                    im *= f;
                 }
             }
         }
@@ -1193,7 +1243,6 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
             z0 = make_double2(f0.x, f0.y);
             z1 = make_double2(f1.x, f1.y);
             refine(n, ld, w, g, z0, z1, yr, piv, true);
-            refine(n, ld, w, g, z0, z1, yr, piv, true);
         }
         const float gamma = gamma16(n, ld, w, g, z0, z1, upper_tab);
 
@@ -1233,7 +1282,7 @@ HalfLayout half_layout(int n, int emi)
     L.ld = n | 1;
     L.off_T = take(8 * n * L.ld);
     L.off_G = take(emi ? 8 * n * L.ld : 0);
-    L.off_vw = take(16 * 32);
+    L.off_vw = take(16 * 64);
     L.off_lu = take(16 * 32);
     L.off_tau = take(8 * 32);
     L.off_d = take(4 * 32);
