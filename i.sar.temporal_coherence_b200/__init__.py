@@ -37,7 +37,7 @@ EXPORTS = (
     "ocl_list_devices", "ocl_open", "ocl_run", "ocl_close",
     "tc_last_error", "tc_set_fatal_handler", "tc_shp_constants", "tc_device_count",
     "tc_open", "tc_run_ex", "tc_run_device", "tc_set_timing", "tc_stage_stats",
-    "tc_close", "tc_fp32_peak",
+    "tc_close", "tc_fp32_peak", "tc_run_device_static",
 )
 
 
@@ -103,6 +103,8 @@ def library():
         lib.tc_stage_stats.argtypes = [vp, vp, vp, i]
         lib.tc_close.argtypes = [vp]
         lib.tc_fp32_peak.argtypes = [i, ctypes.POINTER(ctypes.c_double)]
+        lib.tc_run_device_static.argtypes = [ctypes.POINTER(Settings), i, vp, vp, vp, i, i, i,
+                                             vp, vp, vp, vp, vp, vp]
         lib.ocl_open.restype = vp
         lib.ocl_open.argtypes = [i, i, ctypes.POINTER(Settings), i, sz]
         lib.ocl_run.argtypes = [vp, vp, vp, vp, i, i, i, vp, vp, vp]
@@ -195,6 +197,21 @@ def ocl_close(o):
 
 
 # -- extended interface ---------------------------------------------------------
+
+def run_device_static(settings, padded_cols, slc, amp, valid, rows, cols, coh, count,
+                      pairs=None, phases=None, status=None, stream=None):
+    """tc_run_device_static: the path on device buffers the caller owns,
+    without allocating device memory (see include/tcoh_b200.h). Arguments
+    are CUDA tensors (or objects with data_ptr()); asynchronous on
+    `stream` (a torch.cuda.Stream or raw handle; None is CUDA's default
+    stream) on the current device."""
+    if stream is not None and hasattr(stream, "cuda_stream"):
+        stream = stream.cuda_stream
+    _check(library().tc_run_device_static(
+        ctypes.byref(settings), padded_cols, _ptr(slc), _ptr(amp), _ptr(valid), slc.shape[0],
+        rows, cols, _ptr(coh), _ptr(count), _ptr(pairs), _ptr(phases), _ptr(status),
+        ctypes.c_void_p(int(stream or 0)),
+    ))
 
 class Backend:
     """One device context for strips of a fixed width (tc_open)."""

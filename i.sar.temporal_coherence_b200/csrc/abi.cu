@@ -87,6 +87,17 @@ static void message(const char *fmt, ...)
 
 TC_API const char *tc_last_error(void) { return g_error; }
 
+/* For the other translation units of the library. */
+int tc_error(int code, const char *fmt, ...)
+{
+    va_list ap;
+
+    va_start(ap, fmt);
+    vsnprintf(g_error, sizeof(g_error), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
 TC_API void tc_set_fatal_handler(void (*handler)(const char *message)) { g_fatal = handler; }
 
 /* ------------------------------------------------------------------ */
@@ -246,6 +257,13 @@ static int check_settings(const struct settings *s, int padded_cols)
                          padded_cols, s->win_rg);
     return TC_OK;
 }
+
+int tc_check_settings(const struct settings *s, int padded_cols)
+{
+    return check_settings(s, padded_cols);
+}
+
+float tc_float_literal(double v) { return float_literal(v); }
 
 TC_API int tc_device_count(void)
 {

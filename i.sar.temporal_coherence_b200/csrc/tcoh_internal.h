@@ -67,6 +67,11 @@ __host__ __device__ inline void tc_pixel_yx(const TcChunk &c, int p, int &y, int
     x = tx * TC_TILE_W + (w & 7);
 }
 
+/* Helpers of abi.cu shared with the other translation units. */
+int tc_error(int code, const char *fmt, ...);
+int tc_check_settings(const struct settings *s, int padded_cols);
+float tc_float_literal(double v);
+
 /* Kernel launchers (kernels_*.cu); all asynchronous on `st`. */
 cudaError_t tc_launch_prep(const TcStrip &s, const float *slc_aos, float2 *soa,
                            cudaStream_t st);

@@ -160,6 +160,24 @@ int tc_close(struct ocl *o);
    FMA), the roofline denominator of the kernels on the CUDA cores. */
 int tc_fp32_peak(int device, double *tflops);
 
+/* tc_run_device for callers that must not allocate device memory: no
+   context, no cudaMalloc, on the current device and `stream` (NULL: CUDA's
+   default stream); every pointer is a device address the caller owns. The
+   path's intermediate buffers live in one static device array of 64 MiB,
+   which every GPU that loads the library holds until exit; a strip whose
+   16-row sub-strip needs more (very wide strips with many dates) gets
+   TC_ERR_ARG and a message with the limit. All calls share that array:
+   calls that overlap on the GPU race. The first call on a device looks up
+   the array's address (cudaGetSymbolAddress) and should come before any
+   stream capture. The coherence matrices use plain FP32 (TC_GRAM_FP32).
+   No counterpart in the reference, whose ocl_open always allocates. */
+int tc_run_device_static(const struct settings *s, int padded_cols,
+                         const float *slc, const float *amp,
+                         const unsigned char *valid, int padded_rows,
+                         int rows, int cols, float *coh, int *count,
+                         float *pairs, float *phases, unsigned char *status,
+                         void *stream);
+
 #ifdef __cplusplus
 }
 #endif
