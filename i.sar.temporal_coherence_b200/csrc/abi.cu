@@ -716,6 +716,9 @@ TC_API int tc_run_ex(struct ocl *o, const float *slc, const float *amp,
     tm.end(t);
     CK(cudaStreamSynchronize(st));
     tm.collect();
+    if (o->opt.gram == TC_GRAM_TENSOR && tc_gram_tensor_fault() > 0)
+        return set_error(TC_ERR_DEVICE, "tensor-core Gram: a wait for MMA completion ran out; "
+                         "the tiles concerned are NULL");
     return TC_OK;
 }
 

@@ -89,6 +89,9 @@ cudaError_t tc_launch_gram_tensor(const TcStrip &s, const TcChunk &c, int split_
                                   const float *slc_aos, const uint32_t *mask,
                                   float2 *gram, cudaStream_t st);
 bool tc_gram_tensor_supported(const TcStrip &s);
+/* 1 if a tensor-core Gram wait ran out since the last call (and clears it),
+   0 if not, -1 if the flag cannot be read. Synchronous. */
+int tc_gram_tensor_fault(void);
 int tc_gram_block_for(int n);
 cudaError_t tc_launch_link(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
                            const float2 *gram, const int *count,

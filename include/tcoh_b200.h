@@ -131,7 +131,9 @@ int tc_open(int device, const struct settings *s, int padded_cols,
 
 /* ocl_run with a return code and optional extra outputs: phases
    float [rows][cols][N] and status unsigned char [rows][cols] (either may
-   be NULL). Host buffers. */
+   be NULL). Host buffers. Returns TC_ERR_DEVICE if a bounded wait of the
+   tensor-core Gram ran out during this or an earlier tc_run_device call;
+   the tiles concerned come out NULL. */
 int tc_run_ex(struct ocl *o, const float *slc, const float *amp,
               const unsigned char *valid, int padded_rows, int rows, int cols,
               float *coh, int *count, float *pairs, float *phases,
