@@ -37,7 +37,7 @@ EXPORTS = (
     "ocl_list_devices", "ocl_open", "ocl_run", "ocl_close",
     "tc_last_error", "tc_set_fatal_handler", "tc_shp_constants", "tc_device_count",
     "tc_open", "tc_run_ex", "tc_run_device", "tc_set_timing", "tc_stage_stats",
-    "tc_close", "tc_fp32_peak", "tc_run_device_static",
+    "tc_close", "tc_fp32_peak", "tc_run_device_static", "tc_get_options",
 )
 
 
@@ -102,6 +102,7 @@ def library():
         lib.tc_set_timing.argtypes = [vp, i]
         lib.tc_stage_stats.argtypes = [vp, vp, vp, i]
         lib.tc_close.argtypes = [vp]
+        lib.tc_get_options.argtypes = [vp, ctypes.POINTER(Options)]
         lib.tc_fp32_peak.argtypes = [i, ctypes.POINTER(ctypes.c_double)]
         lib.tc_run_device_static.argtypes = [ctypes.POINTER(Settings), i, vp, vp, vp, i, i, i,
                                              vp, vp, vp, vp, vp, vp]
@@ -229,6 +230,9 @@ class Backend:
                                  ctypes.byref(h), ctypes.byref(m)))
         self.handle = h
         self.max_alloc = m.value
+        _check(library().tc_get_options(h, ctypes.byref(opt)))
+        self.gram = {GRAM_FP32: "fp32", GRAM_TENSOR: "tensor"}[opt.gram]
+        self.split_terms = opt.split_terms
 
     def close(self):
         if self.handle:

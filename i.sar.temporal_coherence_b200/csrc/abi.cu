@@ -351,7 +351,7 @@ TC_API int tc_open(int device, const struct settings *s, int padded_cols,
     o->shp.ad_sigma = float_literal(s->ad_sigma);
     o->shp.ad_crit = float_literal(s->ad_crit);
     o->shp.tlog_crit = float_literal(s->tlog_crit);
-    o->opt.gram = tc_gram_tensor_supported(TcStrip{o->n}) ? TC_GRAM_TENSOR : TC_GRAM_FP32;
+    o->opt.gram = tc_gram_tensor_supported(o->n, o->wa, o->wr) ? TC_GRAM_TENSOR : TC_GRAM_FP32;
     o->opt.split_terms = 3;
     o->opt.chunk_pixels = 0;
     if (opt) {
@@ -367,9 +367,10 @@ TC_API int tc_open(int device, const struct settings *s, int padded_cols,
         delete o;
         return set_error(TC_ERR_ARG, "unknown Gram arithmetic %d", opt->gram);
     }
-    if (o->opt.gram == TC_GRAM_TENSOR && !tc_gram_tensor_supported(TcStrip{o->n})) {
+    if (o->opt.gram == TC_GRAM_TENSOR && !tc_gram_tensor_supported(o->n, o->wa, o->wr)) {
         delete o;
-        return set_error(TC_ERR_ARG, "tensor-core Gram not available for %d dates", s->ndates);
+        return set_error(TC_ERR_ARG, "tensor-core Gram not available for %d dates and a %d x %d "
+                         "window", s->ndates, s->win_az, s->win_rg);
     }
     o->gram_block = tc_gram_block_for(o->n);
     o->timing = false;
@@ -436,6 +437,14 @@ TC_API int tc_close(struct ocl *o)
     free_bufs(o);
     cudaStreamDestroy(o->stream);
     delete o;
+    return TC_OK;
+}
+
+TC_API int tc_get_options(const struct ocl *o, struct tc_options *opt)
+{
+    if (!o || !opt)
+        return set_error(TC_ERR_ARG, "no context or options");
+    *opt = o->opt;
     return TC_OK;
 }
 
@@ -547,8 +556,9 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
                          padded_rows, rows, o->wa);
     if (o->npairs && !pairs)
         return set_error(TC_ERR_ARG, "no pair buffer for %d pair planes", o->npairs);
-    if (o->opt.gram == TC_GRAM_TENSOR && !tc_gram_tensor_supported(TcStrip{o->n}))
-        return set_error(TC_ERR_ARG, "tensor-core Gram not available for %d dates", o->n);
+    if (o->opt.gram == TC_GRAM_TENSOR && !tc_gram_tensor_supported(o->n, o->wa, o->wr))
+        return set_error(TC_ERR_ARG, "tensor-core Gram not available for %d dates and a %d x %d "
+                         "window", o->n, o->wa, o->wr);
 
     TcStrip s;
 
@@ -741,7 +751,7 @@ TC_API struct ocl *ocl_open(int platform, int device, const struct settings *s,
         set_error(TC_ERR_DEVICE, "platform %d not found (1 platform, see -l)", platform);
         fatal("CUDA backend");
     }
-    opt.gram = tc_gram_tensor_supported(TcStrip{s ? s->ndates : 0}) ? TC_GRAM_TENSOR
+    opt.gram = (s && tc_gram_tensor_supported(s->ndates, s->win_az, s->win_rg)) ? TC_GRAM_TENSOR
                                                                      : TC_GRAM_FP32;
     opt.split_terms = 3;
     opt.chunk_pixels = 0;

@@ -53,14 +53,17 @@ constexpr int TMEM_COLS = 256;    /* 2 x PHASE FP32 columns */
 constexpr int STAGE_LD = KB + 2;  /* float2 per date row of the staged samples */
 constexpr uint32_t WAIT_LIMIT = 1u << 22;
 constexpr int MIN_SMEM = 80 << 10; /* keeps at most two CTAs (512 TMEM columns) per SM */
+constexpr int MAX_WR = 25;        /* window row bits of one pixel, shifted by <= 7, fit 32 */
+constexpr int MAX_WA = 64;
 
 /* Shared-memory carve-up (byte offsets). */
 struct GramSmem {
     int b;       /* 3 terms x KCH chunks x 256 rows x 16 B */
     int a;       /* KCH chunks x 128 rows x 16 B */
     int stage;   /* n x STAGE_LD float2 */
-    int mask;    /* mask_words x 128 u32 */
+    int rows;    /* wa x 128 u32: SHP bits of each window row of each pixel */
     int pair;    /* npu x u16 */
+    int expand;  /* 16 x uint2: four mask bits -> four BF16 0/1 */
     int bar;     /* mbarrier (8 B) + TMEM address (4 B) */
     int bytes;
 };
@@ -69,16 +72,17 @@ constexpr int TERM_BYTES = KCH * 2 * PHASE * 16;
 
 __host__ __device__ inline int up16(int x) { return (x + 15) & ~15; }
 
-__host__ __device__ inline GramSmem gram_smem(int n, int mask_words)
+__host__ __device__ inline GramSmem gram_smem(int n, int wa)
 {
     GramSmem g;
 
     g.b = 0;
     g.a = g.b + 3 * TERM_BYTES;
     g.stage = g.a + KCH * 128 * 16;
-    g.mask = g.stage + up16(n * STAGE_LD * 8);
-    g.pair = g.mask + up16(mask_words * 128 * 4);
-    g.bar = g.pair + up16(tc_npu(n) * 2);
+    g.rows = g.stage + up16(n * STAGE_LD * 8);
+    g.pair = g.rows + wa * 128 * 4;
+    g.expand = g.pair + up16(tc_npu(n) * 2);
+    g.bar = g.expand + 16 * 8;
     g.bytes = g.bar + 16;
     return g;
 }
@@ -176,17 +180,63 @@ __device__ __forceinline__ void split_store(const float (&v)[8], unsigned char *
         *(uint4 *)(dst + 2 * TERM_BYTES) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
 }
 
+/* Samples of this thread's share of K block kb: candidate t / 8 of the
+   block, dates t % 8 + 8 i. Zero outside the strip and for non-finite
+   values. */
+struct Prefetch {
+    float2 v[TC_MAX_DATES / 8];
+};
+
+__device__ __forceinline__ void prefetch(Prefetch &f, const TcStrip &s, const float2 *slc,
+                                         int kb, int K, int UW, int y0, int x0, int t)
+{
+    const int u = kb * KB + (t >> 3), sub = t & 7;
+    const float2 *src = nullptr;
+
+    if (u < K) {
+        const int uy = u / UW, py = y0 + uy, px = x0 + (u - uy * UW);
+
+        if (py < s.padded_rows && px < s.W)
+            src = slc + ((long long)py * s.W + px) * s.n;
+    }
+#pragma unroll
+    for (int i = 0; i < TC_MAX_DATES / 8; i++) {
+        const int d = sub + 8 * i;
+
+        f.v[i] = src && d < s.n ? __ldg(src + d) : make_float2(0.f, 0.f);
+    }
+}
+
+__device__ __forceinline__ void stage_store(const Prefetch &f, float2 *stage, int n, int t)
+{
+    const int kk = t >> 3, sub = t & 7;
+
+#pragma unroll
+    for (int i = 0; i < TC_MAX_DATES / 8; i++) {
+        const int d = sub + 8 * i;
+
+        if (d < n) {
+            float2 v = f.v[i];
+
+            if (!isfinite(v.x) || !isfinite(v.y))
+                v = make_float2(0.f, 0.f);
+            stage[d * STAGE_LD + kk] = v;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(THREADS, 2)
 tc_gram_tc_kernel(TcStrip s, TcChunk c, int terms, const float2 *__restrict__ slc,
                   const uint32_t *__restrict__ mask, float2 *__restrict__ gram)
 {
     extern __shared__ __align__(1024) unsigned char sm[];
     const int n = s.n, npu = tc_npu(n);
-    const GramSmem L = gram_smem(n, s.mask_words);
+    const GramSmem L = gram_smem(n, s.wa);
     unsigned char *sB = sm + L.b, *sA = sm + L.a;
     float2 *stage = (float2 *)(sm + L.stage);
-    uint32_t *s_mask = (uint32_t *)(sm + L.mask);
+    uint32_t *s_rows = (uint32_t *)(sm + L.rows);
     unsigned short *s_pair = (unsigned short *)(sm + L.pair);
+    uint2 *s_expand = (uint2 *)(sm + L.expand);
     uint32_t *s_taddr = (uint32_t *)(sm + L.bar + 8);
     const uint32_t bar = smem_u32(sm + L.bar);
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
@@ -196,15 +246,26 @@ tc_gram_tc_kernel(TcStrip s, TcChunk c, int terms, const float2 *__restrict__ sl
     const int x0 = tx * TC_TILE_W;          /* padded column of union column 0 */
     const int UW = TC_TILE_W + s.wr - 1, K = (TC_TILE_H + s.wa - 1) * UW;
     const int nkb = (K + KB - 1) / KB;
+    const uint32_t wr_mask = (1u << s.wr) - 1u;
+    Prefetch pf;
 
-    /* SHP masks of the tile's pixels; zero for pixels outside the output */
-    for (int e = t; e < s.mask_words * TC_TILE_PIX; e += THREADS) {
-        const int w = e >> 7, m = e & 127;
+    prefetch(pf, s, slc, 0, K, UW, y0, x0, t);
+    /* SHP bits of window row dy of pixel m (bit dx), zero for pixels outside
+       the output */
+    for (int e = t; e < s.wa * TC_TILE_PIX; e += THREADS) {
+        const int dy = e >> 7, m = e & 127;
         const int y = y0 + (m >> 3), x = x0 + (m & 7);
+        uint32_t f = 0u;
 
-        s_mask[e] = (y < c.row0 + c.nrows && y < s.rows && x < s.cols)
-                        ? mask[(long long)w * c.npix + (long long)tile * TC_TILE_PIX + m]
-                        : 0u;
+        if (y < c.row0 + c.nrows && y < s.rows && x < s.cols) {
+            const int b = dy * s.wr, w = b >> 5, o = b & 31;
+            const long long p = (long long)tile * TC_TILE_PIX + m;
+            const uint32_t lo = mask[(long long)w * c.npix + p];
+            const uint32_t hi = o + s.wr > 32 ? mask[(long long)(w + 1) * c.npix + p] : 0u;
+
+            f = (uint32_t)(((unsigned long long)hi << 32 | lo) >> o) & wr_mask;
+        }
+        s_rows[e] = f;
     }
     for (int q = t; q < npu; q += THREADS) {
         int i = 0, r = q;
@@ -215,6 +276,10 @@ tc_gram_tc_kernel(TcStrip s, TcChunk c, int terms, const float2 *__restrict__ sl
         }
         s_pair[q] = (unsigned short)(i << 8 | (i + r));
     }
+    if (t < 16)
+        s_expand[t] = make_uint2((t & 1 ? 0x3f80u : 0u) | (t & 2 ? 0x3f800000u : 0u),
+                                 (t & 4 ? 0x3f80u : 0u) | (t & 8 ? 0x3f800000u : 0u));
+    stage_store(pf, stage, n, t);
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                      ::"r"(smem_u32(s_taddr)), "r"(TMEM_COLS) : "memory");
@@ -230,6 +295,9 @@ tc_gram_tc_kernel(TcStrip s, TcChunk c, int terms, const float2 *__restrict__ sl
     const uint32_t tmem = *s_taddr;
     uint32_t parity = 0;
     bool ok = true, pending = false;
+    /* this thread's A rows and B items: pixel / entry t % 128, chunks
+       t / 128 and t / 128 + 2 */
+    const int m = t & 127, py = m >> 3, px = m & 7, g0 = t >> 7;
 
     for (int P0 = 0; P0 < npu && ok; P0 += PHASE) {
         const int np = min(PHASE, npu - P0), h = up16(np);
@@ -237,22 +305,12 @@ tc_gram_tc_kernel(TcStrip s, TcChunk c, int terms, const float2 *__restrict__ sl
         const uint32_t idesc = instr_desc(2 * h);
 
         for (int kb = 0; kb < nkb; kb++) {
-            /* the block's samples, date-major: stage[d * STAGE_LD + kk] */
-            for (int e = t; e < KB * n; e += THREADS) {
-                const int kk = e / n, d = e - kk * n, u = kb * KB + kk;
-                float2 v = make_float2(0.f, 0.f);
+            /* stage holds block kb; fetch the next block (of this phase, or
+               block 0 for the next phase) while this one is built */
+            const int next = kb + 1 < nkb ? kb + 1 : (P0 + PHASE < npu ? 0 : -1);
 
-                if (u < K) {
-                    const int uy = u / UW, py = y0 + uy, px = x0 + (u - uy * UW);
-
-                    if (py < s.padded_rows && px < s.W) {
-                        v = __ldg(slc + ((long long)py * s.W + px) * n + d);
-                        if (!isfinite(v.x) || !isfinite(v.y))
-                            v = make_float2(0.f, 0.f);
-                    }
-                }
-                stage[d * STAGE_LD + kk] = v;
-            }
+            if (next >= 0)
+                prefetch(pf, s, slc, next, K, UW, y0, x0, t);
             if (pending) { /* the previous block's MMAs still read A and B */
                 ok = mbar_wait(bar, parity);
                 if (ok) {
@@ -264,57 +322,66 @@ tc_gram_tc_kernel(TcStrip s, TcChunk c, int terms, const float2 *__restrict__ sl
                 ok = false;
                 break;
             }
-            /* A: pixel m, candidates 8g .. 8g + 7 of the block -> 16 bytes */
-            for (int e = t; e < KCH * TC_TILE_PIX; e += THREADS) {
-                const int g = e >> 7, m = e & 127, py = m >> 3, px = m & 7;
-                const int u = kb * KB + g * 8;
-                int uy = u / UW, ux = u - uy * UW;
-                uint32_t wv[4] = {0u, 0u, 0u, 0u};
-
+            /* A: pixel m, candidates 8g .. 8g + 7 of the block -> 16 bytes.
+               The 8 candidates span at most two union rows (UW >= 8). */
 #pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    const int dy = uy - py, dx = ux - px;
+            for (int gi = 0; gi < 2; gi++) {
+                const int g = g0 + 2 * gi, u0 = kb * KB + g * 8;
+                const int uy = u0 / UW, ux = u0 - uy * UW, cnt = min(8, UW - ux);
+                uint32_t bits = 0u;
+                int dy = uy - py;
 
-                    if (dy >= 0 && dy < s.wa && dx >= 0 && dx < s.wr) {
-                        const int b = dy * s.wr + dx;
+                if (dy >= 0 && dy < s.wa) {
+                    const uint32_t f = s_rows[dy * TC_TILE_PIX + m];
+                    const int sh = ux - px;
 
-                        if ((s_mask[(b >> 5) * TC_TILE_PIX + m] >> (b & 31)) & 1u)
-                            wv[k >> 1] |= 0x3f80u << (16 * (k & 1));
-                    }
-                    if (++ux == UW) {
-                        ux = 0;
-                        uy++;
-                    }
+                    bits = (sh >= 0 ? f >> sh : f << -sh) & ((1u << cnt) - 1u);
                 }
-                *(uint4 *)(sA + (g * TC_TILE_PIX + m) * 16) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+                dy++;
+                if (cnt < 8 && dy >= 0 && dy < s.wa)
+                    bits |= ((s_rows[dy * TC_TILE_PIX + m] << px) & ((1u << (8 - cnt)) - 1u)) << cnt;
+                const uint2 lo = s_expand[bits & 15u], hi = s_expand[bits >> 4];
+
+                *(uint4 *)(sA + (g * TC_TILE_PIX + m) * 16) = make_uint4(lo.x, lo.y, hi.x, hi.y);
             }
             /* B: entry r of the phase, candidates 8g .. 8g + 7; re in row r,
                im in row h + r of each term */
-            for (int e = t; e < KCH * h; e += THREADS) {
-                const int g = e / h, r = e - g * h;
-                float re[8], im[8];
+            if (m < h) {
+                const int r = m;
+                int i = 0, j = 0;
 
                 if (r < np) {
-                    const int pr = s_pair[P0 + r], i = pr >> 8, j = pr & 255;
-                    const float4 *si = (const float4 *)(stage + i * STAGE_LD + g * 8);
-                    const float4 *sj = (const float4 *)(stage + j * STAGE_LD + g * 8);
+                    const int pr = s_pair[P0 + r];
 
-#pragma unroll
-                    for (int k = 0; k < 4; k++) {
-                        const float4 a = si[k], b = sj[k];
-
-                        re[2 * k] = fmaf(a.x, b.x, a.y * b.y);
-                        im[2 * k] = fmaf(a.y, b.x, -(a.x * b.y));
-                        re[2 * k + 1] = fmaf(a.z, b.z, a.w * b.w);
-                        im[2 * k + 1] = fmaf(a.w, b.z, -(a.z * b.w));
-                    }
-                } else {
-#pragma unroll
-                    for (int k = 0; k < 8; k++)
-                        re[k] = im[k] = 0.f;
+                    i = pr >> 8;
+                    j = pr & 255;
                 }
-                split_store(re, sB + (g * 2 * h + r) * 16, terms);
-                split_store(im, sB + (g * 2 * h + h + r) * 16, terms);
+#pragma unroll
+                for (int gi = 0; gi < 2; gi++) {
+                    const int g = g0 + 2 * gi;
+                    float re[8], im[8];
+
+                    if (r < np) {
+                        const float4 *si = (const float4 *)(stage + i * STAGE_LD + g * 8);
+                        const float4 *sj = (const float4 *)(stage + j * STAGE_LD + g * 8);
+
+#pragma unroll
+                        for (int k = 0; k < 4; k++) {
+                            const float4 a = si[k], b = sj[k];
+
+                            re[2 * k] = fmaf(a.x, b.x, a.y * b.y);
+                            im[2 * k] = fmaf(a.y, b.x, -(a.x * b.y));
+                            re[2 * k + 1] = fmaf(a.z, b.z, a.w * b.w);
+                            im[2 * k + 1] = fmaf(a.w, b.z, -(a.z * b.w));
+                        }
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 8; k++)
+                            re[k] = im[k] = 0.f;
+                    }
+                    split_store(re, sB + (g * 2 * h + r) * 16, terms);
+                    split_store(im, sB + (g * 2 * h + h + r) * 16, terms);
+                }
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncthreads();
@@ -335,6 +402,9 @@ tc_gram_tc_kernel(TcStrip s, TcChunk c, int terms, const float2 *__restrict__ sl
                 mma_commit(bar);
             }
             pending = true;
+            /* the B build above was the last reader of stage */
+            if (next >= 0)
+                stage_store(pf, stage, n, t);
         }
         if (!ok)
             break;
@@ -351,8 +421,8 @@ tc_gram_tc_kernel(TcStrip s, TcChunk c, int terms, const float2 *__restrict__ sl
         /* epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (pixels), half
            of the phase's 16-entry column groups */
         {
-            const int lg = warp & 3, m = lg * 32 + lane;
-            const long long p = (long long)tile * TC_TILE_PIX + m;
+            const int lg = warp & 3, pm = lg * 32 + lane;
+            const long long p = (long long)tile * TC_TILE_PIX + pm;
             const uint32_t lane_addr = tmem + ((uint32_t)(lg * 32) << 16);
 
             for (int cg = warp >> 2; cg * 16 < np; cg += 2) {
@@ -395,11 +465,11 @@ tc_gram_tc_kernel(TcStrip s, TcChunk c, int terms, const float2 *__restrict__ sl
 
 } // namespace
 
-bool tc_gram_tensor_supported(const TcStrip &s)
+bool tc_gram_tensor_supported(int n, int wa, int wr)
 {
     int dev = 0, major = 0, minor = 0;
 
-    if (s.n < 2 || s.n > TC_MAX_DATES)
+    if (n < 2 || n > TC_MAX_DATES || wa < 1 || wa > MAX_WA || wr < 1 || wr > MAX_WR)
         return false;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess ||
@@ -414,7 +484,7 @@ cudaError_t tc_launch_gram_tensor(const TcStrip &s, const TcChunk &c, int split_
                                   const float *slc, const uint32_t *mask, float2 *gram,
                                   cudaStream_t st)
 {
-    const GramSmem L = gram_smem(s.n, s.mask_words);
+    const GramSmem L = gram_smem(s.n, s.wa);
     const int bytes = L.bytes < MIN_SMEM ? MIN_SMEM : L.bytes;
     cudaError_t e;
 

@@ -88,7 +88,8 @@ cudaError_t tc_launch_gram_fp32(const TcStrip &s, const TcChunk &c, int block,
 cudaError_t tc_launch_gram_tensor(const TcStrip &s, const TcChunk &c, int split_terms,
                                   const float *slc_aos, const uint32_t *mask,
                                   float2 *gram, cudaStream_t st);
-bool tc_gram_tensor_supported(const TcStrip &s);
+/* Tensor-core Gram for n dates and a wa x wr window on the current device. */
+bool tc_gram_tensor_supported(int n, int wa, int wr);
 /* 1 if a tensor-core Gram wait ran out since the last call (and clears it),
    0 if not, -1 if the flag cannot be read. Synchronous. */
 int tc_gram_tensor_fault(void);

@@ -146,6 +146,10 @@ int tc_run_device(struct ocl *o, const float *slc, const float *amp,
                   int cols, float *coh, int *count, float *pairs,
                   float *phases, unsigned char *status, void *stream);
 
+/* The options a context runs with, defaults resolved (the Gram
+   arithmetic chosen for gram = -1, the split terms in force). */
+int tc_get_options(const struct ocl *o, struct tc_options *opt);
+
 /* Stage timing. With timing on, every launch of the following runs is
    bracketed by CUDA events on its stream, and tc_stage_stats gives, per
    stage, the device milliseconds summed over the last run and the number

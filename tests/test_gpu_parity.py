@@ -226,3 +226,46 @@ def test_device_resident_strip():
     assert np.array_equal(coh.cpu().numpy(), host["coh"], equal_nan=True)
     assert np.array_equal(pairs.cpu().numpy(), host["pairs"], equal_nan=True)
     assert np.array_equal(phases.cpu().numpy(), host["phases"], equal_nan=True)
+
+
+@pytest.mark.parametrize("n,est,win", [(10, "evd", (21, 7)), (64, "evd", (21, 7)),
+                                       (30, "evd", (11, 5))])
+def test_tensor_gram_two_terms(n, est, win):
+    """Two BF16 terms per product (16 significant bits): within the
+    tolerance on well-conditioned estimators."""
+    rows, cols = 37, 29
+    stack = syn.generate(n, rows, cols, seed=n + 1, nregions=3)
+    ha, hr = win[0] // 2, win[1] // 2
+    slc, amp, valid = tcoh_b200.read_strip(stack.real, stack.imag, -ha, rows + 2 * ha, hr)
+    kw = dict(window=win, shp_test="ks", min_shp=n, estimator=est)
+    with backend_for(n, cols, "tensor", split_terms=2, **kw) as be:
+        r = be.run(slc, amp, valid, rows, cols)
+    o = oracle.run_oracle(slc, amp, valid, rows, cols, shp_fp32=True, **kw)
+    assert np.array_equal(r["count"], o["count"])
+    assert_close(r["coh"], o["coh"])
+
+
+@pytest.mark.parametrize("win", [(33, 25), (63, 3), (1, 25)])
+def test_tensor_gram_window_extremes(win):
+    """The widest and tallest windows the tensor-core Gram takes: the union
+    of a tile's windows spans up to 32 columns and 78 rows."""
+    n, rows, cols = 8, 40, 27
+    stack = syn.generate(n, rows, cols, seed=win[0] * 100 + win[1], nregions=2)
+    ha, hr = win[0] // 2, win[1] // 2
+    slc, amp, valid = tcoh_b200.read_strip(stack.real, stack.imag, -ha, rows + 2 * ha, hr)
+    kw = dict(window=win, shp_test="ad", min_shp=n, estimator="evd")
+    with backend_for(n, cols, "tensor", pairs=True, pairs_all=True, **kw) as be:
+        r = be.run(slc, amp, valid, rows, cols)
+    o = oracle.run_oracle(slc, amp, valid, rows, cols, shp_fp32=True, npairs=n * (n - 1) // 2,
+                          pairs_all=True, **kw)
+    assert np.array_equal(r["count"], o["count"])
+    assert_close(r["coh"], o["coh"])
+    assert_close(r["pairs"], o["pairs"])
+
+
+def test_tensor_gram_rejects_windows_beyond_its_tiles():
+    s = tcoh_b200.make_settings(8, window=(5, 27), min_shp=8)
+    with pytest.raises(tcoh_b200.BackendError, match="tensor-core Gram not available"):
+        tcoh_b200.Backend(s, 40, gram="tensor")
+    with tcoh_b200.Backend(s, 40) as be:  # the default falls back to FP32
+        assert be.gram == "fp32"
