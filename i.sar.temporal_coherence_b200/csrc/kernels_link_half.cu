@@ -1130,15 +1130,25 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
     double *V = scratch + ((size_t)blockIdx.x * wpb * 2 + grp) * (size_t)n * ld;
     const int i0 = g.gl, i1 = g.gl + 16;
 
-    for (int q = blockIdx.x * wpb + warp; 2 * q < c.npix; q += gridDim.x * wpb) {
-        const int p = 2 * q + (lane >> 4);
-        int y, x;
+    /* The warps of a CTA take pixel pairs qb + warp and run each stage
+       together, separated by CTA barriers: the stages' code is far larger
+       than the instruction cache, and warps in different stages would keep
+       evicting each other's instructions. */
+    const int nq = (c.npix + 1) / 2;
 
-        tc_pixel_yx(c, p, y, x);
-        const bool inrange = p < c.npix && y < c.row0 + c.nrows && y < s.rows && x < s.cols;
+    for (int qb = blockIdx.x * wpb; qb < nq; qb += gridDim.x * wpb) {
+        const int q = qb + warp;
+        const int p = 2 * q + (lane >> 4);
+        int y = 0, x = 0;
+
+        if (q < nq)
+            tc_pixel_yx(c, p, y, x);
+        const bool inrange =
+            q < nq && p < c.npix && y < c.row0 + c.nrows && y < s.rows && x < s.cols;
         const long long out = inrange ? (long long)y * s.cols + x : 0;
         const int looks = inrange ? count[out] : -1;
         bool active = inrange && looks >= k.min_looks;
+        unsigned st = 0;
 
         if (inrange && !active) {
             if (g.gl == 0)
@@ -1151,119 +1161,138 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
             if (status && g.gl == 0)
                 status[out] = 0;
         }
-        if (!__any_sync(FULL, active))
-            continue;
-        load_T(s, c, k, p, active, looks, gram, upper_tab, w, ld, g);
-        if (active)
-            for (int t = g.gl; t < k.npairs; t += 16) {
-                const int i = pair_tab[t] >> 8, j = pair_tab[t] & 255;
-                const float2 tv = w.T[i * ld + j];
+        bool run = __any_sync(FULL, active);
 
-                pairs[t * plane + out] = hypotf(tv.x, tv.y);
+        /* stage 1: coherence matrix, pair coherences, connectivity */
+        if (run) {
+            load_T(s, c, k, p, active, looks, gram, upper_tab, w, ld, g);
+            if (active)
+                for (int t = g.gl; t < k.npairs; t += 16) {
+                    const int i = pair_tab[t] >> 8, j = pair_tab[t] & 255;
+                    const float2 tv = w.T[i * ld + j];
+
+                    pairs[t * plane + out] = hypotf(tv.x, tv.y);
+                }
+            if (k.bias && active && !linked16(n, ld, w.T, g)) {
+                if (g.gl == 0)
+                    coh[out] = NAN;
+                if (phases)
+                    for (int r = g.gl; r < n; r += 16)
+                        phases[out * n + r] = NAN;
+                if (status && g.gl == 0)
+                    status[out] = TC_STATUS_UNLINKED;
+                active = false;
             }
-        unsigned st = 0;
-
-        if (k.bias && active && !linked16(n, ld, w.T, g)) {
-            if (g.gl == 0)
-                coh[out] = NAN;
-            if (phases)
-                for (int r = g.gl; r < n; r += 16)
-                    phases[out * n + r] = NAN;
-            if (status && g.gl == 0)
-                status[out] = TC_STATUS_UNLINKED;
-            active = false;
-        }
-        gsync(g);
-        if (!active) {
-            /* a well-conditioned stand-in keeps the group in step */
-            for (int r = g.gl; r < n; r += 16)
-                for (int j = 0; j < n; j++)
-                    w.T[r * ld + j] = make_float2(r == j ? 1.f : 0.f, 0.f);
             gsync(g);
+            if (!active) {
+                /* a well-conditioned stand-in keeps the group in step */
+                for (int r = g.gl; r < n; r += 16)
+                    for (int j = 0; j < n; j++)
+                        w.T[r * ld + j] = make_float2(r == j ? 1.f : 0.f, 0.f);
+                gsync(g);
+            }
+            run = __any_sync(FULL, active);
         }
-        if (!__any_sync(FULL, active))
-            continue;
+        __syncthreads();
 
         float2 r0[32], r1[32];
-        double2 z0, z1;
+        double2 z0 = make_double2(0.0, 0.0), z1 = z0;
+        float yr[32], lambda = 0.f, norm = 0.f;
+        float2 f0 = make_float2(0.f, 0.f), f1 = f0;
 
         if (!EMI) {
+            /* stage 2: Householder reduction of T */
+            if (run) {
 #pragma unroll
-            for (int j = 0; j < 32; j++) {
-                r0[j] = (i0 < n && j < n) ? w.T[i0 * ld + j] : make_float2(0.f, 0.f);
-                r1[j] = (i1 < n && j < n) ? w.T[i1 * ld + j] : make_float2(0.f, 0.f);
+                for (int j = 0; j < 32; j++) {
+                    r0[j] = (i0 < n && j < n) ? w.T[i0 * ld + j] : make_float2(0.f, 0.f);
+                    r1[j] = (i1 < n && j < n) ? w.T[i1 * ld + j] : make_float2(0.f, 0.f);
+                }
+                gsync(g);
+                householder(r0, r1, n, w, ld, g);
             }
-            gsync(g);
-            householder(r0, r1, n, w, ld, g);
-            float yr[32], lambda, norm;
-            float2 f0, f1;
-
-            st |= eigvec(n, n - 1, w, ld, g, f0, f1, yr, lambda, norm);
-            z0 = make_double2(f0.x, f0.y);
-            z1 = make_double2(f1.x, f1.y);
+            __syncthreads();
+            /* stage 3: its dominant eigenvector */
+            if (run) {
+                st |= eigvec(n, n - 1, w, ld, g, f0, f1, yr, lambda, norm);
+                z0 = make_double2(f0.x, f0.y);
+                z1 = make_double2(f1.x, f1.y);
+            }
+            __syncthreads();
         }
         else {
-            for (int r = g.gl; r < n; r += 16)
-                for (int j = 0; j < n; j++) {
-                    const float2 t = w.T[r * ld + j];
+            /* stage 2: |T|^-1 in double */
+            if (run) {
+                for (int r = g.gl; r < n; r += 16)
+                    for (int j = 0; j < n; j++) {
+                        const float2 t = w.T[r * ld + j];
 
-                    w.G[r * ld + j] = hypot((double)t.x, (double)t.y);
-                }
-            gsync(g);
-            st |= emi_inverse(n, ld, w, V, g);
-            /* M = |T|^-1 o T in float rows */
-#pragma unroll
-            for (int j = 0; j < 32; j++) {
-                r0[j] = make_float2(0.f, 0.f);
-                r1[j] = make_float2(0.f, 0.f);
-                if (j < n) {
-                    if (i0 < n) {
-                        const double2 m = mval(w, ld, i0, j);
-
-                        r0[j] = make_float2((float)m.x, (float)m.y);
+                        w.G[r * ld + j] = hypot((double)t.x, (double)t.y);
                     }
-                    if (i1 < n) {
-                        const double2 m = mval(w, ld, i1, j);
-
-                        r1[j] = make_float2((float)m.x, (float)m.y);
-                    }
-                }
+                gsync(g);
+                st |= emi_inverse(n, ld, w, V, g);
             }
-            gsync(g);
-            /* The reduction parks its vectors in T's lower triangle, which
-               mval no longer reads (it takes T_ij from i < j). */
-            householder(r0, r1, n, w, ld, g);
-            float yr[32], lambda, norm;
-            float2 f0, f1;
-
-            st |= eigvec(n, 0, w, ld, g, f0, f1, yr, lambda, norm);
-            const unsigned long long piv =
-                tri_lu<float>(n, lambda, 1.0e-6f * fmaxf(norm, 1.0e-30f), w, g);
-
-            z0 = make_double2(f0.x, f0.y);
-            z1 = make_double2(f1.x, f1.y);
-            refine(n, ld, w, g, z0, z1, yr, piv, true);
-        }
-        const float gamma = gamma16(n, ld, w, g, z0, z1, upper_tab);
-
-        if (active) {
-            if (g.gl == 0)
-                coh[out] = gamma;
-            if (phases)
+            __syncthreads();
+            /* stage 3: M = |T|^-1 o T in float rows, Householder reduction */
+            if (run) {
 #pragma unroll
-                for (int t = 0; t < 2; t++) {
-                    const int r = t ? i1 : i0;
+                for (int j = 0; j < 32; j++) {
+                    r0[j] = make_float2(0.f, 0.f);
+                    r1[j] = make_float2(0.f, 0.f);
+                    if (j < n) {
+                        if (i0 < n) {
+                            const double2 m = mval(w, ld, i0, j);
 
-                    if (r < n) {
-                        const float2 u = w.zs[r];
+                            r0[j] = make_float2((float)m.x, (float)m.y);
+                        }
+                        if (i1 < n) {
+                            const double2 m = mval(w, ld, i1, j);
 
-                        phases[out * n + r] = atan2f(u.y, u.x);
+                            r1[j] = make_float2((float)m.x, (float)m.y);
+                        }
                     }
                 }
-            if (status && g.gl == 0)
-                status[out] = (unsigned char)st;
+                gsync(g);
+                /* The reduction parks its vectors in T's lower triangle,
+                   which mval no longer reads (it takes T_ij from i < j). */
+                householder(r0, r1, n, w, ld, g);
+            }
+            __syncthreads();
+            /* stage 4: eigenvector of the smallest eigenvalue, refined */
+            if (run) {
+                st |= eigvec(n, 0, w, ld, g, f0, f1, yr, lambda, norm);
+                const unsigned long long piv =
+                    tri_lu<float>(n, lambda, 1.0e-6f * fmaxf(norm, 1.0e-30f), w, g);
+
+                z0 = make_double2(f0.x, f0.y);
+                z1 = make_double2(f1.x, f1.y);
+                refine(n, ld, w, g, z0, z1, yr, piv, true);
+            }
+            __syncthreads();
         }
-        __syncwarp();
+        /* last stage: phasors, temporal coherence, outputs */
+        if (run) {
+            const float gamma = gamma16(n, ld, w, g, z0, z1, upper_tab);
+
+            if (active) {
+                if (g.gl == 0)
+                    coh[out] = gamma;
+                if (phases)
+#pragma unroll
+                    for (int t = 0; t < 2; t++) {
+                        const int r = t ? i1 : i0;
+
+                        if (r < n) {
+                            const float2 u = w.zs[r];
+
+                            phases[out * n + r] = atan2f(u.y, u.x);
+                        }
+                    }
+                if (status && g.gl == 0)
+                    status[out] = (unsigned char)st;
+            }
+        }
+        __syncthreads();
     }
 }
 
