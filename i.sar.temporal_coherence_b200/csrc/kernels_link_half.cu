@@ -538,54 +538,77 @@ __device__ unsigned eigvec(int n, int index, const HWs &w, int ld, const Grp &g,
 /* EMI: |T|^-1 in double.                                              */
 /* ------------------------------------------------------------------ */
 
-/* Gauss-Jordan without pivoting on the group's symmetric matrix (rows
-   i0, i1 in g0, g1; rows and columns >= n zero), in place. False when a
-   pivot is not above `floor`. */
-__device__ bool gj16(double (&g0)[32], double (&g1)[32], int n, double floor, const HWs &w,
-                     const Grp &g)
+/* Symmetric sweep (Gauss-Jordan elimination without pivoting in the form
+   that keeps the matrix symmetric; Goodnight, The American Statistician 33,
+   1979) of the group's matrix: rows i0, i1 in g0, g1, columns >= n zero.
+   Sweeping pivot k maps
+       a_ij -> a_ij - a_ik a_kj / a_kk,  a_ik, a_kj -> a_ik / a_kk,
+       a_kk -> -1 / a_kk,
+   and sweeping every pivot leaves -A^-1. Because the matrix stays
+   symmetric, pivot row k is assembled from every lane's own column-k
+   entries. The register columns rotate by one per step so that the pivot
+   column is always g[0] (the step loop stays a run-time loop): on return
+   register column p holds true column (p + n) & 31. rs holds 2 x 32
+   doubles (alternate steps use alternate halves). False when a pivot's
+   magnitude is not above `floor`. */
+__device__ bool sweep16(double (&g0)[32], double (&g1)[32], int n, double floor, double *rs,
+                        const Grp &g)
+{
+    const int i0 = g.gl, i1 = g.gl + 16;
+
+    for (int k = 0; k < n; k++) {
+        double *r = rs + 32 * (k & 1);
+
+        /* a_ik, in the order of the registers: rs[p] = a_k,(p + k) & 31 */
+        r[(i0 - k) & 31] = g0[0];
+        r[(i1 - k) & 31] = g1[0];
+        gsync(g);
+        const double d = r[0];
+
+        if (!(fabs(d) > floor))
+            return false;
+        const double id = 1.0 / d;
+        const bool piv0 = i0 == k, piv1 = i1 == k;
+        /* the pivot row scales by 1 / a_kk: a_kj - (1 - 1 / a_kk) a_kj, with
+           a_kj from rs (equal to the row's own value up to rounding) */
+        const double f0 = piv0 ? 1.0 - id : g0[0] * id, f1 = piv1 ? 1.0 - id : g1[0] * id;
+
+#pragma unroll
+        for (int q = 0; q < 32; q += 2) {
+            const double2 a = *(const double2 *)&r[q];
+
+            if (q > 0) {
+                g0[q - 1] = fma(-f0, a.x, g0[q]);
+                g1[q - 1] = fma(-f1, a.x, g1[q]);
+            }
+            g0[q] = fma(-f0, a.y, g0[q + 1]);
+            g1[q] = fma(-f1, a.y, g1[q + 1]);
+        }
+        g0[31] = piv0 ? -id : f0;
+        g1[31] = piv1 ? -id : f1;
+    }
+    return true;
+}
+
+/* Rows i0, i1 of a matrix whose register column p is true column
+   (p + rot) & 31, scaled by s, into dst (n x ld). */
+__device__ __forceinline__ void store_rows(double *dst, int ld, int n, int rot, double s,
+                                           const double (&g0)[32], const double (&g1)[32],
+                                           const Grp &g)
 {
     const int i0 = g.gl, i1 = g.gl + 16;
 
 #pragma unroll
-    for (int k = 0; k < 32; k++) {
-        if (k >= n)
-            break;
-        const double p = gbcast(k < 16 ? g0[k] : g1[k], k, g);
+    for (int p = 0; p < 32; p++) {
+        const int j = (p + rot) & 31;
 
-        if (!(p > floor))
-            return false;
-        const double ip = 1.0 / p;
-
-        if (g.gl == (k & 15)) {
-#pragma unroll
-            for (int j = 0; j < 32; j += 2) {
-                const double a = k < 16 ? g0[j] : g1[j], b = k < 16 ? g0[j + 1] : g1[j + 1];
-
-                *(double2 *)&w.rs[j] = make_double2(a * ip, b * ip);
-            }
+        if (j < n) {
+            if (i0 < n)
+                dst[i0 * ld + j] = s * g0[p];
+            if (i1 < n)
+                dst[i1 * ld + j] = s * g1[p];
         }
-        gsync(g);
-        const double gk0 = g0[k], gk1 = g1[k];
-        const double f0 = i0 == k ? p - 1.0 : gk0, f1 = i1 == k ? p - 1.0 : gk1;
-
-#pragma unroll
-        for (int j = 0; j < 32; j += 2) {
-            const double2 r2 = *(const double2 *)&w.rs[j];
-
-            if (j != k) {
-                g0[j] = fma(-f0, r2.x, g0[j]);
-                g1[j] = fma(-f1, r2.x, g1[j]);
-            }
-            if (j + 1 != k) {
-                g0[j + 1] = fma(-f0, r2.y, g0[j + 1]);
-                g1[j + 1] = fma(-f1, r2.y, g1[j + 1]);
-            }
-        }
-        g0[k] = i0 == k ? ip : -gk0 * ip;
-        g1[k] = i1 == k ? ip : -gk1 * ip;
-        gsync(g);
     }
-    return true;
 }
 
 /* (o0, o1) = rows i0, i1 of A times B; A and B n x ld (memory). */
@@ -706,32 +729,27 @@ __device__ unsigned emi_inverse(int n, int ld, const HWs &w, double *V, const Gr
     const int i0 = g.gl, i1 = g.gl + 16;
     double g0[32], g1[32];
     unsigned st = 0;
+    int rot = n;
 
 #pragma unroll
     for (int j = 0; j < 32; j++) {
         g0[j] = (i0 < n && j < n) ? w.G[i0 * ld + j] : 0.0;
         g1[j] = (i1 < n && j < n) ? w.G[i1 * ld + j] : 0.0;
     }
-    bool ok = gj16(g0, g1, n, 1.0e-5, w, g);
+    bool ok = sweep16(g0, g1, n, 1.0e-5, w.rs, g);
 
     if (!ok) {
-        /* |T| not safely positive definite: (|T|^2)^-1 |T|, with the
-           intermediate inverse in V. */
+        /* a pivot of |T| is close to zero: (|T|^2)^-1 |T|, with the
+           intermediate inverse in V */
         st |= TC_STATUS_EMI_PINV;
         gsync(g);
         rows_times(w.G, w.G, ld, n, i0, i1, g0, g1);
-        ok = gj16(g0, g1, n, 1.0e-300, w, g);
+        ok = sweep16(g0, g1, n, 1.0e-300, w.rs, g);
         if (ok) {
-#pragma unroll
-            for (int j = 0; j < 32; j++)
-                if (j < n) {
-                    if (i0 < n)
-                        V[i0 * ld + j] = g0[j];
-                    if (i1 < n)
-                        V[i1 * ld + j] = g1[j];
-                }
+            store_rows(V, ld, n, n, -1.0, g0, g1, g);
             gsync(g);
             rows_times(V, w.G, ld, n, i0, i1, g0, g1);
+            rot = 0;
         }
     }
     if (ok) {
@@ -746,20 +764,11 @@ __device__ unsigned emi_inverse(int n, int ld, const HWs &w, double *V, const Gr
         ok = mx == mx && n * mx < 1.0e8;
     }
     gsync(g);
-    if (ok) {
-#pragma unroll
-        for (int j = 0; j < 32; j++)
-            if (j < n) {
-                if (i0 < n)
-                    w.G[i0 * ld + j] = g0[j];
-                if (i1 < n)
-                    w.G[i1 * ld + j] = g1[j];
-            }
-    }
-    else {
+    if (ok)
+        store_rows(w.G, ld, n, rot, rot ? -1.0 : 1.0, g0, g1, g);
+    else
         /* G still holds |T| (only registers were changed). */
         st |= TC_STATUS_EMI_PINV | jacobi_pinv16(n, ld, w.G, V, w.lam, g);
-    }
     gsync(g);
     return st;
 }
@@ -1321,7 +1330,7 @@ HalfLayout half_layout(int n, int emi)
     L.off_y = take(4 * 32);
     L.off_nrm = take(4 * 32);
     L.off_zs = take(8 * 32);
-    L.off_rs = take(emi ? 8 * 32 : 0);
+    L.off_rs = take(emi ? 8 * 64 : 0);
     L.off_lam = take(emi ? 8 * 32 : 0);
     L.off_x = take(emi ? 16 * 32 : 0);
     L.per_group = off;
