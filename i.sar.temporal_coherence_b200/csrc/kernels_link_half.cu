@@ -101,6 +101,7 @@ struct HalfLayout {
 };
 
 struct HWs {
+    int n;
     float2 *T;
     double *G;
     float4 *vw;
@@ -116,6 +117,7 @@ __device__ __forceinline__ HWs hws(unsigned char *base, const HalfLayout &L)
 {
     HWs w;
 
+    w.n = L.n;
     w.T = (float2 *)(base + L.off_T);
     w.G = (double *)(base + L.off_G);
     w.vw = (float4 *)(base + L.off_vw);
@@ -129,7 +131,7 @@ __device__ __forceinline__ HWs hws(unsigned char *base, const HalfLayout &L)
     w.nrm = (float *)(base + L.off_nrm);
     w.zs = (float2 *)(base + L.off_zs);
     w.rs = (double *)(base + L.off_rs);
-    w.lam = (double *)(base + L.off_lam);
+    w.lam = nullptr;
     w.x = (double2 *)(base + L.off_x);
     return w;
 }
@@ -723,18 +725,56 @@ __device__ unsigned jacobi_pinv16(int n, int ld, double *G, double *V, double *l
     return status;
 }
 
-/* |T|^-1 into G (shared, double), from |T| in G. Returns status bits. */
-__device__ unsigned emi_inverse(int n, int ld, const HWs &w, double *V, const Grp &g)
+/* Packed entry (i, j) of a symmetric matrix, either triangle. */
+__device__ __forceinline__ int sym_idx(int n, int i, int j)
+{
+    return i <= j ? tc_pidx(n, i, j) : tc_pidx(n, j, i);
+}
+
+/* |T| in double into w.G (packed upper triangle), from T (n <= 32); lane l
+   takes rows l and n - 1 - l, so that every lane has n + 1 entries. */
+__device__ void packed_abs_t(int n, int ld, const HWs &w, const Grp &g)
+{
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+        const int r = t ? n - 1 - g.gl : g.gl;
+
+        if (r < n && (t == 0 ? r <= n - 1 - g.gl : r > g.gl))
+            for (int j = r; j < n; j++) {
+                const float2 v = w.T[r * ld + j];
+
+                w.G[tc_pidx(n, r, j)] = hypot((double)v.x, (double)v.y);
+            }
+    }
+    gsync(g);
+}
+
+/* |T| in full into A (n x ld, global scratch), from its packed copy. */
+__device__ void full_abs_t(double *A, int n, int ld, const double *Gp, const Grp &g)
+{
+    for (int r = g.gl; r < n; r += 16)
+        for (int j = 0; j < n; j++)
+            A[r * ld + j] = Gp[sym_idx(n, r, j)];
+    gsync(g);
+}
+
+/* |T|^-1 into w.G (packed upper triangle, double), from T. The rare
+   fallback tiers work on full matrices A, V (n x ld each) and lam (n) in
+   the group's global scratch. Returns status bits. */
+__device__ unsigned emi_inverse(int n, int ld, const HWs &w, double *A, double *V, double *lam,
+                                const Grp &g)
 {
     const int i0 = g.gl, i1 = g.gl + 16;
     double g0[32], g1[32];
     unsigned st = 0;
     int rot = n;
+    bool full = false;
 
+    packed_abs_t(n, ld, w, g);
 #pragma unroll
     for (int j = 0; j < 32; j++) {
-        g0[j] = (i0 < n && j < n) ? w.G[i0 * ld + j] : 0.0;
-        g1[j] = (i1 < n && j < n) ? w.G[i1 * ld + j] : 0.0;
+        g0[j] = (i0 < n && j < n) ? w.G[sym_idx(n, i0, j)] : 0.0;
+        g1[j] = (i1 < n && j < n) ? w.G[sym_idx(n, i1, j)] : 0.0;
     }
     bool ok = sweep16(g0, g1, n, 1.0e-5, w.rs, g);
 
@@ -743,12 +783,14 @@ __device__ unsigned emi_inverse(int n, int ld, const HWs &w, double *V, const Gr
            intermediate inverse in V */
         st |= TC_STATUS_EMI_PINV;
         gsync(g);
-        rows_times(w.G, w.G, ld, n, i0, i1, g0, g1);
+        full_abs_t(A, n, ld, w.G, g);
+        full = true;
+        rows_times(A, A, ld, n, i0, i1, g0, g1);
         ok = sweep16(g0, g1, n, 1.0e-300, w.rs, g);
         if (ok) {
             store_rows(V, ld, n, n, -1.0, g0, g1, g);
             gsync(g);
-            rows_times(V, w.G, ld, n, i0, i1, g0, g1);
+            rows_times(V, A, ld, n, i0, i1, g0, g1);
             rot = 0;
         }
     }
@@ -764,11 +806,29 @@ __device__ unsigned emi_inverse(int n, int ld, const HWs &w, double *V, const Gr
         ok = mx == mx && n * mx < 1.0e8;
     }
     gsync(g);
-    if (ok)
-        store_rows(w.G, ld, n, rot, rot ? -1.0 : 1.0, g0, g1, g);
-    else
-        /* G still holds |T| (only registers were changed). */
-        st |= TC_STATUS_EMI_PINV | jacobi_pinv16(n, ld, w.G, V, w.lam, g);
+    if (ok) {
+        const double sc = rot ? -1.0 : 1.0;
+
+#pragma unroll
+        for (int p = 0; p < 32; p++) {
+            const int j = (p + rot) & 31;
+
+            if (j < n) {
+                if (i0 <= j)
+                    w.G[tc_pidx(n, i0, j)] = sc * g0[p];
+                if (i1 <= j)
+                    w.G[tc_pidx(n, i1, j)] = sc * g1[p];
+            }
+        }
+    }
+    else {
+        if (!full)
+            full_abs_t(A, n, ld, w.G, g);
+        st |= TC_STATUS_EMI_PINV | jacobi_pinv16(n, ld, A, V, lam, g);
+        for (int r = g.gl; r < n; r += 16)
+            for (int j = r; j < n; j++)
+                w.G[tc_pidx(n, r, j)] = A[r * ld + j];
+    }
     gsync(g);
     return st;
 }
@@ -776,7 +836,7 @@ __device__ unsigned emi_inverse(int n, int ld, const HWs &w, double *V, const Gr
 /* M_ij = inv_ij T_ij (double) */
 __device__ __forceinline__ double2 mval(const HWs &w, int ld, int i, int j)
 {
-    const double gg = w.G[i * ld + j];
+    const double gg = w.G[sym_idx(w.n, i, j)];
     const float2 t = w.T[i < j ? i * ld + j : j * ld + i];
 
     return make_double2(gg * (double)t.x, i < j ? gg * (double)t.y : -gg * (double)t.y);
@@ -1136,7 +1196,7 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
     const HWs w = hws(smem + (size_t)grp * L.per_group, L);
     const int n = s.n, ld = L.ld;
     const long long plane = (long long)s.rows * s.cols;
-    double *V = scratch + ((size_t)blockIdx.x * wpb * 2 + grp) * (size_t)n * ld;
+    double *V = scratch + ((size_t)blockIdx.x * wpb * 2 + grp) * (size_t)(2 * n * ld + 32);
     const int i0 = g.gl, i1 = g.gl + 16;
 
     /* The warps of a CTA take pixel pairs qb + warp and run each stage
@@ -1231,16 +1291,8 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
         }
         else {
             /* stage 2: |T|^-1 in double */
-            if (run) {
-                for (int r = g.gl; r < n; r += 16)
-                    for (int j = 0; j < n; j++) {
-                        const float2 t = w.T[r * ld + j];
-
-                        w.G[r * ld + j] = hypot((double)t.x, (double)t.y);
-                    }
-                gsync(g);
-                st |= emi_inverse(n, ld, w, V, g);
-            }
+            if (run)
+                st |= emi_inverse(n, ld, w, V, V + n * ld, V + 2 * n * ld, g);
             __syncthreads();
             /* stage 3: M = |T|^-1 o T in float rows, Householder reduction */
             if (run) {
@@ -1319,8 +1371,12 @@ HalfLayout half_layout(int n, int emi)
     L.n = n;
     L.ld = n | 1;
     L.off_T = take(8 * n * L.ld);
-    L.off_G = take(emi ? 8 * n * L.ld : 0);
+    L.off_G = take(emi ? 8 * tc_npu(n) : 0);
+    /* stage-local: the sweep's pivot rows (inverse), the Householder
+       vectors (reduction) and the refinement vectors share one region */
     L.off_vw = take(16 * 64);
+    L.off_rs = L.off_vw;
+    L.off_x = L.off_vw;
     L.off_lu = take(16 * 32);
     L.off_tau = take(8 * 32);
     L.off_d = take(4 * 32);
@@ -1330,9 +1386,7 @@ HalfLayout half_layout(int n, int emi)
     L.off_y = take(4 * 32);
     L.off_nrm = take(4 * 32);
     L.off_zs = take(8 * 32);
-    L.off_rs = take(emi ? 8 * 64 : 0);
-    L.off_lam = take(emi ? 8 * 32 : 0);
-    L.off_x = take(emi ? 16 * 32 : 0);
+    L.off_lam = 0;
     L.per_group = off;
     return L;
 }
@@ -1341,9 +1395,12 @@ HalfLayout half_layout(int n, int emi)
 
 size_t tc_link_half_scratch_bytes(int n, int sms)
 {
-    /* Per group (two per warp, at most 12 warps per CTA, one CTA per SM):
-       the Jacobi eigenvectors of |T|. */
-    return (size_t)sms * 24 * n * (n | 1) * sizeof(double);
+    /* EMI only, per group (two per warp, at most 8 warps per CTA, one CTA
+       per SM): |T|, the Jacobi eigenvectors and eigenvalues of the fallback
+       tiers. Stacks of more than 32 dates take the shared-memory kernel. */
+    if (n > 32)
+        return 256;
+    return (size_t)sms * 16 * (2 * n * (n | 1) + 32) * sizeof(double);
 }
 
 cudaError_t tc_launch_link_half(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
@@ -1355,7 +1412,7 @@ cudaError_t tc_launch_link_half(const TcStrip &s, const TcChunk &c, const TcLink
     const HalfLayout L = half_layout(s.n, k.emi);
     const size_t per_warp = 2 * (size_t)L.per_group;
     const int max_warps = k.emi ? 8 : 12;
-    int wpb = (int)((200 * 1024) / per_warp);
+    int wpb = (int)((227 * 1024) / per_warp);
 
     if (wpb > max_warps)
         wpb = max_warps;
