@@ -476,13 +476,15 @@ __device__ __forceinline__ void tri_solve(float (&yr)[32], int n, unsigned long 
    returns the components of rows i0, i1 in z0, z1; y (tridiagonal vector)
    is left in yr. */
 __device__ unsigned eigvec(int n, int index, const HWs &w, int ld, const Grp &g, float2 &z0,
-                           float2 &z1, float (&yr)[32], float &lambda, float &norm)
+                           float2 &z1, float (&yr)[32], float &lambda, float &norm,
+                           unsigned long long &piv)
 {
     unsigned status = 0;
 
     lambda = tri_eigenvalue(n, index, w, g, norm, status);
     const float tiny = 1.0e-6f * fmaxf(norm, 1.0e-30f);
-    const unsigned long long piv = tri_lu<float>(n, lambda, tiny, w, g);
+
+    piv = tri_lu<float>(n, lambda, tiny, w, g);
 
 #pragma unroll
     for (int k = 0; k < 32; k++)
@@ -844,9 +846,12 @@ __device__ __forceinline__ double2 mval(const HWs &w, int ld, int i, int j)
 
 /* One refinement step of the eigenpair of M for the eigenvector (z0, z1)
    of rows (i0, i1): see the file comment. tri and Q are the float
-   reduction of M; y is the tridiagonal eigenvector. */
+   reduction of M; y is the tridiagonal eigenvector. The residual is formed
+   in double; the correction, a small vector that needs only float relative
+   accuracy, is mapped through Q in float after scaling the residual to a
+   unit maximum. */
 __device__ void refine(int n, int ld, const HWs &w, const Grp &g, double2 &x0, double2 &x1,
-                       const float (&yr)[32], unsigned long long piv, bool do_solve)
+                       const float (&yr)[32], unsigned long long piv)
 {
     const int i0 = g.gl, i1 = g.gl + 16;
 
@@ -885,16 +890,24 @@ __device__ void refine(int n, int ld, const HWs &w, const Grp &g, double2 &x0, d
     double mu = x0.x * u0.x + x0.y * u0.y + x1.x * u1.x + x1.y * u1.y;
 
     mu = gsum(mu, g);
-    if (!do_solve)
-        return;
-    /* r = u - mu x; b = Q^H r = H_{n-2} .. H_0 r */
-    double2 b0 = make_double2(u0.x - mu * x0.x, u0.y - mu * x0.y);
-    double2 b1 = make_double2(u1.x - mu * x1.x, u1.y - mu * x1.y);
+    /* r = u - mu x, scaled to a unit maximum */
+    double2 r0 = make_double2(u0.x - mu * x0.x, u0.y - mu * x0.y);
+    double2 r1 = make_double2(u1.x - mu * x1.x, u1.y - mu * x1.y);
 
     if (i0 >= n)
-        b0 = make_double2(0.0, 0.0);
+        r0 = make_double2(0.0, 0.0);
     if (i1 >= n)
-        b1 = make_double2(0.0, 0.0);
+        r1 = make_double2(0.0, 0.0);
+    const double rmax = gmaxd(fmax(fmax(fabs(r0.x), fabs(r0.y)), fmax(fabs(r1.x), fabs(r1.y))), g);
+
+    gsync(g);
+    if (!(rmax > 0.0))
+        return;
+    const double sc = 1.0 / rmax;
+    /* b = Q^H r = H_{n-2} .. H_0 r */
+    float2 b0 = make_float2((float)(r0.x * sc), (float)(r0.y * sc));
+    float2 b1 = make_float2((float)(r1.x * sc), (float)(r1.y * sc));
+
     for (int k = 0; k < n - 1; k++) {
         const float2 ta = w.tau[k];
 
@@ -902,69 +915,69 @@ __device__ void refine(int n, int ld, const HWs &w, const Grp &g, double2 &x0, d
             continue;
         const float2 v0 = i0 > k && i0 < n ? w.T[i0 * ld + k] : make_float2(0.f, 0.f);
         const float2 v1 = i1 > k && i1 < n ? w.T[i1 * ld + k] : make_float2(0.f, 0.f);
-        double sr = (double)v0.x * b0.x + (double)v0.y * b0.y + (double)v1.x * b1.x +
-                    (double)v1.y * b1.y;
-        double si = (double)v0.x * b0.y - (double)v0.y * b0.x + (double)v1.x * b1.y -
-                    (double)v1.y * b1.x;
+        float sr = v0.x * b0.x + v0.y * b0.y + v1.x * b1.x + v1.y * b1.y;
+        float si = v0.x * b0.y - v0.y * b0.x + v1.x * b1.y - v1.y * b1.x;
 
         sr = gsum(sr, g);
         si = gsum(si, g);
         /* H^H b = b - conj(tau) v (v^H b) */
-        const double hr = (double)ta.x * sr + (double)ta.y * si;
-        const double hi = (double)ta.x * si - (double)ta.y * sr;
+        const float hr = ta.x * sr + ta.y * si;
+        const float hi = ta.x * si - ta.y * sr;
 
-        b0.x -= (double)v0.x * hr - (double)v0.y * hi;
-        b0.y -= (double)v0.x * hi + (double)v0.y * hr;
-        b1.x -= (double)v1.x * hr - (double)v1.y * hi;
-        b1.y -= (double)v1.x * hi + (double)v1.y * hr;
+        b0.x -= v0.x * hr - v0.y * hi;
+        b0.y -= v0.x * hi + v0.y * hr;
+        b1.x -= v1.x * hr - v1.y * hi;
+        b1.y -= v1.x * hi + v1.y * hr;
     }
-    /* b is real-tridiagonal space but complex-valued: solve the real and
-       imaginary parts with the float LU of (tri - lambda), off y. */
-    w.x[i0] = b0;
-    w.x[i1] = b1;
+    /* b is in the real-tridiagonal basis but complex-valued: solve the real
+       and imaginary parts with the float LU of (tri - lambda), off y. */
+    float2 *bs = (float2 *)w.x;
+
+    bs[i0] = b0;
+    bs[i1] = b1;
     gsync(g);
     float tr_[32], ti_[32];
-    double ynrm = 0.0, cr = 0.0, ci = 0.0;
+    float ynrm = 0.f, cr = 0.f, ci = 0.f;
 
 #pragma unroll
     for (int k = 0; k < 32; k++) {
-        const double2 bk = k < n ? w.x[k] : make_double2(0.0, 0.0);
+        const float2 bk = k < n ? bs[k] : make_float2(0.f, 0.f);
 
-        ynrm += (double)yr[k] * yr[k];
-        cr += (double)yr[k] * bk.x;
-        ci += (double)yr[k] * bk.y;
-        tr_[k] = (float)bk.x;
-        ti_[k] = (float)bk.y;
+        ynrm = fmaf(yr[k], yr[k], ynrm);
+        cr = fmaf(yr[k], bk.x, cr);
+        ci = fmaf(yr[k], bk.y, ci);
+        tr_[k] = bk.x;
+        ti_[k] = bk.y;
     }
     cr /= ynrm;
     ci /= ynrm;
 #pragma unroll
     for (int k = 0; k < 32; k++) {
-        tr_[k] -= (float)(cr * yr[k]);
-        ti_[k] -= (float)(ci * yr[k]);
+        tr_[k] = fmaf(-cr, yr[k], tr_[k]);
+        ti_[k] = fmaf(-ci, yr[k], ti_[k]);
     }
     tri_solve(tr_, n, piv, w);
     tri_solve(ti_, n, piv, w);
-    double dr = 0.0, di = 0.0;
+    float dr = 0.f, di = 0.f;
 
 #pragma unroll
     for (int k = 0; k < 32; k++)
         if (k < n) {
-            dr += (double)yr[k] * tr_[k];
-            di += (double)yr[k] * ti_[k];
+            dr = fmaf(yr[k], tr_[k], dr);
+            di = fmaf(yr[k], ti_[k], di);
         }
     dr /= ynrm;
     di /= ynrm;
-    double2 t0 = make_double2(0.0, 0.0), t1 = t0;
+    float2 t0 = make_float2(0.f, 0.f), t1 = t0;
 
 #pragma unroll
     for (int k = 0; k < 32; k++) {
         if (k == i0 && k < n)
-            t0 = make_double2(tr_[k] - dr * yr[k], ti_[k] - di * yr[k]);
+            t0 = make_float2(fmaf(-dr, yr[k], tr_[k]), fmaf(-di, yr[k], ti_[k]));
         if (k == i1 && k < n)
-            t1 = make_double2(tr_[k] - dr * yr[k], ti_[k] - di * yr[k]);
+            t1 = make_float2(fmaf(-dr, yr[k], tr_[k]), fmaf(-di, yr[k], ti_[k]));
     }
-    /* d = Q t = H_0 .. H_{n-2} t; x -= d */
+    /* d = Q t = H_0 .. H_{n-2} t; x -= d / sc */
     for (int k = n - 2; k >= 0; k--) {
         const float2 ta = w.tau[k];
 
@@ -972,25 +985,23 @@ __device__ void refine(int n, int ld, const HWs &w, const Grp &g, double2 &x0, d
             continue;
         const float2 v0 = i0 > k && i0 < n ? w.T[i0 * ld + k] : make_float2(0.f, 0.f);
         const float2 v1 = i1 > k && i1 < n ? w.T[i1 * ld + k] : make_float2(0.f, 0.f);
-        double sr = (double)v0.x * t0.x + (double)v0.y * t0.y + (double)v1.x * t1.x +
-                    (double)v1.y * t1.y;
-        double si = (double)v0.x * t0.y - (double)v0.y * t0.x + (double)v1.x * t1.y -
-                    (double)v1.y * t1.x;
+        float sr = v0.x * t0.x + v0.y * t0.y + v1.x * t1.x + v1.y * t1.y;
+        float si = v0.x * t0.y - v0.y * t0.x + v1.x * t1.y - v1.y * t1.x;
 
         sr = gsum(sr, g);
         si = gsum(si, g);
-        const double hr = (double)ta.x * sr - (double)ta.y * si;
-        const double hi = (double)ta.x * si + (double)ta.y * sr;
+        const float hr = ta.x * sr - ta.y * si;
+        const float hi = ta.x * si + ta.y * sr;
 
-        t0.x -= (double)v0.x * hr - (double)v0.y * hi;
-        t0.y -= (double)v0.x * hi + (double)v0.y * hr;
-        t1.x -= (double)v1.x * hr - (double)v1.y * hi;
-        t1.y -= (double)v1.x * hi + (double)v1.y * hr;
+        t0.x -= v0.x * hr - v0.y * hi;
+        t0.y -= v0.x * hi + v0.y * hr;
+        t1.x -= v1.x * hr - v1.y * hi;
+        t1.y -= v1.x * hi + v1.y * hr;
     }
-    x0.x -= t0.x;
-    x0.y -= t0.y;
-    x1.x -= t1.x;
-    x1.y -= t1.y;
+    x0.x -= rmax * t0.x;
+    x0.y -= rmax * t0.y;
+    x1.x -= rmax * t1.x;
+    x1.y -= rmax * t1.y;
     gsync(g);
 }
 
@@ -1283,7 +1294,9 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
             __syncthreads();
             /* stage 3: its dominant eigenvector */
             if (run) {
-                st |= eigvec(n, n - 1, w, ld, g, f0, f1, yr, lambda, norm);
+                unsigned long long piv;
+
+                st |= eigvec(n, n - 1, w, ld, g, f0, f1, yr, lambda, norm, piv);
                 z0 = make_double2(f0.x, f0.y);
                 z1 = make_double2(f1.x, f1.y);
             }
@@ -1321,13 +1334,12 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
             __syncthreads();
             /* stage 4: eigenvector of the smallest eigenvalue, refined */
             if (run) {
-                st |= eigvec(n, 0, w, ld, g, f0, f1, yr, lambda, norm);
-                const unsigned long long piv =
-                    tri_lu<float>(n, lambda, 1.0e-6f * fmaxf(norm, 1.0e-30f), w, g);
+                unsigned long long piv;
 
+                st |= eigvec(n, 0, w, ld, g, f0, f1, yr, lambda, norm, piv);
                 z0 = make_double2(f0.x, f0.y);
                 z1 = make_double2(f1.x, f1.y);
-                refine(n, ld, w, g, z0, z1, yr, piv, true);
+                refine(n, ld, w, g, z0, z1, yr, piv);
             }
             __syncthreads();
         }
