@@ -38,6 +38,8 @@ EXPORTS = (
     "tc_last_error", "tc_set_fatal_handler", "tc_shp_constants", "tc_device_count",
     "tc_open", "tc_run_ex", "tc_run_device", "tc_set_timing", "tc_stage_stats",
     "tc_close", "tc_fp32_peak", "tc_run_device_static", "tc_get_options",
+    "tc_geometry_grid_shape", "tc_geometry_init", "tc_set_geometry", "tc_run_raw",
+    "tc_run_raw_device",
 )
 
 
@@ -79,6 +81,67 @@ class Options(ctypes.Structure):
     ]
 
 
+class Orbit(ctypes.Structure):
+    """struct tc_orbit: one date's state vectors (orbit.c:52-57)."""
+
+    _fields_ = [("n", ctypes.c_int), ("t", ctypes.c_void_p), ("pos", ctypes.c_void_p),
+                ("vel", ctypes.c_void_p)]
+
+
+class Geometry(ctypes.Structure):
+    """struct tc_geometry: raster timing of the reference date and the
+    region (geometry.c:161-216)."""
+
+    _fields_ = [
+        ("ndates", ctypes.c_int), ("ref", ctypes.c_int),
+        ("first_line_time", ctypes.c_double), ("azimuth_time_interval", ctypes.c_double),
+        ("slant_range_time", ctypes.c_double), ("range_sampling_rate", ctypes.c_double),
+        ("wavelength", ctypes.c_double), ("line0", ctypes.c_double), ("sample0", ctypes.c_double),
+        ("rows", ctypes.c_int), ("cols", ctypes.c_int),
+        ("hmin", ctypes.c_double), ("hmax", ctypes.c_double), ("h0", ctypes.c_double),
+    ]
+
+
+def make_geometry(ndates, ref, rows, cols, first_line_time, azimuth_time_interval,
+                  slant_range_time, range_sampling_rate, wavelength, line0=0.0, sample0=0.0,
+                  heights=None, h0=0.0):
+    """struct tc_geometry; the height range is that of `heights` (an
+    elevation map, NaN ignored) or h0 (main.c:684-709)."""
+    if heights is not None:
+        h = np.asarray(heights, np.float64)
+        hmin, hmax = float(np.nanmin(h)), float(np.nanmax(h))
+    else:
+        hmin = hmax = float(h0)
+    return Geometry(ndates, ref, first_line_time, azimuth_time_interval, slant_range_time,
+                    range_sampling_rate, wavelength, line0, sample0, rows, cols, hmin, hmax, h0)
+
+
+def _orbit_array(orbits):
+    keep, arr = [], (Orbit * len(orbits))()
+    for k, (t, pos, vel) in enumerate(orbits):
+        t = np.ascontiguousarray(t, np.float64)
+        pos = np.ascontiguousarray(pos, np.float64)
+        vel = np.ascontiguousarray(vel, np.float64)
+        keep += [t, pos, vel]
+        arr[k] = Orbit(len(t), t.ctypes.data, pos.ctypes.data, vel.ctypes.data)
+    return arr, keep
+
+
+def geometry_grid(geometry, orbits):
+    """tc_geometry_init: the flat-earth / topographic phase grid
+    [grid_rows][grid_cols][nheights][ndates] (float64), computed in double
+    precision on the current device. orbits: per date (t, pos, vel)."""
+    gr, gc, nh = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    hs = (ctypes.c_double * 3)()
+    _check(library().tc_geometry_grid_shape(ctypes.byref(geometry), ctypes.byref(gr),
+                                            ctypes.byref(gc), ctypes.byref(nh), hs))
+    grid = np.empty((gr.value, gc.value, nh.value, geometry.ndates), np.float64)
+    arr, keep = _orbit_array(orbits)
+    _check(library().tc_geometry_init(ctypes.byref(geometry), arr, grid.ctypes.data))
+    del keep
+    return grid
+
+
 _lib = None
 
 
@@ -103,6 +166,11 @@ def library():
         lib.tc_stage_stats.argtypes = [vp, vp, vp, i]
         lib.tc_close.argtypes = [vp]
         lib.tc_get_options.argtypes = [vp, ctypes.POINTER(Options)]
+        lib.tc_geometry_grid_shape.argtypes = [ctypes.POINTER(Geometry), vp, vp, vp, vp]
+        lib.tc_geometry_init.argtypes = [ctypes.POINTER(Geometry), vp, vp]
+        lib.tc_set_geometry.argtypes = [vp, ctypes.POINTER(Geometry), vp]
+        lib.tc_run_raw.argtypes = [vp, vp, vp, vp, i, i, i, i, i, vp, vp, vp, vp, vp]
+        lib.tc_run_raw_device.argtypes = [vp, vp, vp, vp, i, i, i, i, i, vp, vp, vp, vp, vp, vp]
         lib.tc_fp32_peak.argtypes = [i, ctypes.POINTER(ctypes.c_double)]
         lib.tc_run_device_static.argtypes = [ctypes.POINTER(Settings), i, vp, vp, vp, i, i, i,
                                              vp, vp, vp, vp, vp, vp]
@@ -259,6 +327,15 @@ class Backend:
         amp = np.ascontiguousarray(amp, np.float32)
         valid = np.ascontiguousarray(valid, np.uint8)
         padded_rows = amp.shape[0]
+        out = self._outputs(rows, cols, phases, status, out)
+        _check(library().tc_run_ex(
+            self.handle, _ptr(slc), _ptr(amp), _ptr(valid), padded_rows, rows, cols,
+            _ptr(out["coh"]), _ptr(out["count"]), _ptr(out.get("pairs")),
+            _ptr(out.get("phases")), _ptr(out.get("status")),
+        ))
+        return out
+
+    def _outputs(self, rows, cols, phases, status, out):
         out = dict(out or {})
         out.setdefault("coh", np.empty((rows, cols), np.float32))
         out.setdefault("count", np.empty((rows, cols), np.int32))
@@ -268,11 +345,6 @@ class Backend:
             out.setdefault("phases", np.empty((rows, cols, self.n), np.float32))
         if status:
             out.setdefault("status", np.empty((rows, cols), np.uint8))
-        _check(library().tc_run_ex(
-            self.handle, _ptr(slc), _ptr(amp), _ptr(valid), padded_rows, rows, cols,
-            _ptr(out["coh"]), _ptr(out["count"]), _ptr(out.get("pairs")),
-            _ptr(out.get("phases")), _ptr(out.get("status")),
-        ))
         return out
 
     def run_device(self, slc, amp, valid, rows, cols, coh, count, pairs=None, phases=None,
@@ -299,18 +371,60 @@ class Backend:
         library().tc_stage_stats(self.handle, ms, nl, 5)
         return {name: (ms[i], nl[i]) for i, name in enumerate(STAGES)}
 
+    def set_geometry(self, geometry, grid):
+        """tc_set_geometry: attach a phase grid (geometry_grid) for run_raw;
+        None detaches it."""
+        if grid is None:
+            _check(library().tc_set_geometry(self.handle, None, None))
+            self._grid = None
+            return
+        self._grid = np.ascontiguousarray(grid, np.float64)
+        _check(library().tc_set_geometry(self.handle, ctypes.byref(geometry),
+                                         self._grid.ctypes.data))
+
+    def run_raw(self, re, im, elevation, row0, region_rows, rows, cols, phases=False,
+                status=False, out=None):
+        """tc_run_raw: one strip from raw I/Q rows re, im (N, padded_rows,
+        cols) of region rows row0 .., elevation (padded_rows, cols) or None;
+        the strip preparation (validity, sorted amplitudes, geometric phase)
+        runs on the device. Returns the outputs as run() does."""
+        re = np.ascontiguousarray(re, np.float32)
+        im = np.ascontiguousarray(im, np.float32)
+        elev = None if elevation is None else np.ascontiguousarray(elevation, np.float64)
+        padded_rows = re.shape[1]
+        out = self._outputs(rows, cols, phases, status, out)
+        _check(library().tc_run_raw(
+            self.handle, re.ctypes.data, im.ctypes.data, _ptr(elev), row0, region_rows,
+            padded_rows, rows, cols, _ptr(out["coh"]), _ptr(out["count"]), _ptr(out.get("pairs")),
+            _ptr(out.get("phases")), _ptr(out.get("status"))))
+        return out
+
+    def run_raw_device(self, re, im, elevation, row0, region_rows, rows, cols, coh, count,
+                       pairs=None, phases=None, status=None, stream=None):
+        """tc_run_raw_device: run_raw on CUDA tensors, asynchronously."""
+        if stream is not None and hasattr(stream, "cuda_stream"):
+            stream = stream.cuda_stream
+        _check(library().tc_run_raw_device(
+            self.handle, _ptr(re), _ptr(im), _ptr(elevation), row0, region_rows, re.shape[1],
+            rows, cols, _ptr(coh), _ptr(count), _ptr(pairs), _ptr(phases), _ptr(status),
+            ctypes.c_void_p(int(stream or 0))))
+
 
 def temporal_coherence(stack, window=(21, 7), shp_test="ks", alpha=0.05, min_shp=20,
                        estimator="evd", bias_correction=False, pairs=False,
                        pairs_mode="consecutive", phase=None, elevation=None, memory=300,
                        device=-1, gram=None, split_terms=3, with_phases=False,
-                       with_status=False, backend=None):
+                       with_status=False, backend=None, geometry=None, orbits=None):
     """Temporal coherence of a stack (N, rows, cols) complex, NaN = NULL, by
     the module's strip loop (main.c:724-825) over the B200 backend.
 
     phase: optional (N, rows, cols) geometric phase to remove (radians,
     date k is multiplied by exp(i phase_k)); elevation: optional (rows, cols)
-    heights whose NaN cells are invalid. Returns (coh, count) with NaN / -1
+    heights whose NaN cells are invalid. geometry (make_geometry) and orbits
+    (per date (t, pos, vel)) instead of phase: the flat-earth / topographic
+    phase is computed from the orbits (tc_geometry_init) and removed on the
+    device at each cell's elevation (else geometry.h0), main.c:655-712.
+    Returns (coh, count) with NaN / -1
     for NULL, plus pairs (npairs, rows, cols) when `pairs`, and phases /
     status arrays when asked, in a dict.
     """
@@ -333,12 +447,33 @@ def temporal_coherence(stack, window=(21, 7), shp_test="ks", alpha=0.05, min_shp
         pl = np.empty((s.npairs, nrows, ncols), np.float32) if s.npairs else None
         ph = np.empty((nrows, ncols, n), np.float32) if with_phases else None
         stt = np.empty((nrows, ncols), np.uint8) if with_status else None
+        raw = geometry is not None
+        if raw:
+            if phase is not None:
+                raise ValueError("give either phase or geometry and orbits")
+            be.set_geometry(geometry, geometry_grid(geometry, orbits))
+            elev = None if elevation is None else np.asarray(elevation, np.float64)
         for row0 in range(0, nrows, strip_rows):
             rows = min(strip_rows, nrows - row0)
             padded_rows = rows + 2 * halo_az
-            slc, amp, valid = read_strip(re, im, row0 - halo_az, padded_rows, halo_rg,
-                                         phase=phase, elevation=elevation)
-            r = be.run(slc, amp, valid, rows, ncols, phases=with_phases, status=with_status)
+            if raw:
+                lo, hi = max(row0 - halo_az, 0), min(row0 - halo_az + padded_rows, nrows)
+                rre = np.zeros((n, padded_rows, ncols), np.float32)
+                rim = np.zeros((n, padded_rows, ncols), np.float32)
+                off = lo - (row0 - halo_az)
+                rre[:, off:off + hi - lo] = re[:, lo:hi]
+                rim[:, off:off + hi - lo] = im[:, lo:hi]
+                rel = None
+                if elev is not None:
+                    rel = np.zeros((padded_rows, ncols))
+                    rel[off:off + hi - lo] = elev[lo:hi]
+                r = be.run_raw(rre, rim, rel, row0 - halo_az, nrows, rows, ncols,
+                               phases=with_phases, status=with_status)
+            else:
+                slc, amp, valid = read_strip(re, im, row0 - halo_az, padded_rows, halo_rg,
+                                             phase=phase, elevation=elevation)
+                r = be.run(slc, amp, valid, rows, ncols, phases=with_phases,
+                           status=with_status)
             coh[row0:row0 + rows] = r["coh"]
             count[row0:row0 + rows] = r["count"]
             if s.npairs:

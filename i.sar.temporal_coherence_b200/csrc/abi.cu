@@ -228,6 +228,9 @@ struct ocl {
     cudaStream_t stream;
     DevBuf slc, amp, valid, coh, count, pairs, phases, status;
     DevBuf soa, logstat, mask, gram, upper_tab, pair_tab, link_scratch;
+    DevBuf raw_re, raw_im, raw_elev, geo_grid;
+    bool has_geo;
+    TcGeo geo;
     bool timing;
     float stage_ms[ST_COUNT];
     int stage_launches[ST_COUNT];
@@ -294,7 +297,8 @@ static void free_bufs(struct ocl *o)
 {
     DevBuf *b[] = {&o->slc, &o->amp, &o->valid, &o->coh, &o->count, &o->pairs,
                    &o->phases, &o->status, &o->soa, &o->logstat, &o->mask, &o->gram,
-                   &o->upper_tab, &o->pair_tab, &o->link_scratch};
+                   &o->upper_tab, &o->pair_tab, &o->link_scratch, &o->raw_re, &o->raw_im,
+                   &o->raw_elev, &o->geo_grid};
 
     for (size_t i = 0; i < sizeof(b) / sizeof(b[0]); i++)
         if (b[i]->p) {
@@ -374,6 +378,7 @@ TC_API int tc_open(int device, const struct settings *s, int padded_cols,
     }
     o->gram_block = tc_gram_block_for(o->n);
     o->timing = false;
+    o->has_geo = false;
     memset(o->stage_ms, 0, sizeof(o->stage_ms));
     memset(o->stage_launches, 0, sizeof(o->stage_launches));
 
@@ -659,6 +664,66 @@ TC_API int tc_run_device(struct ocl *o, const float *slc, const float *amp,
     return rc;
 }
 
+/* Outputs of a run on the context's device buffers, back to the host. */
+static int fetch(struct ocl *o, size_t nout, float *coh, int *count, float *pairs, float *phases,
+                 unsigned char *status, Timer &tm)
+{
+    cudaStream_t st = o->stream;
+    const int t = tm.begin(ST_COPY);
+
+    CK(cudaMemcpyAsync(coh, o->coh.p, nout * sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(count, o->count.p, nout * sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (o->npairs && pairs)
+        CK(cudaMemcpyAsync(pairs, o->pairs.p, o->npairs * nout * sizeof(float),
+                           cudaMemcpyDeviceToHost, st));
+    if (phases)
+        CK(cudaMemcpyAsync(phases, o->phases.p, nout * o->n * sizeof(float),
+                           cudaMemcpyDeviceToHost, st));
+    if (status)
+        CK(cudaMemcpyAsync(status, o->status.p, nout, cudaMemcpyDeviceToHost, st));
+    tm.end(t);
+    CK(cudaStreamSynchronize(st));
+    tm.collect();
+    if (o->opt.gram == TC_GRAM_TENSOR && tc_gram_tensor_fault() > 0)
+        return set_error(TC_ERR_DEVICE, "tensor-core Gram: a wait for MMA completion ran out; "
+                         "the tiles concerned are NULL");
+    return TC_OK;
+}
+
+/* Device output buffers of the context for a strip of nout pixels. */
+static int ensure_outputs(struct ocl *o, size_t nout, bool phases, bool status)
+{
+    CK(ensure(o->coh, nout * sizeof(float)));
+    CK(ensure(o->count, nout * sizeof(int)));
+    if (o->npairs)
+        CK(ensure(o->pairs, o->npairs * nout * sizeof(float)));
+    if (phases)
+        CK(ensure(o->phases, nout * o->n * sizeof(float)));
+    if (status)
+        CK(ensure(o->status, nout));
+    return TC_OK;
+}
+
+static int run_context_buffers(struct ocl *o, int padded_rows, int rows, int cols, float *coh,
+                               int *count, float *pairs, float *phases, unsigned char *status,
+                               Timer &tm)
+{
+    const size_t nout = (size_t)rows * cols;
+    int rc = run_device(o, (const float *)o->slc.p, (const float *)o->amp.p,
+                        (const unsigned char *)o->valid.p, padded_rows, rows, cols,
+                        (float *)o->coh.p, (int *)o->count.p,
+                        o->npairs ? (float *)o->pairs.p : nullptr,
+                        phases ? (float *)o->phases.p : nullptr,
+                        status ? (unsigned char *)o->status.p : nullptr, o->stream, tm);
+
+    if (rc != TC_OK) {
+        cudaStreamSynchronize(o->stream);
+        tm.collect();
+        return rc;
+    }
+    return fetch(o, nout, coh, count, pairs, phases, status, tm);
+}
+
 TC_API int tc_run_ex(struct ocl *o, const float *slc, const float *amp,
                      const unsigned char *valid, int padded_rows, int rows, int cols,
                      float *coh, int *count, float *pairs, float *phases,
@@ -675,7 +740,6 @@ TC_API int tc_run_ex(struct ocl *o, const float *slc, const float *amp,
                          rows, cols, padded_rows, o->padded_cols, o->wa, o->wr);
     CK(cudaSetDevice(o->device));
     const size_t npad = (size_t)padded_rows * o->padded_cols;
-    const size_t nout = (size_t)rows * cols;
     const size_t n = o->n;
     cudaStream_t st = o->stream;
     Timer tm(o, st);
@@ -685,51 +749,192 @@ TC_API int tc_run_ex(struct ocl *o, const float *slc, const float *amp,
     CK(ensure(o->slc, npad * n * 2 * sizeof(float)));
     CK(ensure(o->amp, npad * n * sizeof(float)));
     CK(ensure(o->valid, npad));
-    CK(ensure(o->coh, nout * sizeof(float)));
-    CK(ensure(o->count, nout * sizeof(int)));
-    if (o->npairs)
-        CK(ensure(o->pairs, o->npairs * nout * sizeof(float)));
-    if (phases)
-        CK(ensure(o->phases, nout * n * sizeof(float)));
-    if (status)
-        CK(ensure(o->status, nout));
+    int rc = ensure_outputs(o, (size_t)rows * cols, phases != nullptr, status != nullptr);
 
+    if (rc != TC_OK)
+        return rc;
     int t = tm.begin(ST_COPY);
 
     CK(cudaMemcpyAsync(o->slc.p, slc, npad * n * 2 * sizeof(float), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(o->amp.p, amp, npad * n * sizeof(float), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(o->valid.p, valid, npad, cudaMemcpyHostToDevice, st));
     tm.end(t);
-    int rc = run_device(o, (const float *)o->slc.p, (const float *)o->amp.p,
-                        (const unsigned char *)o->valid.p, padded_rows, rows, cols,
-                        (float *)o->coh.p, (int *)o->count.p,
-                        o->npairs ? (float *)o->pairs.p : nullptr,
-                        phases ? (float *)o->phases.p : nullptr,
-                        status ? (unsigned char *)o->status.p : nullptr, st, tm);
+    return run_context_buffers(o, padded_rows, rows, cols, coh, count, pairs, phases, status, tm);
+}
 
-    if (rc != TC_OK) {
+/* ------------------------------------------------------------------ */
+/* Geometry and raw strips.                                            */
+/* ------------------------------------------------------------------ */
+
+TC_API int tc_geometry_grid_shape(const struct tc_geometry *g, int *grid_rows, int *grid_cols,
+                                  int *nheights, double *heights)
+{
+    TcGeo d;
+    int rc;
+
+    if (!g)
+        return set_error(TC_ERR_ARG, "no geometry");
+    if ((rc = tc_geometry_shape(*g, d)) != TC_OK)
+        return rc;
+    if (grid_rows)
+        *grid_rows = d.grid_rows;
+    if (grid_cols)
+        *grid_cols = d.grid_cols;
+    if (nheights)
+        *nheights = d.nheights;
+    if (heights)
+        for (int i = 0; i < 3; i++)
+            heights[i] = d.heights[i];
+    return TC_OK;
+}
+
+TC_API int tc_geometry_init(const struct tc_geometry *g, const struct tc_orbit *orbits,
+                            double *grid)
+{
+    TcGeo d;
+    int rc;
+    cudaStream_t st;
+
+    if (!g || !orbits || !grid)
+        return set_error(TC_ERR_ARG, "no geometry, orbits or grid");
+    if ((rc = tc_geometry_shape(*g, d)) != TC_OK)
+        return rc;
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    rc = tc_geometry_grid(d, orbits, grid, st);
+    cudaStreamDestroy(st);
+    return rc;
+}
+
+TC_API int tc_set_geometry(struct ocl *o, const struct tc_geometry *g, const double *grid)
+{
+    if (!o)
+        return set_error(TC_ERR_ARG, "no context");
+    if (!g || !grid) {
+        o->has_geo = false;
+        return TC_OK;
+    }
+    TcGeo d;
+    int rc;
+
+    if ((rc = tc_geometry_shape(*g, d)) != TC_OK)
+        return rc;
+    if (d.ndates != o->n)
+        return set_error(TC_ERR_ARG, "geometry of %d dates for a context of %d", d.ndates, o->n);
+    const size_t bytes = (size_t)d.grid_rows * d.grid_cols * d.nheights * d.ndates * sizeof(double);
+
+    CK(cudaSetDevice(o->device));
+    CK(ensure(o->geo_grid, bytes));
+    CK(cudaMemcpyAsync(o->geo_grid.p, grid, bytes, cudaMemcpyHostToDevice, o->stream));
+    CK(cudaStreamSynchronize(o->stream));
+    o->geo = d;
+    o->has_geo = true;
+    return TC_OK;
+}
+
+static int check_raw(struct ocl *o, const float *re, const float *im, int region_rows,
+                     int padded_rows, int rows, int cols, const float *coh, const int *count)
+{
+    if (!o)
+        return set_error(TC_ERR_ARG, "no context");
+    if (!re || !im || !coh || !count)
+        return set_error(TC_ERR_ARG, "missing raw rows or output buffer");
+    if (rows < 1 || cols < 1 || region_rows < 1 || padded_rows != rows + o->wa - 1 ||
+        cols + o->wr - 1 != o->padded_cols)
+        return set_error(TC_ERR_ARG, "raw strip of %d x %d (padded %d rows, %d columns) does "
+                         "not match the window %d x %d", rows, cols, padded_rows,
+                         o->padded_cols, o->wa, o->wr);
+    if (o->has_geo && (cols > (o->geo.grid_cols - 1) * 16 ||
+                       region_rows > (o->geo.grid_rows - 1) * 16))
+        return set_error(TC_ERR_ARG, "region of %d rows x %d columns beyond the geometry grid",
+                         region_rows, cols);
+    return TC_OK;
+}
+
+static int prepare_raw(struct ocl *o, const float *re, const float *im, const double *elev,
+                       int row0, int region_rows, int padded_rows, int cols, cudaStream_t st,
+                       Timer &tm)
+{
+    const size_t npad = (size_t)padded_rows * o->padded_cols;
+    const size_t n = o->n;
+
+    CK(ensure(o->slc, npad * n * 2 * sizeof(float)));
+    CK(ensure(o->amp, npad * n * sizeof(float)));
+    CK(ensure(o->valid, npad));
+    const int t = tm.begin(ST_PREP);
+
+    CK(tc_launch_prep_raw(o->n, re, im, elev, row0, region_rows, padded_rows, cols, o->wr / 2,
+                          o->has_geo ? &o->geo : nullptr, (const double *)o->geo_grid.p,
+                          (float *)o->slc.p, (float *)o->amp.p, (unsigned char *)o->valid.p,
+                          st));
+    tm.end(t);
+    return TC_OK;
+}
+
+TC_API int tc_run_raw(struct ocl *o, const float *re, const float *im, const double *elevation,
+                      int row0, int region_rows, int padded_rows, int rows, int cols,
+                      float *coh, int *count, float *pairs, float *phases,
+                      unsigned char *status)
+{
+    int rc;
+
+    if ((rc = check_raw(o, re, im, region_rows, padded_rows, rows, cols, coh, count)) != TC_OK)
+        return rc;
+    CK(cudaSetDevice(o->device));
+    const size_t plane = (size_t)padded_rows * cols;
+    const size_t n = o->n;
+    cudaStream_t st = o->stream;
+    Timer tm(o, st);
+
+    memset(o->stage_ms, 0, sizeof(o->stage_ms));
+    memset(o->stage_launches, 0, sizeof(o->stage_launches));
+    CK(ensure(o->raw_re, n * plane * sizeof(float)));
+    CK(ensure(o->raw_im, n * plane * sizeof(float)));
+    if (elevation)
+        CK(ensure(o->raw_elev, plane * sizeof(double)));
+    if ((rc = ensure_outputs(o, (size_t)rows * cols, phases != nullptr, status != nullptr)) !=
+        TC_OK)
+        return rc;
+    const int t = tm.begin(ST_COPY);
+
+    CK(cudaMemcpyAsync(o->raw_re.p, re, n * plane * sizeof(float), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(o->raw_im.p, im, n * plane * sizeof(float), cudaMemcpyHostToDevice, st));
+    if (elevation)
+        CK(cudaMemcpyAsync(o->raw_elev.p, elevation, plane * sizeof(double),
+                           cudaMemcpyHostToDevice, st));
+    tm.end(t);
+    if ((rc = prepare_raw(o, (const float *)o->raw_re.p, (const float *)o->raw_im.p,
+                          elevation ? (const double *)o->raw_elev.p : nullptr, row0, region_rows,
+                          padded_rows, cols, st, tm)) != TC_OK)
+        return rc;
+    return run_context_buffers(o, padded_rows, rows, cols, coh, count, pairs, phases, status, tm);
+}
+
+TC_API int tc_run_raw_device(struct ocl *o, const float *re, const float *im,
+                             const double *elevation, int row0, int region_rows, int padded_rows,
+                             int rows, int cols, float *coh, int *count, float *pairs,
+                             float *phases, unsigned char *status, void *stream)
+{
+    int rc;
+
+    if ((rc = check_raw(o, re, im, region_rows, padded_rows, rows, cols, coh, count)) != TC_OK)
+        return rc;
+    CK(cudaSetDevice(o->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    Timer tm(o, st);
+
+    memset(o->stage_ms, 0, sizeof(o->stage_ms));
+    memset(o->stage_launches, 0, sizeof(o->stage_launches));
+    if ((rc = prepare_raw(o, re, im, elevation, row0, region_rows, padded_rows, cols, st, tm)) !=
+        TC_OK)
+        return rc;
+    rc = run_device(o, (const float *)o->slc.p, (const float *)o->amp.p,
+                    (const unsigned char *)o->valid.p, padded_rows, rows, cols, coh, count,
+                    pairs, phases, status, st, tm);
+    if (o->timing) {
         cudaStreamSynchronize(st);
         tm.collect();
-        return rc;
     }
-    t = tm.begin(ST_COPY);
-    CK(cudaMemcpyAsync(coh, o->coh.p, nout * sizeof(float), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(count, o->count.p, nout * sizeof(int), cudaMemcpyDeviceToHost, st));
-    if (o->npairs && pairs)
-        CK(cudaMemcpyAsync(pairs, o->pairs.p, o->npairs * nout * sizeof(float),
-                           cudaMemcpyDeviceToHost, st));
-    if (phases)
-        CK(cudaMemcpyAsync(phases, o->phases.p, nout * n * sizeof(float),
-                           cudaMemcpyDeviceToHost, st));
-    if (status)
-        CK(cudaMemcpyAsync(status, o->status.p, nout, cudaMemcpyDeviceToHost, st));
-    tm.end(t);
-    CK(cudaStreamSynchronize(st));
-    tm.collect();
-    if (o->opt.gram == TC_GRAM_TENSOR && tc_gram_tensor_fault() > 0)
-        return set_error(TC_ERR_DEVICE, "tensor-core Gram: a wait for MMA completion ran out; "
-                         "the tiles concerned are NULL");
-    return TC_OK;
+    return rc;
 }
 
 /* ------------------------------------------------------------------ */

@@ -67,6 +67,28 @@ __host__ __device__ inline void tc_pixel_yx(const TcChunk &c, int p, int &y, int
     x = tx * TC_TILE_W + (w & 7);
 }
 
+/* Geometry (geometry.cu): the device copy of struct tc_geometry with the
+   grid shape, and the orbits of all dates concatenated. */
+struct TcGeo {
+    int ndates, ref, grid_rows, grid_cols, nheights;
+    double heights[3];
+    double first_line_time, azimuth_time_interval, slant_range_time, range_sampling_rate;
+    double wavelength, line0, sample0, h0;
+};
+
+struct TcOrbitSet {
+    const int *count, *offset;
+    const double *t, *pos, *vel;
+};
+
+int tc_geometry_shape(const struct tc_geometry &in, TcGeo &g);
+int tc_geometry_grid(const TcGeo &g, const struct tc_orbit *orbits, double *grid_host,
+                     cudaStream_t st);
+cudaError_t tc_launch_prep_raw(int n, const float *re, const float *im, const double *elev,
+                               int row0, int region_rows, int padded_rows, int cols, int halo,
+                               const TcGeo *g, const double *grid, float *slc, float *amp,
+                               unsigned char *valid, cudaStream_t st);
+
 /* Helpers of abi.cu shared with the other translation units. */
 int tc_error(int code, const char *fmt, ...);
 int tc_check_settings(const struct settings *s, int padded_cols);

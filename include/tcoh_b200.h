@@ -150,6 +150,70 @@ int tc_run_device(struct ocl *o, const float *slc, const float *amp,
    arithmetic chosen for gram = -1, the split terms in force). */
 int tc_get_options(const struct ocl *o, struct tc_options *opt);
 
+/* Flat-earth and topographic phase removal and strip preparation on the
+   device (geometry.c, orbit.c, main.c:52-127). */
+
+/* Orbit of one date (orbit.c:52-57): n >= 8 state vectors, times in
+   seconds (increasing), Earth-fixed positions and velocities [n][3] in m
+   and m/s. */
+struct tc_orbit {
+    int n;
+    const double *t;
+    const double *pos;
+    const double *vel;
+};
+
+/* Acquisition geometry (geometry.c:161-216): the raster timing of the
+   reference date's image and the region in it. */
+struct tc_geometry {
+    int ndates, ref;              /* dates; the reference date */
+    double first_line_time;       /* s, time of image line 0 */
+    double azimuth_time_interval; /* s per line */
+    double slant_range_time;      /* s, two-way time of image sample 0 */
+    double range_sampling_rate;   /* Hz */
+    double wavelength;            /* m */
+    double line0, sample0;        /* image line and sample of region cell (0, 0) */
+    int rows, cols;               /* region size */
+    double hmin, hmax;            /* height range of the elevation map; h0, h0 without */
+    double h0;                    /* height used without an elevation map */
+};
+
+/* Shape of the phase grid: nodes every 16 lines and samples, one height
+   level when hmax - hmin < 1 m, else three (hmin, mid, hmax), written to
+   heights[3]. The grid is double [grid_rows][grid_cols][nheights][ndates]. */
+int tc_geometry_grid_shape(const struct tc_geometry *g, int *grid_rows, int *grid_cols,
+                           int *nheights, double *heights);
+
+/* The phase grid, computed in double precision on the current device
+   (geometry_init, geometry.c:161-254): for every node and height level the
+   ground point of the reference date is located on the WGS84 ellipsoid and
+   every date's phase 4 pi / lambda (R_k - R_ref) at its zero-Doppler time is
+   written to grid (host). orbits[ndates]. TC_ERR_ARG when a point cannot be
+   located or falls outside an orbit, as the reference's fatal errors. */
+int tc_geometry_init(const struct tc_geometry *g, const struct tc_orbit *orbits,
+                     double *grid);
+
+/* Attaches a phase grid (host, as tc_geometry_init writes it) to the
+   context for tc_run_raw; grid NULL detaches it. */
+int tc_set_geometry(struct ocl *o, const struct tc_geometry *g, const double *grid);
+
+/* tc_run_ex from raw rows: re, im float [ndates][padded_rows][cols] (host)
+   are the I/Q samples of region rows row0 .. row0 + padded_rows - 1 (rows
+   outside 0 .. region_rows - 1 are ignored; NaN marks NULL), elevation
+   double [padded_rows][cols] or NULL. The strip preparation of
+   main.c:52-127 runs on the device: validity, sorted amplitudes, and, with
+   a geometry attached, the rotation of date k by exp(i phase_k) interpolated
+   at each cell's height (the elevation, else h0). */
+int tc_run_raw(struct ocl *o, const float *re, const float *im, const double *elevation,
+               int row0, int region_rows, int padded_rows, int rows, int cols, float *coh,
+               int *count, float *pairs, float *phases, unsigned char *status);
+
+/* The same on device buffers, asynchronously on `stream`. */
+int tc_run_raw_device(struct ocl *o, const float *re, const float *im,
+                      const double *elevation, int row0, int region_rows, int padded_rows,
+                      int rows, int cols, float *coh, int *count, float *pairs,
+                      float *phases, unsigned char *status, void *stream);
+
 /* Stage timing. With timing on, every launch of the following runs is
    bracketed by CUDA events on its stream, and tc_stage_stats gives, per
    stage, the device milliseconds summed over the last run and the number

@@ -86,6 +86,99 @@ def _settings(n, window, shp_test, alpha, estimator, bias, min_shp, npairs, pair
     )
 
 
+class _Orbit(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("t", ctypes.c_void_p), ("pos", ctypes.c_void_p),
+                ("vel", ctypes.c_void_p)]
+
+
+class _Geometry(ctypes.Structure):
+    _fields_ = [
+        ("ndates", ctypes.c_int), ("ref", ctypes.c_int),
+        ("first_line_time", ctypes.c_double), ("azimuth_time_interval", ctypes.c_double),
+        ("slant_range_time", ctypes.c_double), ("range_sampling_rate", ctypes.c_double),
+        ("wavelength", ctypes.c_double), ("line0", ctypes.c_double), ("sample0", ctypes.c_double),
+        ("rows", ctypes.c_int), ("cols", ctypes.c_int),
+        ("hmin", ctypes.c_double), ("hmax", ctypes.c_double), ("h0", ctypes.c_double),
+    ]
+
+
+def _geometry(geo):
+    """geo: dict with the fields of orc_geometry."""
+    return _Geometry(*(geo[name] for name, _ in _Geometry._fields_))
+
+
+def _orbits(orbits):
+    """orbits: list of (t [n], pos [n][3], vel [n][3]); returns the ctypes
+    array and the arrays it points into (kept alive by the caller)."""
+    keep = []
+    arr = (_Orbit * len(orbits))()
+    for k, (t, pos, vel) in enumerate(orbits):
+        t = np.ascontiguousarray(t, np.float64)
+        pos = np.ascontiguousarray(pos, np.float64)
+        vel = np.ascontiguousarray(vel, np.float64)
+        keep += [t, pos, vel]
+        arr[k] = _Orbit(len(t), t.ctypes.data, pos.ctypes.data, vel.ctypes.data)
+    return arr, keep
+
+
+def geometry_shape(geo):
+    """(grid_rows, grid_cols, nheights, heights[3]) of geometry.c:201-216."""
+    gr, gc, nh = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    hs = np.zeros(3)
+    g = _geometry(geo)
+    lib().orc_geometry_shape(ctypes.byref(g), ctypes.byref(gr), ctypes.byref(gc),
+                             ctypes.byref(nh), _ptr(hs))
+    return gr.value, gc.value, nh.value, hs
+
+
+def geometry_grid(geo, orbits):
+    """The coarse phase grid [grid_rows][grid_cols][nheights][ndates]
+    (geometry.c:161-254), FP64; raises if a point cannot be located."""
+    gr, gc, nh, _ = geometry_shape(geo)
+    grid = np.zeros((gr, gc, nh, geo["ndates"]))
+    arr, keep = _orbits(orbits)
+    g = _geometry(geo)
+    rc = lib().orc_geometry_grid(ctypes.byref(g), arr, _ptr(grid))
+    if rc != 0:
+        raise ValueError("geometry grid failed (%d)" % rc)
+    return grid
+
+
+def geometry_phases(geo, grid, heights):
+    """Interpolated phase (ndates, rows, cols) at every region cell and its
+    height (geometry.c:256-291)."""
+    grid = np.ascontiguousarray(grid, np.float64)
+    heights = np.asarray(heights, np.float64)
+    rows, cols = heights.shape
+    g = _geometry(geo)
+    out = np.zeros((geo["ndates"], rows, cols))
+    ph = np.zeros(geo["ndates"])
+    for r in range(rows):
+        for c in range(cols):
+            lib().orc_geometry_phases(ctypes.byref(g), _ptr(grid), r, c,
+                                      ctypes.c_double(heights[r, c]), _ptr(ph))
+            out[:, r, c] = ph
+    return out
+
+
+def prepare_strip(re, im, elevation, row0, region_rows, halo_cols, geo=None, grid=None):
+    """main.c:52-127 on raw I/Q planes re, im (ndates, padded_rows, cols) of
+    region rows row0 ..; returns (slc, amp, valid) of the padded strip."""
+    re = np.ascontiguousarray(re, np.float32)
+    im = np.ascontiguousarray(im, np.float32)
+    n, prow, cols = re.shape
+    w = cols + 2 * halo_cols
+    slc = np.empty((prow, w, n, 2), np.float32)
+    amp = np.empty((prow, w, n), np.float32)
+    valid = np.empty((prow, w), np.uint8)
+    elev = None if elevation is None else np.ascontiguousarray(elevation, np.float64)
+    g = None if geo is None else ctypes.byref(_geometry(geo))
+    grid = None if grid is None else np.ascontiguousarray(grid, np.float64)
+    lib().orc_prepare_strip(n, _ptr(re), _ptr(im), _ptr(elev), row0, region_rows, prow, cols,
+                            halo_cols, g, _ptr(grid), _ptr(slc), _ptr(amp), _ptr(valid))
+    return slc, amp, valid
+
+
 def kernel_constants(n, shp_test="ks", alpha=0.05):
     """The float constants that the reference kernel is built with."""
     s = _settings(n, (21, 7), shp_test, alpha, "evd", False, n, 0, False, True)

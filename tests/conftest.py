@@ -26,6 +26,9 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a B200 GPU and the built CUDA library")
 
 
+GEOMETRY_CASES = ["flat_earth_ref0", "flat_earth_ref2", "topographic"]
+
+
 def golden_names():
     return sorted(
         os.path.basename(f)[:-4]
@@ -65,6 +68,45 @@ class Case:
             estimator=o.get("estimator", "evd"),
             bias=o.get("bias_correction", False),
         )
+
+    def geometry(self):
+        """For the geometry cases: the orbits (per date (t, pos, vel)), the
+        geometry fields of struct tc_geometry / orc_geometry (region = the
+        whole reference image) and the elevation map (None for flat earth),
+        as the module reads them from each date's metadata (geometry.c:161-
+        200, main.c:684-709)."""
+        d = self.data
+        orbits = [(d["orbit_t"][k], d["orbit_pos"][k], d["orbit_vel"][k]) for k in range(self.n)]
+        heights = d["heights"]
+        h0 = float(d["geo_terrain_height"])
+        topo = bool(np.any(heights != h0))
+        geo = dict(ndates=self.n, ref=int(d["geo_ref"]),
+                   first_line_time=float(d["geo_first_line_time"]),
+                   azimuth_time_interval=float(d["geo_azimuth_time_interval"]),
+                   slant_range_time=float(d["geo_slant_range_time"]),
+                   range_sampling_rate=float(d["geo_range_sampling_rate"]),
+                   wavelength=float(d["geo_wavelength"]), line0=0.0, sample0=0.0,
+                   rows=self.rows, cols=self.cols,
+                   hmin=float(heights.min()) if topo else h0,
+                   hmax=float(heights.max()) if topo else h0, h0=h0)
+        return geo, orbits, (heights if topo else None)
+
+    def raw_strip(self):
+        """Raw I/Q planes (N, padded_rows, cols) of the region rows of the
+        one strip, and its elevation rows, as main.c's read_strip reads
+        them (rows outside the region are NULL)."""
+        ha = self.window[0] // 2
+        prow = self.rows + 2 * ha
+        re = np.full((self.n, prow, self.cols), np.nan, np.float32)
+        im = re.copy()
+        re[:, ha:ha + self.rows] = self.stack.real
+        im[:, ha:ha + self.rows] = self.stack.imag
+        _geo, _orbits, heights = self.geometry() if "orbit_t" in self.data else (None, None, None)
+        elev = None
+        if heights is not None:
+            elev = np.full((prow, self.cols), np.nan)
+            elev[ha:ha + self.rows] = heights
+        return re, im, elev, -ha
 
     def strip(self):
         """The whole region as one padded strip, as main.c reads it."""

@@ -96,3 +96,51 @@ def test_oracle_float_shp_is_the_reference_kernel(n, test, alpha):
     r = oracle.run_reference(slc, amp, valid, 40, 32, **kw)
     o = oracle.run_oracle(slc, amp, valid, 40, 32, shp_fp32=True, **kw)
     assert np.array_equal(r["count"], o["count"])
+
+
+@pytest.mark.parametrize("name", ["flat_earth_ref0", "flat_earth_ref2", "topographic"])
+def test_geometry_oracle_matches_the_orbit_model(name):
+    """The phase grid restated from geometry.c and orbit.c, interpolated at
+    every cell, against the reference test's independent orbit model
+    (tests/geometry_model.py, Stack.phases): the grid's interpolation error
+    is a fraction of a milliradian on phases of tens of thousands of
+    radians."""
+    c = Case(name)
+    geo, orbits, heights = c.geometry()
+    grid = oracle.geometry_grid(geo, orbits)
+    h = heights if heights is not None else np.full((c.rows, c.cols), geo["h0"])
+    ph = oracle.geometry_phases(geo, grid, h)
+    assert np.abs(np.angle(np.exp(1j * (ph - c.phase)))).max() < 1e-3
+
+
+@pytest.mark.parametrize("name", ["flat_earth_ref0", "flat_earth_ref2", "topographic"])
+def test_geometry_oracle_end_to_end(name):
+    """test_flat_earth_phase / test_topographic_phase of the reference
+    (tests/i_sar_temporal_coherence_test.py:389-458): the coherence with the
+    orbit-derived, grid-interpolated phase removed matches reference.py fed
+    with the exact model phase within the tolerance."""
+    c = Case(name)
+    geo, orbits, _heights = c.geometry()
+    grid = oracle.geometry_grid(geo, orbits)
+    re, im, elev, row0 = c.raw_strip()
+    slc, amp, valid = oracle.prepare_strip(re, im, elev, row0, c.rows, c.window[1] // 2, geo, grid)
+    npairs = c.n * (c.n - 1) // 2
+    o = oracle.run_oracle(slc, amp, valid, c.rows, c.cols, npairs=npairs, pairs_all=True,
+                          **c.kwargs())
+    assert np.array_equal(o["count"], c.count)
+    assert np.allclose(o["coh"], c.coh, rtol=0, atol=TOLERANCE, equal_nan=True)
+    assert np.allclose(o["pairs"], c.pairs, rtol=0, atol=TOLERANCE, equal_nan=True)
+
+
+def test_strip_preparation_oracle_matches_the_host_reader():
+    """Without geometry, the C restatement of main.c:52-127 and the package's
+    host reader build the same strip, bit for bit."""
+    import tcoh_b200
+
+    c = Case("nulls")
+    re, im, _elev, row0 = c.raw_strip()
+    slc, amp, valid = oracle.prepare_strip(re, im, None, row0, c.rows, c.window[1] // 2)
+    hs, ha, hv = c.strip()
+    assert np.array_equal(valid, hv)
+    assert np.array_equal(amp, ha)
+    assert np.array_equal(slc, hs)
