@@ -39,7 +39,7 @@ EXPORTS = (
     "tc_open", "tc_run_ex", "tc_run_device", "tc_set_timing", "tc_stage_stats",
     "tc_close", "tc_fp32_peak", "tc_run_device_static", "tc_get_options",
     "tc_geometry_grid_shape", "tc_geometry_init", "tc_set_geometry", "tc_run_raw",
-    "tc_run_raw_device",
+    "tc_run_raw_device", "tc_adjoint_raw",
 )
 
 
@@ -171,6 +171,7 @@ def library():
         lib.tc_set_geometry.argtypes = [vp, ctypes.POINTER(Geometry), vp]
         lib.tc_run_raw.argtypes = [vp, vp, vp, vp, i, i, i, i, i, vp, vp, vp, vp, vp]
         lib.tc_run_raw_device.argtypes = [vp, vp, vp, vp, i, i, i, i, i, vp, vp, vp, vp, vp, vp]
+        lib.tc_adjoint_raw.argtypes = [vp, vp, vp, vp, vp, vp, i, i, i, i, i, vp, vp, vp, vp]
         lib.tc_fp32_peak.argtypes = [i, ctypes.POINTER(ctypes.c_double)]
         lib.tc_run_device_static.argtypes = [ctypes.POINTER(Settings), i, vp, vp, vp, i, i, i,
                                              vp, vp, vp, vp, vp, vp]
@@ -397,6 +398,28 @@ class Backend:
             self.handle, re.ctypes.data, im.ctypes.data, _ptr(elev), row0, region_rows,
             padded_rows, rows, cols, _ptr(out["coh"]), _ptr(out["count"]), _ptr(out.get("pairs")),
             _ptr(out.get("phases")), _ptr(out.get("status"))))
+        return out
+
+    def adjoint_raw(self, re, im, elevation, dh, psi, row0, region_rows, rows, cols):
+        """tc_adjoint_raw: gamma of a raw strip (as run_raw) and the gradient
+        of the sum of gamma over its estimated pixels with respect to a
+        height error dh (padded_rows, cols) and a phase screen psi (N,
+        padded_rows, cols) added to the removed phase (either None for
+        zero). Returns a dict with coh, count, grad_dh and grad_psi."""
+        re = np.ascontiguousarray(re, np.float32)
+        im = np.ascontiguousarray(im, np.float32)
+        n, padded_rows, _ = re.shape
+        elev = None if elevation is None else np.ascontiguousarray(elevation, np.float64)
+        dh = None if dh is None else np.ascontiguousarray(dh, np.float64)
+        psi = None if psi is None else np.ascontiguousarray(psi, np.float32)
+        out = {"coh": np.empty((rows, cols), np.float32),
+               "count": np.empty((rows, cols), np.int32),
+               "grad_dh": np.empty((padded_rows, cols), np.float32),
+               "grad_psi": np.empty((n, padded_rows, cols), np.float32)}
+        _check(library().tc_adjoint_raw(
+            self.handle, re.ctypes.data, im.ctypes.data, _ptr(elev), _ptr(dh), _ptr(psi), row0,
+            region_rows, padded_rows, rows, cols, _ptr(out["coh"]), _ptr(out["count"]),
+            _ptr(out["grad_dh"]), _ptr(out["grad_psi"])))
         return out
 
     def run_raw_device(self, re, im, elevation, row0, region_rows, rows, cols, coh, count,

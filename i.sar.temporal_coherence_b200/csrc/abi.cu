@@ -228,7 +228,7 @@ struct ocl {
     cudaStream_t stream;
     DevBuf slc, amp, valid, coh, count, pairs, phases, status;
     DevBuf soa, logstat, mask, gram, upper_tab, pair_tab, link_scratch;
-    DevBuf raw_re, raw_im, raw_elev, geo_grid;
+    DevBuf raw_re, raw_im, raw_elev, geo_grid, adj_dh, adj_psi, adj_gbar, adj_dtheta, adj_gdh;
     bool has_geo;
     TcGeo geo;
     bool timing;
@@ -298,7 +298,8 @@ static void free_bufs(struct ocl *o)
     DevBuf *b[] = {&o->slc, &o->amp, &o->valid, &o->coh, &o->count, &o->pairs,
                    &o->phases, &o->status, &o->soa, &o->logstat, &o->mask, &o->gram,
                    &o->upper_tab, &o->pair_tab, &o->link_scratch, &o->raw_re, &o->raw_im,
-                   &o->raw_elev, &o->geo_grid};
+                   &o->raw_elev, &o->geo_grid, &o->adj_dh, &o->adj_psi, &o->adj_gbar,
+                   &o->adj_dtheta, &o->adj_gdh};
 
     for (size_t i = 0; i < sizeof(b) / sizeof(b[0]); i++)
         if (b[i]->p) {
@@ -546,10 +547,17 @@ static int chunk_rows_for(const struct ocl *o, int rows, int cols)
 }
 
 /* The computation on device buffers (asynchronous on st). */
+/* The adjoint's per-run state: the Gram-gradient buffer and dL/dtheta. */
+struct AdjRun {
+    float2 *gbar;
+    float *dtheta;
+};
+
 static int run_device(struct ocl *o, const float *slc, const float *amp,
                       const unsigned char *valid, int padded_rows, int rows, int cols,
                       float *coh, int *count, float *pairs, float *phases,
-                      unsigned char *status, cudaStream_t st, Timer &tm)
+                      unsigned char *status, cudaStream_t st, Timer &tm,
+                      const AdjRun *adj = nullptr)
 {
     if (rows < 1 || cols < 1)
         return set_error(TC_ERR_ARG, "empty strip (%d x %d)", rows, cols);
@@ -632,10 +640,21 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
                                      (float2 *)o->gram.p, st));
         tm.end(t);
         t = tm.begin(ST_LINK);
-        CK(tc_launch_link(s, c, lk, (const float2 *)o->gram.p, count,
-                          (const unsigned short *)o->upper_tab.p,
-                          (const unsigned short *)o->pair_tab.p, (double *)o->link_scratch.p,
-                          coh, pairs, phases, status, o->sms, st));
+        if (!adj)
+            CK(tc_launch_link(s, c, lk, (const float2 *)o->gram.p, count,
+                              (const unsigned short *)o->upper_tab.p,
+                              (const unsigned short *)o->pair_tab.p,
+                              (double *)o->link_scratch.p, coh, pairs, phases, status, o->sms,
+                              st));
+        else {
+            CK(tc_launch_link_adjoint(s, c, lk, (const float2 *)o->gram.p, count,
+                                      (const unsigned short *)o->upper_tab.p,
+                                      (const unsigned short *)o->pair_tab.p,
+                                      (double *)o->link_scratch.p, coh, pairs, adj->gbar,
+                                      o->sms, st));
+            CK(tc_launch_adjoint_scatter(s, c, o->wr / 2, adj->gbar, (const uint32_t *)o->mask.p,
+                                         slc, adj->dtheta, st));
+        }
         tm.end(t);
     }
     return TC_OK;
@@ -852,7 +871,7 @@ static int check_raw(struct ocl *o, const float *re, const float *im, int region
 
 static int prepare_raw(struct ocl *o, const float *re, const float *im, const double *elev,
                        int row0, int region_rows, int padded_rows, int cols, cudaStream_t st,
-                       Timer &tm)
+                       Timer &tm, const double *dh = nullptr, const float *psi = nullptr)
 {
     const size_t npad = (size_t)padded_rows * o->padded_cols;
     const size_t n = o->n;
@@ -863,7 +882,7 @@ static int prepare_raw(struct ocl *o, const float *re, const float *im, const do
     const int t = tm.begin(ST_PREP);
 
     CK(tc_launch_prep_raw(o->n, re, im, elev, row0, region_rows, padded_rows, cols, o->wr / 2,
-                          o->has_geo ? &o->geo : nullptr, (const double *)o->geo_grid.p,
+                          o->has_geo ? &o->geo : nullptr, (const double *)o->geo_grid.p, dh, psi,
                           (float *)o->slc.p, (float *)o->amp.p, (unsigned char *)o->valid.p,
                           st));
     tm.end(t);
@@ -935,6 +954,98 @@ TC_API int tc_run_raw_device(struct ocl *o, const float *re, const float *im,
         tm.collect();
     }
     return rc;
+}
+
+TC_API int tc_adjoint_raw(struct ocl *o, const float *re, const float *im,
+                          const double *elevation, const double *dh, const float *psi, int row0,
+                          int region_rows, int padded_rows, int rows, int cols, float *coh,
+                          int *count, float *grad_dh, float *grad_psi)
+{
+    int rc;
+
+    if ((rc = check_raw(o, re, im, region_rows, padded_rows, rows, cols, coh, count)) != TC_OK)
+        return rc;
+    if (o->n > 32)
+        return set_error(TC_ERR_ARG, "the adjoint takes stacks of up to 32 dates, not %d", o->n);
+    if (!grad_psi)
+        return set_error(TC_ERR_ARG, "no gradient buffer");
+    CK(cudaSetDevice(o->device));
+    const size_t plane = (size_t)padded_rows * cols;
+    const size_t n = o->n;
+    cudaStream_t st = o->stream;
+    Timer tm(o, st);
+
+    memset(o->stage_ms, 0, sizeof(o->stage_ms));
+    memset(o->stage_launches, 0, sizeof(o->stage_launches));
+    CK(ensure(o->raw_re, n * plane * sizeof(float)));
+    CK(ensure(o->raw_im, n * plane * sizeof(float)));
+    if (elevation)
+        CK(ensure(o->raw_elev, plane * sizeof(double)));
+    if (dh)
+        CK(ensure(o->adj_dh, plane * sizeof(double)));
+    if (psi)
+        CK(ensure(o->adj_psi, n * plane * sizeof(float)));
+    CK(ensure(o->adj_dtheta, n * plane * sizeof(float)));
+    CK(ensure(o->adj_gdh, plane * sizeof(float)));
+    if ((rc = ensure_outputs(o, (size_t)rows * cols, false, false)) != TC_OK)
+        return rc;
+    int t = tm.begin(ST_COPY);
+
+    CK(cudaMemcpyAsync(o->raw_re.p, re, n * plane * sizeof(float), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(o->raw_im.p, im, n * plane * sizeof(float), cudaMemcpyHostToDevice, st));
+    if (elevation)
+        CK(cudaMemcpyAsync(o->raw_elev.p, elevation, plane * sizeof(double),
+                           cudaMemcpyHostToDevice, st));
+    if (dh)
+        CK(cudaMemcpyAsync(o->adj_dh.p, dh, plane * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (psi)
+        CK(cudaMemcpyAsync(o->adj_psi.p, psi, n * plane * sizeof(float), cudaMemcpyHostToDevice,
+                           st));
+    CK(cudaMemsetAsync(o->adj_dtheta.p, 0, n * plane * sizeof(float), st));
+    tm.end(t);
+    const double *d_elev = elevation ? (const double *)o->raw_elev.p : nullptr;
+    const double *d_dh = dh ? (const double *)o->adj_dh.p : nullptr;
+
+    if ((rc = prepare_raw(o, (const float *)o->raw_re.p, (const float *)o->raw_im.p, d_elev, row0,
+                          region_rows, padded_rows, cols, st, tm, d_dh,
+                          psi ? (const float *)o->adj_psi.p : nullptr)) != TC_OK)
+        return rc;
+    /* the Gram gradient has the Gram's size */
+    const int crows = chunk_rows_for(o, rows, cols);
+    const size_t max_npix = (size_t)(crows / TC_TILE_H) * ((cols + TC_TILE_W - 1) / TC_TILE_W) *
+                            TC_TILE_PIX;
+
+    CK(ensure(o->adj_gbar, sizeof(float2) * tc_npu(o->n) * max_npix));
+    AdjRun adj = {(float2 *)o->adj_gbar.p, (float *)o->adj_dtheta.p};
+
+    rc = run_device(o, (const float *)o->slc.p, (const float *)o->amp.p,
+                    (const unsigned char *)o->valid.p, padded_rows, rows, cols, (float *)o->coh.p,
+                    (int *)o->count.p, o->npairs ? (float *)o->pairs.p : nullptr, nullptr, nullptr,
+                    st, tm, &adj);
+    if (rc != TC_OK) {
+        cudaStreamSynchronize(st);
+        return rc;
+    }
+    CK(tc_launch_adjoint_height(o->n, padded_rows, cols, row0, region_rows, d_elev, d_dh,
+                                o->has_geo ? &o->geo : nullptr, (const double *)o->geo_grid.p,
+                                (const float *)o->adj_dtheta.p, (float *)o->adj_gdh.p, st));
+    t = tm.begin(ST_COPY);
+    CK(cudaMemcpyAsync(coh, o->coh.p, (size_t)rows * cols * sizeof(float), cudaMemcpyDeviceToHost,
+                       st));
+    CK(cudaMemcpyAsync(count, o->count.p, (size_t)rows * cols * sizeof(int),
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(grad_psi, o->adj_dtheta.p, n * plane * sizeof(float),
+                       cudaMemcpyDeviceToHost, st));
+    if (grad_dh)
+        CK(cudaMemcpyAsync(grad_dh, o->adj_gdh.p, plane * sizeof(float), cudaMemcpyDeviceToHost,
+                           st));
+    tm.end(t);
+    CK(cudaStreamSynchronize(st));
+    tm.collect();
+    if (o->opt.gram == TC_GRAM_TENSOR && tc_gram_tensor_fault() > 0)
+        return set_error(TC_ERR_DEVICE, "tensor-core Gram: a wait for MMA completion ran out; "
+                         "the tiles concerned are NULL");
+    return TC_OK;
 }
 
 /* ------------------------------------------------------------------ */

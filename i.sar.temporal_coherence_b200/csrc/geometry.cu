@@ -280,6 +280,7 @@ __global__ void __launch_bounds__(256)
 tc_prep_raw_kernel(int n, const float *__restrict__ re, const float *__restrict__ im,
                    const double *__restrict__ elev, int row0, int region_rows, int padded_rows,
                    int cols, int halo, int use_geo, TcGeo g, const double *__restrict__ grid,
+                   const double *__restrict__ dh, const float *__restrict__ psi,
                    float2 *__restrict__ slc, float *__restrict__ amp,
                    unsigned char *__restrict__ valid)
 {
@@ -323,7 +324,7 @@ tc_prep_raw_kernel(int n, const float *__restrict__ re, const float *__restrict_
     for (int k = 0; k < NP; k++)
         if (k < n)
             a_out[k] = a[k];
-    if (!use_geo) {
+    if (!use_geo && !psi) {
         for (int k = 0; k < n; k++)
             s[k] = make_float2(re[k * plane + at], im[k * plane + at]);
         return;
@@ -331,10 +332,11 @@ tc_prep_raw_kernel(int n, const float *__restrict__ re, const float *__restrict_
     const int gr = row / GEO_STEP, gc = c / GEO_STEP;
     const double fr = (double)(row - gr * GEO_STEP) / GEO_STEP;
     const double fc = (double)(c - gc * GEO_STEP) / GEO_STEP;
-    const double h = elev ? elev[at] : g.h0;
+    /* the adjoint's variables: a height error and a phase screen */
+    const double h = (elev ? elev[at] : g.h0) + (dh ? dh[at] : 0.0);
     double wh[3] = {1.0, 0.0, 0.0};
 
-    if (g.nheights == 3) {
+    if (use_geo && g.nheights == 3) {
         const double *x = g.heights;
 
         wh[0] = (h - x[1]) * (h - x[2]) / ((x[0] - x[1]) * (x[0] - x[2]));
@@ -342,7 +344,8 @@ tc_prep_raw_kernel(int n, const float *__restrict__ re, const float *__restrict_
         wh[2] = (h - x[0]) * (h - x[1]) / ((x[2] - x[0]) * (x[2] - x[1]));
     }
     for (int k = 0; k < n; k++) {
-        const double ph = grid_phase(g, grid, gr, gc, fr, fc, wh, k);
+        const double ph = (use_geo ? grid_phase(g, grid, gr, gc, fr, fc, wh, k) : 0.0) +
+                          (psi ? (double)psi[k * plane + at] : 0.0);
         double sn, cs;
 
         sincos(ph, &sn, &cs);
@@ -482,8 +485,9 @@ int tc_geometry_grid(const TcGeo &g, const struct tc_orbit *orbits, double *grid
 
 cudaError_t tc_launch_prep_raw(int n, const float *re, const float *im, const double *elev,
                                int row0, int region_rows, int padded_rows, int cols, int halo,
-                               const TcGeo *g, const double *grid, float *slc, float *amp,
-                               unsigned char *valid, cudaStream_t st)
+                               const TcGeo *g, const double *grid, const double *dh,
+                               const float *psi, float *slc, float *amp, unsigned char *valid,
+                               cudaStream_t st)
 {
     const long long cells = (long long)padded_rows * (cols + 2 * halo);
     const unsigned blocks = (unsigned)((cells + 255) / 256);
@@ -494,19 +498,19 @@ cudaError_t tc_launch_prep_raw(int n, const float *re, const float *im, const do
 
     if (n <= 8)
         tc_prep_raw_kernel<8><<<blocks, 256, 0, st>>>(n, re, im, elev, row0, region_rows,
-                                                      padded_rows, cols, halo, use, gg, grid, s,
+                                                      padded_rows, cols, halo, use, gg, grid, dh, psi, s,
                                                       amp, valid);
     else if (n <= 16)
         tc_prep_raw_kernel<16><<<blocks, 256, 0, st>>>(n, re, im, elev, row0, region_rows,
-                                                       padded_rows, cols, halo, use, gg, grid, s,
+                                                       padded_rows, cols, halo, use, gg, grid, dh, psi, s,
                                                        amp, valid);
     else if (n <= 32)
         tc_prep_raw_kernel<32><<<blocks, 256, 0, st>>>(n, re, im, elev, row0, region_rows,
-                                                       padded_rows, cols, halo, use, gg, grid, s,
+                                                       padded_rows, cols, halo, use, gg, grid, dh, psi, s,
                                                        amp, valid);
     else
         tc_prep_raw_kernel<64><<<blocks, 256, 0, st>>>(n, re, im, elev, row0, region_rows,
-                                                       padded_rows, cols, halo, use, gg, grid, s,
+                                                       padded_rows, cols, halo, use, gg, grid, dh, psi, s,
                                                        amp, valid);
     return cudaGetLastError();
 }

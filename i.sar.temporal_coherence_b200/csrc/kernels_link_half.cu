@@ -96,7 +96,7 @@ __device__ __forceinline__ void gsync(const Grp &g) { __syncwarp(g.mask); }
 struct HalfLayout {
     int n, ld;
     int off_T, off_G, off_vw, off_lu, off_tau, off_d, off_e, off_df, off_e2f, off_y,
-        off_nrm, off_zs, off_rs, off_lam, off_x;
+        off_nrm, off_zs, off_rs, off_lam, off_x, off_Tb, off_Db;
     int per_group;
 };
 
@@ -844,6 +844,112 @@ __device__ __forceinline__ double2 mval(const HWs &w, int ld, int i, int j)
     return make_double2(gg * (double)t.x, i < j ? gg * (double)t.y : -gg * (double)t.y);
 }
 
+/* t = Q (tri - lambda)^+ Q^H b off the eigen-direction, rows (i0, i1):
+   Q and tri are the float reduction of the group's matrix (Householder
+   vectors in T's lower triangle, tau), lambda the eigenvalue of the
+   tridiagonal eigenvector y, piv / w.lu the LU of (tri - lambda). b is
+   mapped by Q^H, its component along y removed, the real and imaginary
+   parts solved with the LU, the y component removed again, and the result
+   mapped back by Q. Scratch: the first 32 float2 of w.x. */
+__device__ void solve_off(int n, int ld, const HWs &w, const Grp &g, const float (&yr)[32],
+                          unsigned long long piv, float2 b0, float2 b1, float2 &t0, float2 &t1)
+{
+    const int i0 = g.gl, i1 = g.gl + 16;
+
+    /* b = Q^H b = H_{n-2} .. H_0 b */
+    for (int k = 0; k < n - 1; k++) {
+        const float2 ta = w.tau[k];
+
+        if (ta.x == 0.f && ta.y == 0.f)
+            continue;
+        const float2 v0 = i0 > k && i0 < n ? w.T[i0 * ld + k] : make_float2(0.f, 0.f);
+        const float2 v1 = i1 > k && i1 < n ? w.T[i1 * ld + k] : make_float2(0.f, 0.f);
+        float sr = v0.x * b0.x + v0.y * b0.y + v1.x * b1.x + v1.y * b1.y;
+        float si = v0.x * b0.y - v0.y * b0.x + v1.x * b1.y - v1.y * b1.x;
+
+        sr = gsum(sr, g);
+        si = gsum(si, g);
+        /* H^H b = b - conj(tau) v (v^H b) */
+        const float hr = ta.x * sr + ta.y * si;
+        const float hi = ta.x * si - ta.y * sr;
+
+        b0.x -= v0.x * hr - v0.y * hi;
+        b0.y -= v0.x * hi + v0.y * hr;
+        b1.x -= v1.x * hr - v1.y * hi;
+        b1.y -= v1.x * hi + v1.y * hr;
+    }
+    /* b is in the real-tridiagonal basis but complex-valued: solve the real
+       and imaginary parts with the float LU of (tri - lambda), off y. */
+    float2 *bs = (float2 *)w.x;
+
+    bs[i0] = b0;
+    bs[i1] = b1;
+    gsync(g);
+    float tr_[32], ti_[32];
+    float ynrm = 0.f, cr = 0.f, ci = 0.f;
+
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+        const float2 bk = k < n ? bs[k] : make_float2(0.f, 0.f);
+
+        ynrm = fmaf(yr[k], yr[k], ynrm);
+        cr = fmaf(yr[k], bk.x, cr);
+        ci = fmaf(yr[k], bk.y, ci);
+        tr_[k] = bk.x;
+        ti_[k] = bk.y;
+    }
+    gsync(g);
+    cr /= ynrm;
+    ci /= ynrm;
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+        tr_[k] = fmaf(-cr, yr[k], tr_[k]);
+        ti_[k] = fmaf(-ci, yr[k], ti_[k]);
+    }
+    tri_solve(tr_, n, piv, w);
+    tri_solve(ti_, n, piv, w);
+    float dr = 0.f, di = 0.f;
+
+#pragma unroll
+    for (int k = 0; k < 32; k++)
+        if (k < n) {
+            dr = fmaf(yr[k], tr_[k], dr);
+            di = fmaf(yr[k], ti_[k], di);
+        }
+    dr /= ynrm;
+    di /= ynrm;
+    t0 = make_float2(0.f, 0.f);
+    t1 = t0;
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+        if (k == i0 && k < n)
+            t0 = make_float2(fmaf(-dr, yr[k], tr_[k]), fmaf(-di, yr[k], ti_[k]));
+        if (k == i1 && k < n)
+            t1 = make_float2(fmaf(-dr, yr[k], tr_[k]), fmaf(-di, yr[k], ti_[k]));
+    }
+    /* t = Q t = H_0 .. H_{n-2} t */
+    for (int k = n - 2; k >= 0; k--) {
+        const float2 ta = w.tau[k];
+
+        if (ta.x == 0.f && ta.y == 0.f)
+            continue;
+        const float2 v0 = i0 > k && i0 < n ? w.T[i0 * ld + k] : make_float2(0.f, 0.f);
+        const float2 v1 = i1 > k && i1 < n ? w.T[i1 * ld + k] : make_float2(0.f, 0.f);
+        float sr = v0.x * t0.x + v0.y * t0.y + v1.x * t1.x + v1.y * t1.y;
+        float si = v0.x * t0.y - v0.y * t0.x + v1.x * t1.y - v1.y * t1.x;
+
+        sr = gsum(sr, g);
+        si = gsum(si, g);
+        const float hr = ta.x * sr - ta.y * si;
+        const float hi = ta.x * si + ta.y * sr;
+
+        t0.x -= v0.x * hr - v0.y * hi;
+        t0.y -= v0.x * hi + v0.y * hr;
+        t1.x -= v1.x * hr - v1.y * hi;
+        t1.y -= v1.x * hi + v1.y * hr;
+    }
+}
+
 /* One refinement step of the eigenpair of M for the eigenvector (z0, z1)
    of rows (i0, i1): see the file comment. tri and Q are the float
    reduction of M; y is the tridiagonal eigenvector. The residual is formed
@@ -904,100 +1010,11 @@ __device__ void refine(int n, int ld, const HWs &w, const Grp &g, double2 &x0, d
     if (!(rmax > 0.0))
         return;
     const double sc = 1.0 / rmax;
-    /* b = Q^H r = H_{n-2} .. H_0 r */
-    float2 b0 = make_float2((float)(r0.x * sc), (float)(r0.y * sc));
-    float2 b1 = make_float2((float)(r1.x * sc), (float)(r1.y * sc));
+    float2 t0, t1;
 
-    for (int k = 0; k < n - 1; k++) {
-        const float2 ta = w.tau[k];
-
-        if (ta.x == 0.f && ta.y == 0.f)
-            continue;
-        const float2 v0 = i0 > k && i0 < n ? w.T[i0 * ld + k] : make_float2(0.f, 0.f);
-        const float2 v1 = i1 > k && i1 < n ? w.T[i1 * ld + k] : make_float2(0.f, 0.f);
-        float sr = v0.x * b0.x + v0.y * b0.y + v1.x * b1.x + v1.y * b1.y;
-        float si = v0.x * b0.y - v0.y * b0.x + v1.x * b1.y - v1.y * b1.x;
-
-        sr = gsum(sr, g);
-        si = gsum(si, g);
-        /* H^H b = b - conj(tau) v (v^H b) */
-        const float hr = ta.x * sr + ta.y * si;
-        const float hi = ta.x * si - ta.y * sr;
-
-        b0.x -= v0.x * hr - v0.y * hi;
-        b0.y -= v0.x * hi + v0.y * hr;
-        b1.x -= v1.x * hr - v1.y * hi;
-        b1.y -= v1.x * hi + v1.y * hr;
-    }
-    /* b is in the real-tridiagonal basis but complex-valued: solve the real
-       and imaginary parts with the float LU of (tri - lambda), off y. */
-    float2 *bs = (float2 *)w.x;
-
-    bs[i0] = b0;
-    bs[i1] = b1;
-    gsync(g);
-    float tr_[32], ti_[32];
-    float ynrm = 0.f, cr = 0.f, ci = 0.f;
-
-#pragma unroll
-    for (int k = 0; k < 32; k++) {
-        const float2 bk = k < n ? bs[k] : make_float2(0.f, 0.f);
-
-        ynrm = fmaf(yr[k], yr[k], ynrm);
-        cr = fmaf(yr[k], bk.x, cr);
-        ci = fmaf(yr[k], bk.y, ci);
-        tr_[k] = bk.x;
-        ti_[k] = bk.y;
-    }
-    cr /= ynrm;
-    ci /= ynrm;
-#pragma unroll
-    for (int k = 0; k < 32; k++) {
-        tr_[k] = fmaf(-cr, yr[k], tr_[k]);
-        ti_[k] = fmaf(-ci, yr[k], ti_[k]);
-    }
-    tri_solve(tr_, n, piv, w);
-    tri_solve(ti_, n, piv, w);
-    float dr = 0.f, di = 0.f;
-
-#pragma unroll
-    for (int k = 0; k < 32; k++)
-        if (k < n) {
-            dr = fmaf(yr[k], tr_[k], dr);
-            di = fmaf(yr[k], ti_[k], di);
-        }
-    dr /= ynrm;
-    di /= ynrm;
-    float2 t0 = make_float2(0.f, 0.f), t1 = t0;
-
-#pragma unroll
-    for (int k = 0; k < 32; k++) {
-        if (k == i0 && k < n)
-            t0 = make_float2(fmaf(-dr, yr[k], tr_[k]), fmaf(-di, yr[k], ti_[k]));
-        if (k == i1 && k < n)
-            t1 = make_float2(fmaf(-dr, yr[k], tr_[k]), fmaf(-di, yr[k], ti_[k]));
-    }
-    /* d = Q t = H_0 .. H_{n-2} t; x -= d / sc */
-    for (int k = n - 2; k >= 0; k--) {
-        const float2 ta = w.tau[k];
-
-        if (ta.x == 0.f && ta.y == 0.f)
-            continue;
-        const float2 v0 = i0 > k && i0 < n ? w.T[i0 * ld + k] : make_float2(0.f, 0.f);
-        const float2 v1 = i1 > k && i1 < n ? w.T[i1 * ld + k] : make_float2(0.f, 0.f);
-        float sr = v0.x * t0.x + v0.y * t0.y + v1.x * t1.x + v1.y * t1.y;
-        float si = v0.x * t0.y - v0.y * t0.x + v1.x * t1.y - v1.y * t1.x;
-
-        sr = gsum(sr, g);
-        si = gsum(si, g);
-        const float hr = ta.x * sr - ta.y * si;
-        const float hi = ta.x * si + ta.y * sr;
-
-        t0.x -= v0.x * hr - v0.y * hi;
-        t0.y -= v0.x * hi + v0.y * hr;
-        t1.x -= v1.x * hr - v1.y * hi;
-        t1.y -= v1.x * hi + v1.y * hr;
-    }
+    solve_off(n, ld, w, g, yr, piv, make_float2((float)(r0.x * sc), (float)(r0.y * sc)),
+              make_float2((float)(r1.x * sc), (float)(r1.y * sc)), t0, t1);
+    /* x -= Q (tri - mu)^+ Q^H r */
     x0.x -= rmax * t0.x;
     x0.y -= rmax * t0.y;
     x1.x -= rmax * t1.x;
@@ -1120,7 +1137,7 @@ __device__ bool linked16(int n, int ld, const float2 *T, const Grp &g)
    then the goodness of fit (tcoh.cl:728-744), pairs spread evenly over the
    lanes. */
 __device__ float gamma16(int n, int ld, const HWs &w, const Grp &g, double2 z0, double2 z1,
-                         const unsigned short *__restrict__ upper_tab)
+                         const unsigned short *__restrict__ upper_tab, float2 *sum = nullptr)
 {
     const int i0 = g.gl, i1 = g.gl + 16;
     const double m0 = i0 < n ? hypot(z0.x, z0.y) : 0.0, m1 = i1 < n ? hypot(z1.x, z1.y) : 0.0;
@@ -1187,17 +1204,317 @@ __device__ float gamma16(int n, int ld, const HWs &w, const Grp &g, double2 z0, 
     }
     sr = gsum(sr, g);
     si = gsum(si, g);
+    if (sum)
+        *sum = make_float2(sr, si);
     return hypotf(sr, si) / (0.5f * n * (n - 1));
 }
 
+/* ------------------------------------------------------------------ */
+/* Adjoint.                                                            */
+/* ------------------------------------------------------------------ */
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b)
+{
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) /* a conj(b) */
+{
+    return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+/* T_ij of either triangle from the upper one (the lower holds the
+   Householder vectors). */
+__device__ __forceinline__ float2 t_full(const HWs &w, int ld, int i, int j)
+{
+    if (i == j)
+        return make_float2(1.f, 0.f);
+    const float2 t = w.T[(i < j ? i : j) * ld + (i < j ? j : i)];
+
+    return i < j ? t : make_float2(t.x, -t.y);
+}
+
+/* Gradient of gamma with respect to the pixel's coherence sums, written as
+   the Hermitian matrix G (upper triangle, gbar[pidx][p]) such that
+   d gamma = Re sum_ij conj(G_ij) dC_ij. The chain, in reverse:
+   gamma = |S| / npairs, S = sum_{i<j} unit(T_ij) conj(e_i) e_j; phasors
+   e_k = unit(z_k conj(z_ref)) (1 below the 1e-3 floor); the eigenvector z
+   of X (X = T for EVD, M = |T|^-1 o T for EMI) through
+   dz = (lambda - X)^+ dX z, applied with the float reduction of X
+   (solve_off); for EMI, M-bar = y z^H gives T-bar += |T|^-1 o M-bar and
+   |T|-bar = -|T|^-1 Re(conj(M-bar) o T) |T|^-1 (double); the bias correction
+   |T| = sqrt((L |t|^2 - 1) / (L - 1)); the normalization
+   t_ij = C_ij / sqrt(C_ii C_jj) (C_ii does not depend on the phases).
+   z0, z1: the final eigenvector rows; S: the sum of gamma16; Tb: n x ld
+   float2 scratch, Db: n x ld double scratch (EMI). An inactive pixel gets
+   G = 0. */
 template <bool EMI>
-__global__ void __launch_bounds__(EMI ? 256 : 384)
+__device__ void backward16(int n, int ld, const HWs &w, const Grp &g, double2 z0d, double2 z1d,
+                           float2 S, const float (&yr)[32], unsigned long long piv, int looks,
+                           bool bias, bool active, float2 *Tb, double *Db,
+                           const unsigned short *__restrict__ upper_tab, float2 *gbar,
+                           long long npix, long long p)
+{
+    const int i0 = g.gl, i1 = g.gl + 16;
+    const int npu = tc_npu(n);
+
+    /* unit-norm z in float; the phasor decisions (reference date, floor)
+       are those of gamma16, from the double rows */
+    const double m0 = i0 < n ? hypot(z0d.x, z0d.y) : 0.0, m1 = i1 < n ? hypot(z1d.x, z1d.y) : 0.0;
+    const double mx = gmaxd(fmax(m0, m1), g);
+    int ref = n / 2;
+    const double mref = gbcast(ref < 16 ? m0 : m1, ref, g);
+
+    if (mref <= 1.0e-3 * mx) {
+        int last = -1;
+
+        if (i0 < n && m0 == mx)
+            last = i0;
+        if (i1 < n && m1 == mx)
+            last = i1;
+#pragma unroll
+        for (int o = 8; o; o >>= 1)
+            last = max(last, __shfl_xor_sync(g.mask, last, o));
+        ref = last;
+    }
+    const bool big0 = i0 < n && m0 > mx * 1.0e-3, big1 = i1 < n && m1 > mx * 1.0e-3;
+    const double nn = gsum(m0 * m0 + m1 * m1, g);
+    const double inv = nn > 0.0 ? 1.0 / sqrt(nn) : 0.0;
+    const float2 z0 = make_float2((float)(z0d.x * inv), (float)(z0d.y * inv));
+    const float2 z1 = make_float2((float)(z1d.x * inv), (float)(z1d.y * inv));
+    float2 *zb = (float2 *)w.x + 32;
+
+    zb[i0] = i0 < n ? z0 : make_float2(0.f, 0.f);
+    zb[i1] = i1 < n ? z1 : make_float2(0.f, 0.f);
+    gsync(g);
+    const float2 zr = zb[ref];
+    /* S-bar */
+    const float P = 0.5f * n * (n - 1), sm = hypotf(S.x, S.y);
+    const float2 Sb = sm > 0.f ? make_float2(S.x / (sm * P), S.y / (sm * P)) : make_float2(0.f, 0.f);
+    const float2 Sc = make_float2(Sb.x, -Sb.y);
+    float2 vb[2];
+
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+        const int r = t ? i1 : i0;
+        float2 eb = make_float2(0.f, 0.f);
+
+        if (r < n) {
+            const float2 er = w.zs[r];
+
+            for (int j = 0; j < n; j++) {
+                float2 tb = make_float2(0.f, 0.f);
+
+                if (j != r) {
+                    const float2 tv = t_full(w, ld, r, j);
+                    const float m2 = tv.x * tv.x + tv.y * tv.y;
+                    const float im = m2 > 0.f ? rsqrtf(m2) : 0.f;
+                    const float2 wv = m2 > 0.f ? make_float2(tv.x * im, tv.y * im)
+                                               : make_float2(1.f, 0.f);
+                    const float2 ej = w.zs[j];
+                    /* j > r: e-bar_r += conj(S-bar) w_rj e_j; j < r: e-bar_r +=
+                       S-bar conj(w_jr) e_j = S-bar w_rj e_j */
+                    const float2 c = cmul(cmul(j > r ? Sc : Sb, wv), ej);
+
+                    eb = make_float2(eb.x + c.x, eb.y + c.y);
+                    if (j > r && m2 > 0.f) {
+                        /* w-bar_rj = S-bar e_r conj(e_j), through w = T / |T| */
+                        const float2 wb = cmul(Sb, cmulc(er, ej));
+                        const float rr = wv.x * wb.x + wv.y * wb.y;
+
+                        tb = make_float2((wb.x - wv.x * rr) * im, (wb.y - wv.y * rr) * im);
+                    }
+                }
+                Tb[r * ld + j] = tb;
+            }
+        }
+        /* v-bar_r = (e-bar - e Re(conj(e) e-bar)) / |v_r| */
+        vb[t] = make_float2(0.f, 0.f);
+        if (t ? big1 : big0) {
+            const float2 er = w.zs[r];
+            const float2 zv = t ? z1 : z0;
+            const float vm = hypotf(zv.x, zv.y) * hypotf(zr.x, zr.y);
+            const float rr = er.x * eb.x + er.y * eb.y;
+
+            vb[t] = make_float2((eb.x - er.x * rr) / vm, (eb.y - er.y * rr) / vm);
+        }
+    }
+    /* v_k = z_k conj(z_ref): z-bar_k = v-bar_k z_ref, z-bar_ref += sum_k conj(v-bar_k) z_k */
+    float2 zbar[2] = {cmul(vb[0], zr), cmul(vb[1], zr)};
+    {
+        const float2 c0 = cmul(make_float2(vb[0].x, -vb[0].y), z0);
+        const float2 c1 = cmul(make_float2(vb[1].x, -vb[1].y), z1);
+        const float cx = gsum(c0.x + c1.x, g), cy = gsum(c0.y + c1.y, g);
+
+        if (i0 == ref) {
+            zbar[0].x += cx;
+            zbar[0].y += cy;
+        }
+        if (i1 == ref) {
+            zbar[1].x += cx;
+            zbar[1].y += cy;
+        }
+    }
+    /* r = (I - z z^H) z-bar */
+    float2 al = make_float2(z0.x * zbar[0].x + z0.y * zbar[0].y + z1.x * zbar[1].x + z1.y * zbar[1].y,
+                            z0.x * zbar[0].y - z0.y * zbar[0].x + z1.x * zbar[1].y - z1.y * zbar[1].x);
+
+    al.x = gsum(al.x, g);
+    al.y = gsum(al.y, g);
+    float2 b0 = make_float2(zbar[0].x - cmul(z0, al).x, zbar[0].y - cmul(z0, al).y);
+    float2 b1 = make_float2(zbar[1].x - cmul(z1, al).x, zbar[1].y - cmul(z1, al).y);
+
+    if (i0 >= n)
+        b0 = make_float2(0.f, 0.f);
+    if (i1 >= n)
+        b1 = make_float2(0.f, 0.f);
+    /* y = (lambda - X)^+ r = -(X - lambda)^+ r; X-bar = y z^H */
+    float2 y0, y1;
+
+    solve_off(n, ld, w, g, yr, piv, b0, b1, y0, y1);
+    y0 = make_float2(-y0.x, -y0.y);
+    y1 = make_float2(-y1.x, -y1.y);
+    gsync(g);
+    if (!EMI) {
+#pragma unroll
+        for (int t = 0; t < 2; t++) {
+            const int r = t ? i1 : i0;
+            const float2 yv = t ? y1 : y0;
+
+            if (r < n)
+                for (int j = 0; j < n; j++) {
+                    const float2 xb = cmulc(yv, zb[j]);
+
+                    Tb[r * ld + j].x += xb.x;
+                    Tb[r * ld + j].y += xb.y;
+                }
+        }
+    }
+    else {
+        /* M = A o T with A = |T|^-1 (packed, double): T-bar += A o M-bar,
+           A-bar = Re(conj(M-bar) o T) */
+#pragma unroll
+        for (int t = 0; t < 2; t++) {
+            const int r = t ? i1 : i0;
+            const float2 yv = t ? y1 : y0;
+
+            if (r < n)
+                for (int j = 0; j < n; j++) {
+                    const float2 mb = cmulc(yv, zb[j]);
+                    const double a = w.G[sym_idx(n, r, j)];
+                    const float2 tv = t_full(w, ld, r, j);
+
+                    Tb[r * ld + j].x += (float)a * mb.x;
+                    Tb[r * ld + j].y += (float)a * mb.y;
+                    Db[r * ld + j] = (double)mb.x * tv.x + (double)mb.y * tv.y;
+                }
+        }
+        gsync(g);
+        /* |T|-bar = -A A-bar A, rows (i0, i1): P = A A-bar in registers */
+        double p0[32], p1[32];
+
+#pragma unroll
+        for (int j = 0; j < 32; j++)
+            p0[j] = p1[j] = 0.0;
+        for (int l = 0; l < n; l++) {
+            const double a0 = i0 < n ? w.G[sym_idx(n, i0, l)] : 0.0;
+            const double a1 = i1 < n ? w.G[sym_idx(n, i1, l)] : 0.0;
+
+#pragma unroll
+            for (int j = 0; j < 32; j++)
+                if (j < n) {
+                    const double ab = Db[l * ld + j];
+
+                    p0[j] = fma(a0, ab, p0[j]);
+                    p1[j] = fma(a1, ab, p1[j]);
+                }
+        }
+#pragma unroll
+        for (int t = 0; t < 2; t++) {
+            const int r = t ? i1 : i0;
+
+            if (r < n)
+                for (int j = 0; j < n; j++) {
+                    double bb = 0.0;
+
+#pragma unroll
+                    for (int k = 0; k < 32; k++)
+                        if (k < n)
+                            bb = fma(t ? p1[k] : p0[k], w.G[sym_idx(n, k, j)], bb);
+                    bb = -bb;
+                    if (j != r) {
+                        const float2 tv = t_full(w, ld, r, j);
+                        const float m = hypotf(tv.x, tv.y);
+
+                        if (m > 0.f) {
+                            Tb[r * ld + j].x += (float)bb * tv.x / m;
+                            Tb[r * ld + j].y += (float)bb * tv.y / m;
+                        }
+                    }
+                }
+        }
+    }
+    /* bias correction and normalization: C-bar_rj = t-bar_rj / (nrm_r nrm_j) */
+    const float L = (float)looks;
+
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+        const int r = t ? i1 : i0;
+
+        if (r < n)
+            for (int j = 0; j < n; j++) {
+                float2 tb = Tb[r * ld + j];
+
+                if (j == r)
+                    tb = make_float2(0.f, 0.f);
+                else if (bias && looks > 1) {
+                    const float2 tv = t_full(w, ld, r, j);
+                    const float mT = hypotf(tv.x, tv.y);
+
+                    if (mT > 0.f) {
+                        /* t = unit(T) |t|, |t|^2 = ((L - 1) |T|^2 + 1) / L */
+                        const float m2 = ((L - 1.f) * mT * mT + 1.f) / L;
+                        const float mt = sqrtf(m2), c = mT / mt;
+                        const float2 tt = make_float2(tv.x / c, tv.y / c);
+                        const float kap = (tb.x * tt.x + tb.y * tt.y) / (c * (L - 1.f) * m2 * m2);
+
+                        tb = make_float2(c * tb.x + kap * tt.x, c * tb.y + kap * tt.y);
+                    }
+                    else
+                        tb = make_float2(0.f, 0.f);
+                }
+                const float sc = 1.f / (w.nrm[r] * w.nrm[j]);
+
+                Tb[r * ld + j] = make_float2(tb.x * sc, tb.y * sc);
+            }
+    }
+    gsync(g);
+    /* G_ij = (C-bar_ij + conj(C-bar_ji)) / 2, upper triangle */
+    for (int q = g.gl; q < npu; q += 16) {
+        const int i = upper_tab[q] >> 8, j = upper_tab[q] & 255;
+        float2 v = make_float2(0.f, 0.f);
+
+        if (active && i != j) {
+            const float2 a = Tb[i * ld + j], b = Tb[j * ld + i];
+
+            v = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
+        }
+        gbar[(long long)q * npix + p] = v;
+    }
+    gsync(g);
+}
+
+/* ADJ: after gamma, backward16 writes the gradient of gamma with respect
+   to the pixel's coherence sums into gbar (same layout as gram). */
+template <bool EMI, bool ADJ>
+__global__ void __launch_bounds__(EMI || ADJ ? 256 : 384)
 tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
                     const float2 *__restrict__ gram, const int *__restrict__ count,
                     const unsigned short *__restrict__ upper_tab,
                     const unsigned short *__restrict__ pair_tab, double *__restrict__ scratch,
                     float *__restrict__ coh, float *__restrict__ pairs,
-                    float *__restrict__ phases, unsigned char *__restrict__ status)
+                    float *__restrict__ phases, unsigned char *__restrict__ status,
+                    float2 *__restrict__ gbar)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1279,6 +1596,7 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
         double2 z0 = make_double2(0.0, 0.0), z1 = z0;
         float yr[32], lambda = 0.f, norm = 0.f;
         float2 f0 = make_float2(0.f, 0.f), f1 = f0;
+        unsigned long long piv = 0ull;
 
         if (!EMI) {
             /* stage 2: Householder reduction of T */
@@ -1294,8 +1612,6 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
             __syncthreads();
             /* stage 3: its dominant eigenvector */
             if (run) {
-                unsigned long long piv;
-
                 st |= eigvec(n, n - 1, w, ld, g, f0, f1, yr, lambda, norm, piv);
                 z0 = make_double2(f0.x, f0.y);
                 z1 = make_double2(f1.x, f1.y);
@@ -1334,8 +1650,6 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
             __syncthreads();
             /* stage 4: eigenvector of the smallest eigenvalue, refined */
             if (run) {
-                unsigned long long piv;
-
                 st |= eigvec(n, 0, w, ld, g, f0, f1, yr, lambda, norm, piv);
                 z0 = make_double2(f0.x, f0.y);
                 z1 = make_double2(f1.x, f1.y);
@@ -1344,8 +1658,10 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
             __syncthreads();
         }
         /* last stage: phasors, temporal coherence, outputs */
+        float2 ssum = make_float2(0.f, 0.f);
+
         if (run) {
-            const float gamma = gamma16(n, ld, w, g, z0, z1, upper_tab);
+            const float gamma = gamma16(n, ld, w, g, z0, z1, upper_tab, &ssum);
 
             if (active) {
                 if (g.gl == 0)
@@ -1365,11 +1681,21 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
                     status[out] = (unsigned char)st;
             }
         }
+        if (ADJ && q < nq) {
+            if (run)
+                backward16<EMI>(n, ld, w, g, z0, z1, ssum, yr, piv, looks, k.bias != 0, active,
+                                (float2 *)(smem + (size_t)grp * L.per_group + L.off_Tb),
+                                (double *)(smem + (size_t)grp * L.per_group + L.off_Db),
+                                upper_tab, gbar, c.npix, p);
+            else
+                for (int t = g.gl; t < tc_npu(n); t += 16)
+                    gbar[(long long)t * c.npix + p] = make_float2(0.f, 0.f);
+        }
         __syncthreads();
     }
 }
 
-HalfLayout half_layout(int n, int emi)
+HalfLayout half_layout(int n, int emi, int adj = 0)
 {
     HalfLayout L;
     int off = 0;
@@ -1399,6 +1725,8 @@ HalfLayout half_layout(int n, int emi)
     L.off_nrm = take(4 * 32);
     L.off_zs = take(8 * 32);
     L.off_lam = 0;
+    L.off_Tb = take(adj ? 8 * n * L.ld : 0);
+    L.off_Db = take(adj && emi ? 8 * n * L.ld : 0);
     L.per_group = off;
     return L;
 }
@@ -1415,15 +1743,16 @@ size_t tc_link_half_scratch_bytes(int n, int sms)
     return (size_t)sms * 16 * (2 * n * (n | 1) + 32) * sizeof(double);
 }
 
-cudaError_t tc_launch_link_half(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
-                                const float2 *gram, const int *count,
-                                const unsigned short *upper_tab, const unsigned short *pair_tab,
-                                double *scratch, float *coh, float *pairs, float *phases,
-                                unsigned char *status, int sms, cudaStream_t st)
+template <bool EMI, bool ADJ>
+static cudaError_t launch_half(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
+                               const float2 *gram, const int *count,
+                               const unsigned short *upper_tab, const unsigned short *pair_tab,
+                               double *scratch, float *coh, float *pairs, float *phases,
+                               unsigned char *status, float2 *gbar, int sms, cudaStream_t st)
 {
-    const HalfLayout L = half_layout(s.n, k.emi);
+    const HalfLayout L = half_layout(s.n, EMI, ADJ);
     const size_t per_warp = 2 * (size_t)L.per_group;
-    const int max_warps = k.emi ? 8 : 12;
+    const int max_warps = EMI || ADJ ? 8 : 12;
     int wpb = (int)((227 * 1024) / per_warp);
 
     if (wpb > max_warps)
@@ -1433,23 +1762,40 @@ cudaError_t tc_launch_link_half(const TcStrip &s, const TcChunk &c, const TcLink
     const size_t smem = per_warp * wpb;
     const int want = (c.npix / 2 + wpb - 1) / wpb;
     const int blocks = want < sms ? want : sms;
-    cudaError_t e;
+    cudaError_t e = cudaFuncSetAttribute(tc_link_half_kernel<EMI, ADJ>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 
-    if (k.emi) {
-        e = cudaFuncSetAttribute(tc_link_half_kernel<true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess)
-            tc_link_half_kernel<true><<<blocks, wpb * 32, smem, st>>>(
-                s, c, k, L, gram, count, upper_tab, pair_tab, scratch, coh, pairs, phases, status);
-    }
-    else {
-        e = cudaFuncSetAttribute(tc_link_half_kernel<false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess)
-            tc_link_half_kernel<false><<<blocks, wpb * 32, smem, st>>>(
-                s, c, k, L, gram, count, upper_tab, pair_tab, scratch, coh, pairs, phases, status);
-    }
     if (e != cudaSuccess)
         return e;
+    tc_link_half_kernel<EMI, ADJ><<<blocks, wpb * 32, smem, st>>>(
+        s, c, k, L, gram, count, upper_tab, pair_tab, scratch, coh, pairs, phases, status, gbar);
     return cudaGetLastError();
+}
+
+cudaError_t tc_launch_link_half(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
+                                const float2 *gram, const int *count,
+                                const unsigned short *upper_tab, const unsigned short *pair_tab,
+                                double *scratch, float *coh, float *pairs, float *phases,
+                                unsigned char *status, int sms, cudaStream_t st)
+{
+    if (k.emi)
+        return launch_half<true, false>(s, c, k, gram, count, upper_tab, pair_tab, scratch, coh,
+                                        pairs, phases, status, nullptr, sms, st);
+    return launch_half<false, false>(s, c, k, gram, count, upper_tab, pair_tab, scratch, coh,
+                                     pairs, phases, status, nullptr, sms, st);
+}
+
+cudaError_t tc_launch_link_adjoint(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
+                                   const float2 *gram, const int *count,
+                                   const unsigned short *upper_tab,
+                                   const unsigned short *pair_tab, double *scratch, float *coh,
+                                   float *pairs, float2 *gbar, int sms, cudaStream_t st)
+{
+    if (s.n > 32)
+        return cudaErrorInvalidValue;
+    if (k.emi)
+        return launch_half<true, true>(s, c, k, gram, count, upper_tab, pair_tab, scratch, coh,
+                                       pairs, nullptr, nullptr, gbar, sms, st);
+    return launch_half<false, true>(s, c, k, gram, count, upper_tab, pair_tab, scratch, coh,
+                                    pairs, nullptr, nullptr, gbar, sms, st);
 }

@@ -86,8 +86,18 @@ int tc_geometry_grid(const TcGeo &g, const struct tc_orbit *orbits, double *grid
                      cudaStream_t st);
 cudaError_t tc_launch_prep_raw(int n, const float *re, const float *im, const double *elev,
                                int row0, int region_rows, int padded_rows, int cols, int halo,
-                               const TcGeo *g, const double *grid, float *slc, float *amp,
-                               unsigned char *valid, cudaStream_t st);
+                               const TcGeo *g, const double *grid, const double *dh,
+                               const float *psi, float *slc, float *amp, unsigned char *valid,
+                               cudaStream_t st);
+/* Adjoint (adjoint.cu): dL/dtheta += the chunk's contribution (dtheta
+   [n][padded_rows][cols], zeroed by the caller); dL/ddh from dL/dtheta. */
+cudaError_t tc_launch_adjoint_scatter(const TcStrip &s, const TcChunk &c, int halo,
+                                      const float2 *gbar, const uint32_t *mask,
+                                      const float *slc, float *dtheta, cudaStream_t st);
+cudaError_t tc_launch_adjoint_height(int n, int padded_rows, int cols, int row0, int region_rows,
+                                     const double *elev, const double *dh, const TcGeo *g,
+                                     const double *grid, const float *dtheta, float *gdh,
+                                     cudaStream_t st);
 
 /* Helpers of abi.cu shared with the other translation units. */
 int tc_error(int code, const char *fmt, ...);
@@ -128,5 +138,13 @@ cudaError_t tc_launch_link_half(const TcStrip &s, const TcChunk &c, const TcLink
                                 double *scratch, float *coh, float *pairs, float *phases,
                                 unsigned char *status, int sms, cudaStream_t st);
 size_t tc_link_half_scratch_bytes(int n, int sms);
+/* The link stage with the adjoint (n <= 32): gamma into coh, and into gbar
+   (layout of gram) the gradient of gamma with respect to each pixel's
+   coherence sums, zero for the pixels not estimated. */
+cudaError_t tc_launch_link_adjoint(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
+                                   const float2 *gram, const int *count,
+                                   const unsigned short *upper_tab,
+                                   const unsigned short *pair_tab, double *scratch, float *coh,
+                                   float *pairs, float2 *gbar, int sms, cudaStream_t st);
 
 #endif

@@ -214,6 +214,23 @@ int tc_run_raw_device(struct ocl *o, const float *re, const float *im,
                       int rows, int cols, float *coh, int *count, float *pairs,
                       float *phases, unsigned char *status, void *stream);
 
+/* Adjoint of the temporal coherence (no counterpart in the reference,
+   whose module only evaluates it). The objective is L = the sum of gamma
+   over the strip's estimated pixels, as a function of the phase removed
+   from every sample, theta_k = phi_k(h + dh) + psi_k: the attached
+   geometry's phase (tc_set_geometry; none: phi = 0) at the cell's height
+   (elevation, else h0) plus a height error dh, and a per-date phase screen
+   psi. Arguments as tc_run_raw, plus dh double [padded_rows][cols] and psi
+   float [ndates][padded_rows][cols] (either NULL for zero). Outputs: coh
+   and count of the forward, grad_psi float [ndates][padded_rows][cols] =
+   dL/dpsi = dL/dtheta, and grad_dh float [padded_rows][cols] = dL/ddh (NULL
+   to skip; zero without three height levels). Stacks of up to 32 dates;
+   the SHP selection depends on the amplitudes only and is held fixed. */
+int tc_adjoint_raw(struct ocl *o, const float *re, const float *im, const double *elevation,
+                   const double *dh, const float *psi, int row0, int region_rows,
+                   int padded_rows, int rows, int cols, float *coh, int *count,
+                   float *grad_dh, float *grad_psi);
+
 /* Stage timing. With timing on, every launch of the following runs is
    bracketed by CUDA events on its stream, and tc_stage_stats gives, per
    stage, the device milliseconds summed over the last run and the number

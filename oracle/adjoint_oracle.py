@@ -170,4 +170,4 @@ def adjoint(re, im, heights, dh, psi, row0, region_rows, halo_cols, mask, count,
     total, gam = gamma_sum(a, mask, count, window, min_looks, estimator, bias)
     total.backward()
     g_dh = dh_t.grad.numpy() if dh_t.grad is not None else np.zeros_like(np.asarray(dh))
-    return float(total), gam, g_dh, psi_t.grad.numpy()
+    return float(total.detach()), gam, g_dh, psi_t.grad.numpy()
