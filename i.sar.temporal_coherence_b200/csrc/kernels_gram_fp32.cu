@@ -7,7 +7,7 @@
  * matrix and accumulates the block in registers, reading the candidates'
  * samples from the date-major planes so that the 32 lanes of a warp (8
  * consecutive columns of 4 rows) load contiguous 64-byte runs. Output is the
- * packed upper triangle, gram[tc_pidx(i, j)][p] (float2: re, im).
+ * packed upper triangle, pixel-major: gram[p][tc_pidx(i, j)] (float2: re, im).
  */
 #include "tcoh_internal.h"
 
@@ -75,7 +75,7 @@ tc_gram_fp32_kernel(TcStrip s, TcChunk c, const float2 *__restrict__ soa,
                     const int i = I * B + a, j = J * B + b2;
 
                     if (i < n && j < n && i <= j)
-                        gram[(long long)tc_pidx(n, i, j) * c.npix + p] =
+                        gram[tc_gram_at(tc_npu(n), p, tc_pidx(n, i, j))] =
                             i == j ? make_float2(acc[a][b2].x, 0.f) : acc[a][b2];
                 }
         }

@@ -28,7 +28,7 @@
  * without swizzle (8-row x 16-byte core matrices), and one thread issues the
  * MMAs (M = 128, N = 2h, K = 16) and commits them to an mbarrier; the next
  * block's samples load while they run. The epilogue reads the accumulator
- * with tcgen05.ld and writes gram[pidx][p] (float2), the layout the linking
+ * with tcgen05.ld and writes gram[p][pidx] (float2), the layout the linking
  * kernels read.
  *
  * Candidates that are not finite contribute zero: a product with A = 0 must
@@ -421,9 +421,14 @@ tc_gram_tc_kernel(TcStrip s, TcChunk c, int terms, const float2 *__restrict__ sl
         /* epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (pixels), half
            of the phase's 16-entry column groups */
         {
-            const int lg = warp & 3, pm = lg * 32 + lane;
-            const long long p = (long long)tile * TC_TILE_PIX + pm;
+            const int lg = warp & 3;
             const uint32_t lane_addr = tmem + ((uint32_t)(lg * 32) << 16);
+
+            /* The warp's 32 pixels x 16 entries go through shared memory
+               (the B operand's region, idle until the next phase's first
+               barrier) so that each store writes two pixels' 16
+               consecutive entries: whole 128-byte lines. */
+            float2 *stg = (float2 *)sB + warp * 32 * 17;
 
             for (int cg = warp >> 2; cg * 16 < np; cg += 2) {
                 uint32_t vr[16], vi[16];
@@ -433,16 +438,24 @@ tc_gram_tc_kernel(TcStrip s, TcChunk c, int terms, const float2 *__restrict__ sl
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
                 for (int k = 0; k < 16; k++) {
-                    const int r = cg * 16 + k;
+                    const int r = cg * 16 + k, pr = r < np ? s_pair[P0 + r] : 0;
 
-                    if (r < np) {
-                        const int q = P0 + r, pr = s_pair[q];
-
-                        gram[(long long)q * c.npix + p] =
-                            make_float2(__uint_as_float(vr[k]),
-                                        (pr >> 8) == (pr & 255) ? 0.f : __uint_as_float(vi[k]));
-                    }
+                    stg[lane * 17 + k] =
+                        make_float2(__uint_as_float(vr[k]),
+                                    (pr >> 8) == (pr & 255) ? 0.f : __uint_as_float(vi[k]));
                 }
+                __syncwarp();
+                const int k = lane & 15, r = cg * 16 + k;
+
+#pragma unroll 4
+                for (int it = 0; it < 16; it++) {
+                    const int px = 2 * it + (lane >> 4);
+
+                    if (r < np)
+                        gram[tc_gram_at(npu, (long long)tile * TC_TILE_PIX + lg * 32 + px,
+                                        P0 + r)] = stg[px * 17 + k];
+                }
+                __syncwarp();
             }
         }
         fence_before();
@@ -453,7 +466,7 @@ tc_gram_tc_kernel(TcStrip s, TcChunk c, int terms, const float2 *__restrict__ sl
         if (pending)
             mbar_wait(bar, parity);
         for (int e = t; e < npu * TC_TILE_PIX; e += THREADS)
-            gram[(long long)(e >> 7) * c.npix + (long long)tile * TC_TILE_PIX + (e & 127)] =
+            gram[tc_gram_at(npu, (long long)tile * TC_TILE_PIX + (e & 127), e >> 7)] =
                 make_float2(__int_as_float(0x7fc00000), __int_as_float(0x7fc00000));
     }
     __syncthreads();

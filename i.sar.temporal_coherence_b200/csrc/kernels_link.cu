@@ -749,7 +749,7 @@ __device__ void load_coherence(const TcStrip &s, const TcChunk &c, const TcLinkC
     const int n = s.n, npu = tc_npu(n);
 
     for (int r = lane; r < n; r += 32)
-        w.nrm[r] = __fsqrt_rn(gram[(long long)tc_pidx(n, r, r) * c.npix + p].x);
+        w.nrm[r] = __fsqrt_rn(gram[tc_gram_at(tc_npu(n), p, tc_pidx(n, r, r))].x);
     __syncwarp();
     const float fl = (float)looks;
 
@@ -760,7 +760,7 @@ __device__ void load_coherence(const TcStrip &s, const TcChunk &c, const TcLinkC
             w.T[i * ld + i] = make_float2(1.f, 0.f);
             continue;
         }
-        const float2 g = gram[(long long)q * c.npix + p];
+        const float2 g = gram[tc_gram_at(tc_npu(n), p, q)];
         const float dd = __fmul_rn(w.nrm[i], w.nrm[j]);
         float re = 0.f, im = 0.f;
 

@@ -1039,13 +1039,13 @@ __device__ void load_T(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
     float2 gv[33];
 
     /* every load issued before any use */
-    const float d0 = (active && i0 < n) ? gram[(long long)tc_pidx(n, i0, i0) * c.npix + p].x : 1.f;
-    const float d1 = (active && i1 < n) ? gram[(long long)tc_pidx(n, i1, i1) * c.npix + p].x : 1.f;
+    const float d0 = (active && i0 < n) ? gram[tc_gram_at(npu, p, tc_pidx(n, i0, i0))].x : 1.f;
+    const float d1 = (active && i1 < n) ? gram[tc_gram_at(npu, p, tc_pidx(n, i1, i1))].x : 1.f;
 #pragma unroll
     for (int t = 0; t < 33; t++) {
         const int q = g.gl + 16 * t;
 
-        gv[t] = (active && q < npu) ? gram[(long long)q * c.npix + p] : make_float2(0.f, 0.f);
+        gv[t] = (active && q < npu) ? gram[tc_gram_at(npu, p, q)] : make_float2(0.f, 0.f);
     }
     if (i0 < n)
         w.nrm[i0] = __fsqrt_rn(d0);

@@ -52,6 +52,13 @@ struct TcLinkConst {
 
 __host__ __device__ inline int tc_npu(int n) { return n * (n + 1) / 2; }
 
+/* The coherence sums of a chunk are float2 [npix][npu], pixel-major: the
+   lanes that load one pixel's matrix read contiguous bytes. */
+__host__ __device__ inline long long tc_gram_at(int npu, long long p, int q)
+{
+    return p * npu + q;
+}
+
 /* Packed upper-triangle index of (i, j), i <= j. */
 __host__ __device__ inline int tc_pidx(int n, int i, int j)
 {
