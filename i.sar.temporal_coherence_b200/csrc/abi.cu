@@ -217,6 +217,10 @@ static cudaError_t ensure(DevBuf &b, size_t size)
 
 enum { ST_PREP, ST_SHP, ST_GRAM, ST_LINK, ST_COPY, ST_COUNT };
 
+/* tc_run_ex copies a strip in this many row blocks on a second stream, and
+   each chunk waits only for the blocks holding its rows. */
+#define TC_COPY_BLOCKS 32
+
 struct ocl {
     int device;
     int sms;
@@ -226,6 +230,8 @@ struct ocl {
     tc_options opt;
     int gram_block;
     cudaStream_t stream;
+    cudaStream_t copy_stream; /* host -> device copies of tc_run_ex, by row blocks */
+    cudaEvent_t block_done[TC_COPY_BLOCKS];
     DevBuf slc, amp, valid, coh, count, pairs, phases, status;
     DevBuf soa, logstat, mask, gram, upper_tab, pair_tab, link_scratch;
     DevBuf raw_re, raw_im, raw_elev, geo_grid, adj_dh, adj_psi, adj_gbar, adj_dtheta, adj_gdh;
@@ -385,9 +391,13 @@ TC_API int tc_open(int device, const struct settings *s, int padded_cols,
 
     cudaError_t e = cudaStreamCreateWithFlags(&o->stream, cudaStreamNonBlocking);
 
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithFlags(&o->copy_stream, cudaStreamNonBlocking);
+    for (int b = 0; b < TC_COPY_BLOCKS && e == cudaSuccess; b++)
+        e = cudaEventCreateWithFlags(&o->block_done[b], cudaEventDisableTiming);
     if (e != cudaSuccess) {
         delete o;
-        return set_error(TC_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+        return set_error(TC_ERR_CUDA, "stream / event creation: %s", cudaGetErrorString(e));
     }
     /* Date pairs of the packed upper triangle and of the pair planes. */
     {
@@ -416,6 +426,9 @@ TC_API int tc_open(int device, const struct settings *s, int padded_cols,
         free(pt);
         if (e != cudaSuccess) {
             free_bufs(o);
+            for (int b = 0; b < TC_COPY_BLOCKS; b++)
+                cudaEventDestroy(o->block_done[b]);
+            cudaStreamDestroy(o->copy_stream);
             cudaStreamDestroy(o->stream);
             delete o;
             return set_error(TC_ERR_CUDA, "table upload: %s", cudaGetErrorString(e));
@@ -440,7 +453,11 @@ TC_API int tc_close(struct ocl *o)
         return TC_OK;
     cudaSetDevice(o->device);
     cudaStreamSynchronize(o->stream);
+    cudaStreamSynchronize(o->copy_stream);
     free_bufs(o);
+    for (int b = 0; b < TC_COPY_BLOCKS; b++)
+        cudaEventDestroy(o->block_done[b]);
+    cudaStreamDestroy(o->copy_stream);
     cudaStreamDestroy(o->stream);
     delete o;
     return TC_OK;
@@ -553,11 +570,18 @@ struct AdjRun {
     float *dtheta;
 };
 
+/* Padded rows still arriving by blocks: block b (rows b * block_rows ..)
+   is complete once block_done[b] has fired. */
+struct RowsReady {
+    int block_rows, nblocks;
+    const cudaEvent_t *done;
+};
+
 static int run_device(struct ocl *o, const float *slc, const float *amp,
                       const unsigned char *valid, int padded_rows, int rows, int cols,
                       float *coh, int *count, float *pairs, float *phases,
                       unsigned char *status, cudaStream_t st, Timer &tm,
-                      const AdjRun *adj = nullptr)
+                      const AdjRun *adj = nullptr, const RowsReady *ready = nullptr)
 {
     if (rows < 1 || cols < 1)
         return set_error(TC_ERR_ARG, "empty strip (%d x %d)", rows, cols);
@@ -601,6 +625,9 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
 
     int t;
 
+    /* the date-plane transpose and the log statistics read the whole strip */
+    if (ready && (o->opt.gram == TC_GRAM_FP32 || o->test == SHP_TLOG))
+        CK(cudaStreamWaitEvent(st, ready->done[ready->nblocks - 1], 0));
     if (o->opt.gram == TC_GRAM_FP32) {
         t = tm.begin(ST_PREP);
         CK(tc_launch_prep(s, slc, (float2 *)o->soa.p, st));
@@ -626,6 +653,14 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
         c.tiles_x = tiles_x;
         c.tiles_y = (c.nrows + TC_TILE_H - 1) / TC_TILE_H;
         c.npix = c.tiles_x * c.tiles_y * TC_TILE_PIX;
+        if (ready) {
+            const int last = row0 + c.nrows + o->wa - 2; /* last padded row read */
+            int b = last / ready->block_rows;
+
+            if (b >= ready->nblocks)
+                b = ready->nblocks - 1;
+            CK(cudaStreamWaitEvent(st, ready->done[b], 0));
+        }
 
         t = tm.begin(ST_SHP);
         CK(tc_launch_shp(s, c, o->shp, amp, valid, (const float2 *)o->logstat.p,
@@ -772,13 +807,47 @@ TC_API int tc_run_ex(struct ocl *o, const float *slc, const float *amp,
 
     if (rc != TC_OK)
         return rc;
-    int t = tm.begin(ST_COPY);
+    /* the strip goes over in row blocks on the copy stream; each chunk
+       waits for the blocks that hold its rows */
+    const size_t W = o->padded_cols;
+    const int block_rows = (padded_rows + TC_COPY_BLOCKS - 1) / TC_COPY_BLOCKS;
+    RowsReady ready;
 
-    CK(cudaMemcpyAsync(o->slc.p, slc, npad * n * 2 * sizeof(float), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(o->amp.p, amp, npad * n * sizeof(float), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(o->valid.p, valid, npad, cudaMemcpyHostToDevice, st));
-    tm.end(t);
-    return run_context_buffers(o, padded_rows, rows, cols, coh, count, pairs, phases, status, tm);
+    ready.block_rows = block_rows;
+    ready.nblocks = (padded_rows + block_rows - 1) / block_rows;
+    ready.done = o->block_done;
+    /* work already queued on the context's stream may still read the strip
+       buffers (a wait captures the event as recorded at the call) */
+    CK(cudaEventRecord(o->block_done[0], st));
+    CK(cudaStreamWaitEvent(o->copy_stream, o->block_done[0], 0));
+    for (int b = 0; b < ready.nblocks; b++) {
+        const size_t r0 = (size_t)b * block_rows;
+        const size_t nr = (size_t)(b + 1 < ready.nblocks ? block_rows : padded_rows - r0);
+        const size_t px = r0 * W, np_ = nr * W;
+
+        CK(cudaMemcpyAsync((float *)o->slc.p + px * n * 2, slc + px * n * 2,
+                           np_ * n * 2 * sizeof(float), cudaMemcpyHostToDevice, o->copy_stream));
+        CK(cudaMemcpyAsync((float *)o->amp.p + px * n, amp + px * n, np_ * n * sizeof(float),
+                           cudaMemcpyHostToDevice, o->copy_stream));
+        CK(cudaMemcpyAsync((unsigned char *)o->valid.p + px, valid + px, np_,
+                           cudaMemcpyHostToDevice, o->copy_stream));
+        CK(cudaEventRecord(o->block_done[b], o->copy_stream));
+    }
+    const size_t nout = (size_t)rows * cols;
+
+    rc = run_device(o, (const float *)o->slc.p, (const float *)o->amp.p,
+                    (const unsigned char *)o->valid.p, padded_rows, rows, cols, (float *)o->coh.p,
+                    (int *)o->count.p, o->npairs ? (float *)o->pairs.p : nullptr,
+                    phases ? (float *)o->phases.p : nullptr,
+                    status ? (unsigned char *)o->status.p : nullptr, st, tm, nullptr, &ready);
+
+    if (rc != TC_OK) {
+        cudaStreamSynchronize(o->copy_stream);
+        cudaStreamSynchronize(st);
+        tm.collect();
+        return rc;
+    }
+    return fetch(o, nout, coh, count, pairs, phases, status, tm);
 }
 
 /* ------------------------------------------------------------------ */
