@@ -154,33 +154,31 @@ tc_shp_kernel(TcStrip s, TcChunk c, TcShpConst k, const float *__restrict__ amp,
                         for (int j = 0; j < n; j++)
                             b_s[j * 32 + lane] = b[j];
                         b_s[n * 32 + lane] = INFINITY;
-                        /* Merge walk, centre first on ties: 2N - 1 steps,
-                           branch-free; a side that ran out is never taken. */
-                        int ia = 0, ib = 0;
+                        /* Merge walk, centre first on ties: 2N - 1 steps.
+                           Both series end in an INFINITY sentinel, so a
+                           side that ran out is never taken without bound
+                           checks; after step j, ib = j - ia. */
+                        const float *bl = b_s + lane;
+                        int ia = 0;
 
                         if (TEST == 0) {
                             int d = 0;
 
-                            for (int st = 0; st < 2 * n - 1; st++) {
-                                const bool take_a =
-                                    ia < n && (ib >= n || a_s[ia] <= b_s[ib * 32 + lane]);
-
-                                ia += take_a;
-                                ib += !take_a;
-                                d = max(d, abs(ia - ib));
+#pragma unroll 4
+                            for (int j = 1; j < 2 * n; j++) {
+                                ia += a_s[ia] <= bl[(j - 1 - ia) * 32];
+                                d = max(d, abs(2 * ia - j));
                             }
                             ok = d <= k.ks_max;
                         }
                         else {
                             float acc = 0.f;
+                            const float *tj = tab;
 
-                            for (int j = 1; j < 2 * n; j++) {
-                                const bool take_a =
-                                    ia < n && (ib >= n || a_s[ia] <= b_s[ib * 32 + lane]);
-
-                                ia += take_a;
-                                ib += !take_a;
-                                acc = __fadd_rn(acc, tab[(j - 1) * (n + 1) + ia]);
+#pragma unroll 4
+                            for (int j = 1; j < 2 * n; j++, tj += n + 1) {
+                                ia += a_s[ia] <= bl[(j - 1 - ia) * 32];
+                                acc = __fadd_rn(acc, tj[ia]);
                             }
                             ok = __fdiv_rn(__fsub_rn(__fmul_rn(k.ad_norm, acc), 1.0f),
                                            k.ad_sigma) <= k.ad_crit;
