@@ -19,6 +19,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <vector>
 
 #define TC_API extern "C" __attribute__((visibility("default")))
 
@@ -232,6 +233,8 @@ struct ocl {
     cudaStream_t stream;
     cudaStream_t copy_stream; /* host -> device copies of tc_run_ex, by row blocks */
     cudaEvent_t block_done[TC_COPY_BLOCKS];
+    cudaStream_t out_stream;  /* device -> host copies of the outputs, by chunks */
+    std::vector<cudaEvent_t> chunk_done;
     DevBuf slc, amp, valid, coh, count, pairs, phases, status;
     DevBuf soa, logstat, mask, gram, upper_tab, pair_tab, link_scratch;
     DevBuf raw_re, raw_im, raw_elev, geo_grid, adj_dh, adj_psi, adj_gbar, adj_dtheta, adj_gdh;
@@ -393,6 +396,8 @@ TC_API int tc_open(int device, const struct settings *s, int padded_cols,
 
     if (e == cudaSuccess)
         e = cudaStreamCreateWithFlags(&o->copy_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithFlags(&o->out_stream, cudaStreamNonBlocking);
     for (int b = 0; b < TC_COPY_BLOCKS && e == cudaSuccess; b++)
         e = cudaEventCreateWithFlags(&o->block_done[b], cudaEventDisableTiming);
     if (e != cudaSuccess) {
@@ -428,6 +433,7 @@ TC_API int tc_open(int device, const struct settings *s, int padded_cols,
             free_bufs(o);
             for (int b = 0; b < TC_COPY_BLOCKS; b++)
                 cudaEventDestroy(o->block_done[b]);
+            cudaStreamDestroy(o->out_stream);
             cudaStreamDestroy(o->copy_stream);
             cudaStreamDestroy(o->stream);
             delete o;
@@ -454,9 +460,13 @@ TC_API int tc_close(struct ocl *o)
     cudaSetDevice(o->device);
     cudaStreamSynchronize(o->stream);
     cudaStreamSynchronize(o->copy_stream);
+    cudaStreamSynchronize(o->out_stream);
     free_bufs(o);
     for (int b = 0; b < TC_COPY_BLOCKS; b++)
         cudaEventDestroy(o->block_done[b]);
+    for (cudaEvent_t ev : o->chunk_done)
+        cudaEventDestroy(ev);
+    cudaStreamDestroy(o->out_stream);
     cudaStreamDestroy(o->copy_stream);
     cudaStreamDestroy(o->stream);
     delete o;
@@ -581,7 +591,8 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
                       const unsigned char *valid, int padded_rows, int rows, int cols,
                       float *coh, int *count, float *pairs, float *phases,
                       unsigned char *status, cudaStream_t st, Timer &tm,
-                      const AdjRun *adj = nullptr, const RowsReady *ready = nullptr)
+                      const AdjRun *adj = nullptr, const RowsReady *ready = nullptr,
+                      bool mark_chunks = false)
 {
     if (rows < 1 || cols < 1)
         return set_error(TC_ERR_ARG, "empty strip (%d x %d)", rows, cols);
@@ -645,6 +656,16 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
     lk.min_looks = o->min_looks;
     lk.npairs = o->npairs;
     lk.pairs_all = o->pairs_all;
+    if (mark_chunks) {
+        const size_t nchunks = (size_t)((rows + crows - 1) / crows);
+
+        while (o->chunk_done.size() < nchunks) {
+            cudaEvent_t ev;
+
+            CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            o->chunk_done.push_back(ev);
+        }
+    }
     for (int row0 = 0; row0 < rows; row0 += crows) {
         TcChunk c;
 
@@ -691,6 +712,8 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
                                          slc, adj->dtheta, st));
         }
         tm.end(t);
+        if (mark_chunks)
+            CK(cudaEventRecord(o->chunk_done[row0 / crows], st));
     }
     return TC_OK;
 }
@@ -718,32 +741,6 @@ TC_API int tc_run_device(struct ocl *o, const float *slc, const float *amp,
     return rc;
 }
 
-/* Outputs of a run on the context's device buffers, back to the host. */
-static int fetch(struct ocl *o, size_t nout, float *coh, int *count, float *pairs, float *phases,
-                 unsigned char *status, Timer &tm)
-{
-    cudaStream_t st = o->stream;
-    const int t = tm.begin(ST_COPY);
-
-    CK(cudaMemcpyAsync(coh, o->coh.p, nout * sizeof(float), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(count, o->count.p, nout * sizeof(int), cudaMemcpyDeviceToHost, st));
-    if (o->npairs && pairs)
-        CK(cudaMemcpyAsync(pairs, o->pairs.p, o->npairs * nout * sizeof(float),
-                           cudaMemcpyDeviceToHost, st));
-    if (phases)
-        CK(cudaMemcpyAsync(phases, o->phases.p, nout * o->n * sizeof(float),
-                           cudaMemcpyDeviceToHost, st));
-    if (status)
-        CK(cudaMemcpyAsync(status, o->status.p, nout, cudaMemcpyDeviceToHost, st));
-    tm.end(t);
-    CK(cudaStreamSynchronize(st));
-    tm.collect();
-    if (o->opt.gram == TC_GRAM_TENSOR && tc_gram_tensor_fault() > 0)
-        return set_error(TC_ERR_DEVICE, "tensor-core Gram: a wait for MMA completion ran out; "
-                         "the tiles concerned are NULL");
-    return TC_OK;
-}
-
 /* Device output buffers of the context for a strip of nout pixels. */
 static int ensure_outputs(struct ocl *o, size_t nout, bool phases, bool status)
 {
@@ -758,24 +755,73 @@ static int ensure_outputs(struct ocl *o, size_t nout, bool phases, bool status)
     return TC_OK;
 }
 
+/* The outputs of a run on the context's buffers back to the host, chunk
+   by chunk on the output stream as each chunk's kernels complete: all the
+   strip's kernels are queued first, so the GPU keeps computing even where
+   the host buffers are pageable and a copy holds the calling thread. */
+static int stream_outputs(struct ocl *o, int rows, int cols, float *coh, int *count,
+                          float *pairs, float *phases, unsigned char *status)
+{
+    const int crows = chunk_rows_for(o, rows, cols);
+    const size_t plane = (size_t)rows * cols;
+    cudaStream_t os = o->out_stream;
+
+    for (int row0 = 0; row0 < rows; row0 += crows) {
+        const int nr = rows - row0 < crows ? rows - row0 : crows;
+        const size_t at = (size_t)row0 * cols, np_ = (size_t)nr * cols;
+
+        CK(cudaStreamWaitEvent(os, o->chunk_done[row0 / crows], 0));
+        CK(cudaMemcpyAsync(coh + at, (float *)o->coh.p + at, np_ * sizeof(float),
+                           cudaMemcpyDeviceToHost, os));
+        CK(cudaMemcpyAsync(count + at, (int *)o->count.p + at, np_ * sizeof(int),
+                           cudaMemcpyDeviceToHost, os));
+        if (o->npairs && pairs)
+            CK(cudaMemcpy2DAsync(pairs + at, plane * sizeof(float), (float *)o->pairs.p + at,
+                                 plane * sizeof(float), np_ * sizeof(float), o->npairs,
+                                 cudaMemcpyDeviceToHost, os));
+        if (phases)
+            CK(cudaMemcpyAsync(phases + at * o->n, (float *)o->phases.p + at * o->n,
+                               np_ * o->n * sizeof(float), cudaMemcpyDeviceToHost, os));
+        if (status)
+            CK(cudaMemcpyAsync(status + at, (unsigned char *)o->status.p + at, np_,
+                               cudaMemcpyDeviceToHost, os));
+    }
+    return TC_OK;
+}
+
+static int finish_run(struct ocl *o, Timer &tm)
+{
+    CK(cudaStreamSynchronize(o->stream));
+    CK(cudaStreamSynchronize(o->out_stream));
+    tm.collect();
+    if (o->opt.gram == TC_GRAM_TENSOR && tc_gram_tensor_fault() > 0)
+        return set_error(TC_ERR_DEVICE, "tensor-core Gram: a wait for MMA completion ran out; "
+                         "the tiles concerned are NULL");
+    return TC_OK;
+}
+
 static int run_context_buffers(struct ocl *o, int padded_rows, int rows, int cols, float *coh,
                                int *count, float *pairs, float *phases, unsigned char *status,
-                               Timer &tm)
+                               Timer &tm, const RowsReady *ready = nullptr)
 {
-    const size_t nout = (size_t)rows * cols;
     int rc = run_device(o, (const float *)o->slc.p, (const float *)o->amp.p,
                         (const unsigned char *)o->valid.p, padded_rows, rows, cols,
                         (float *)o->coh.p, (int *)o->count.p,
                         o->npairs ? (float *)o->pairs.p : nullptr,
                         phases ? (float *)o->phases.p : nullptr,
-                        status ? (unsigned char *)o->status.p : nullptr, o->stream, tm);
+                        status ? (unsigned char *)o->status.p : nullptr, o->stream, tm, nullptr,
+                        ready, true);
 
+    if (rc == TC_OK)
+        rc = stream_outputs(o, rows, cols, coh, count, pairs, phases, status);
     if (rc != TC_OK) {
+        cudaStreamSynchronize(o->copy_stream);
+        cudaStreamSynchronize(o->out_stream);
         cudaStreamSynchronize(o->stream);
         tm.collect();
         return rc;
     }
-    return fetch(o, nout, coh, count, pairs, phases, status, tm);
+    return finish_run(o, tm);
 }
 
 TC_API int tc_run_ex(struct ocl *o, const float *slc, const float *amp,
@@ -833,21 +879,8 @@ TC_API int tc_run_ex(struct ocl *o, const float *slc, const float *amp,
                            cudaMemcpyHostToDevice, o->copy_stream));
         CK(cudaEventRecord(o->block_done[b], o->copy_stream));
     }
-    const size_t nout = (size_t)rows * cols;
-
-    rc = run_device(o, (const float *)o->slc.p, (const float *)o->amp.p,
-                    (const unsigned char *)o->valid.p, padded_rows, rows, cols, (float *)o->coh.p,
-                    (int *)o->count.p, o->npairs ? (float *)o->pairs.p : nullptr,
-                    phases ? (float *)o->phases.p : nullptr,
-                    status ? (unsigned char *)o->status.p : nullptr, st, tm, nullptr, &ready);
-
-    if (rc != TC_OK) {
-        cudaStreamSynchronize(o->copy_stream);
-        cudaStreamSynchronize(st);
-        tm.collect();
-        return rc;
-    }
-    return fetch(o, nout, coh, count, pairs, phases, status, tm);
+    return run_context_buffers(o, padded_rows, rows, cols, coh, count, pairs, phases, status,
+                               tm, &ready);
 }
 
 /* ------------------------------------------------------------------ */
