@@ -40,6 +40,11 @@ sys.path.insert(0, ROOT)
 WORKLOAD = dict(n=30, rows=4096, cols=4096, window=(21, 7), shp_test="ad", alpha=0.05,
                 min_shp=20, estimator="emi", bias=True, nregions=32, g0_max=0.99, spacing=12.0)
 METRIC = "Mpixel/s temporal coherence at N=30, 21x7 window, <=1e-4 vs FP64"
+# DRAM bytes (read + write) per pixel of one phase-linking launch, from an
+# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of one
+# 65,536-pixel chunk at N=30, AD / EMI / bias correction: 244.4 MB read (the
+# packed Gram, 465 x 8 B per pixel, read once) + 7.1 MB written.
+LINK_DRAM_BYTES_PER_PIXEL = 251.5e6 / 65536
 
 
 def parse():
@@ -52,6 +57,11 @@ def parse():
     p.add_argument("--cols", type=int, default=WORKLOAD["cols"])
     p.add_argument("--gram", default="tensor", choices=["tensor", "fp32"],
                    help="arithmetic of the coherence matrices (the tensor cores, else plain FP32)")
+    p.add_argument("--workload", default="emi", choices=["emi", "adjoint"],
+                   help="emi: the metric's configuration (default); adjoint: forward + "
+                        "adjoint with geometry, a height error and a phase screen, and 20 "
+                        "steps of gradient ascent on the height error (2048 x 2048 unless "
+                        "--rows / --cols)")
     p.add_argument("--no-extras", action="store_true",
                    help="skip the e2e, plain-FP32, CPU and accuracy legs")
     return p.parse_args()
@@ -236,8 +246,111 @@ def accuracy(slc, amp, valid, coh_gpu, count_gpu, rows, cols, kw, size=48):
 
 # ---------------------------------------------------------------------------
 
+def adjoint_workload(args):
+    """Forward + adjoint throughput and a height-error ascent.
+
+    N=30, 2048 x 2048 (unless --rows / --cols), synthetic distributed
+    scatterers (32 regions, coherence <= 0.99), synthetic orbits and a
+    fractal height field (0 - 2000 m); the simulated samples carry the
+    geometric phase at the true heights h + dh_true (dh_true: N(0, 15 m)
+    smoothed over 9 x 9 and rescaled to 15 m RMS) and a per-date fractal
+    phase screen (0 - 2 rad). The module removes the phase at h + dh and the
+    screen psi; starting from dh = psi = 0, each step is one forward +
+    adjoint (tc_adjoint_raw, host buffers) and an Adam step. The variable is
+    u with dh = S u, S the 9 x 9 box average (its gradient S dL/d(dh)):
+    gamma only sees height differences inside a window, and a free per-pixel
+    dh fits the speckle instead of the height error (plain Adam on dh raises
+    gamma further while the height error grows). Reported: Mpixel/s of
+    forward + adjoint, mean gamma and the RMS of dh - dh_true (mean removed:
+    gamma does not see a height offset common to a window) before and after
+    the ascent, and mean gamma at dh = dh_true."""
+    import numpy as np
+    import torch
+
+    import tcoh_b200
+    import tcoh_b200.scene as scene
+    import tcoh_b200.synthetic as syn
+
+    n = 30
+    rows = args.rows if args.rows != WORKLOAD["rows"] else 2048
+    cols = args.cols if args.cols != WORKLOAD["cols"] else 2048
+    ha, hr = 10, 3
+    geo, orbits = scene.acquisition(n, rows, cols, seed=11)
+    h = scene.fbm_heights(rows, cols, hurst=0.8, hmax=2000.0, seed=12)
+    rng = np.random.default_rng(13)
+    dh_true = scene.smooth(rng.normal(0.0, 15.0, (rows, cols)), 9)
+    dh_true *= 15.0 / dh_true.std()
+    screen = np.stack([scene.fbm_heights(rows, cols, hurst=0.8, hmax=2.0, seed=100 + k)
+                       for k in range(n)])
+    g = tcoh_b200.make_geometry(heights=h, h0=0.0, **geo)
+    grid = tcoh_b200.geometry_grid(g, orbits)
+    levels = ([g.hmin, 0.5 * (g.hmin + g.hmax), g.hmax] if grid.shape[2] == 3
+              else [0.5 * (g.hmin + g.hmax)])
+    phase = scene.grid_phases(grid, levels, h + dh_true) + screen
+    stack = syn.generate(n, rows, cols, nregions=32, g0_max=0.99, seed=14, null_frac=0.0)
+    stack = (stack * np.exp(-1j * phase)).astype(np.complex64)
+    del phase
+    prow = rows + 2 * ha
+    re = np.full((n, prow, cols), np.nan, np.float32)
+    im = re.copy()
+    re[:, ha:ha + rows] = stack.real
+    im[:, ha:ha + rows] = stack.imag
+    del stack
+    elev = np.zeros((prow, cols))
+    elev[ha:ha + rows] = h
+    s = tcoh_b200.make_settings(n, window=(21, 7), shp_test="tlog", alpha=0.05, min_shp=20,
+                                estimator="evd")
+    be = tcoh_b200.Backend(s, cols + 2 * hr)
+    be.set_geometry(g, grid)
+    u = np.zeros((prow, cols))
+    dh = u
+    m_t, v_t = np.zeros_like(u), np.zeros_like(u)
+    lr, b1, b2, box = 2.0, 0.9, 0.999, 9
+    inner = (slice(ha, ha + rows), slice(None))
+
+    def err(d):
+        e = d[inner] - dh_true
+        return float(np.sqrt(np.mean((e - e.mean()) ** 2)))
+
+    r = be.adjoint_raw(re, im, elev, dh, None, -ha, rows, rows, cols)  # warm-up
+    first = {"mean_gamma": float(np.nanmean(r["coh"])), "dh_rms_error_m": err(dh)}
+    r = be.adjoint_raw(re, im, elev, np.pad(dh_true, ((ha, ha), (0, 0))), None, -ha, rows, rows,
+                       cols)
+    truth = float(np.nanmean(r["coh"]))
+    times = []
+    steps = 20
+    for it in range(1, steps + 1):
+        t = time.perf_counter()
+        r = be.adjoint_raw(re, im, elev, dh, None, -ha, rows, rows, cols)
+        times.append(time.perf_counter() - t)
+        gu = scene.smooth(r["grad_dh"].astype(np.float64), box)
+        m_t = b1 * m_t + (1 - b1) * gu
+        v_t = b2 * v_t + (1 - b2) * gu * gu
+        mh, vh = m_t / (1 - b1 ** it), v_t / (1 - b2 ** it)
+        u = u + lr * mh / (np.sqrt(vh) + 1e-12)
+        dh = scene.smooth(u, box)
+    r = be.adjoint_raw(re, im, elev, dh, None, -ha, rows, rows, cols)
+    be.close()
+    ms = 1e3 * float(np.median(times))
+    line = {"metric": "Mpixel/s forward + adjoint of temporal coherence, N=30, 21x7 window",
+            "value": rows * cols / (ms * 1e-3) / 1e6, "unit": "Mpixel/s", "n_gpus": 1,
+            "steps": steps, "warmup": 1, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "N=30 %dx%d tlog/evd window 21x7, geometry with fBm heights "
+                                   "0-2000 m, dh_true 15 m RMS, phase screen 0-2 rad" % (rows, cols),
+                       "api": "tc_adjoint_raw (host buffers, strip preparation on the device)"},
+            "ascent": {"optimizer": "Adam on u, dh = %dx%d box average of u, lr %.1f m"
+                                    % (box, box, lr), "steps": steps,
+                       "mean_gamma_at_dh_true": truth, "before": first,
+                       "after": {"mean_gamma": float(np.nanmean(r["coh"])),
+                                 "dh_rms_error_m": err(dh)}}}
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
+    if args.workload == "adjoint" and args.impl != "reference":
+        return adjoint_workload(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -375,9 +488,16 @@ def main():
     roofline = {"kernel": dom, "bound": d["bound"], "achieved": d["achieved_tflops"],
                 "peak": d["peak_tflops"], "unit": "TFLOP/s",
                 "frac": d["frac"], "traffic": None,
+                "algorithmic_bytes_per_launch": None,
                 "peak_source": ("measured FP32 FMA microbenchmark (tc_fp32_peak)"
                                 if d["bound"] == "fp32" else "MEASURED_PEAKS.json bf16_tflops")}
 
+    if dom == "link" and w["n"] == 30 and w["estimator"] == "emi":
+        px_launch = npix / d["launches"]
+        roofline["traffic"] = LINK_DRAM_BYTES_PER_PIXEL * px_launch
+        roofline["algorithmic_bytes_per_launch"] = (8.0 * w["n"] * (w["n"] + 1) / 2 + 4) * px_launch
+        roofline["traffic_source"] = ("ncu dram bytes of one 65,536-pixel launch, scaled by "
+                                      "the pixels per launch")
     line = {"metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
