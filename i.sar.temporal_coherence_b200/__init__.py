@@ -30,7 +30,7 @@ LIBRARY = os.path.join(HERE, "libtcoh_b200.so")
 SHP_TESTS = {"ks": 0, "ad": 1, "tlog": 2}
 GRAM_TENSOR, GRAM_FP32 = 0, 1
 STATUS_EMI_PINV, STATUS_UNLINKED, STATUS_ITER_CAP = 1, 2, 4
-STAGES = ("prep", "shp", "gram", "link", "copy")
+STAGES = ("prep", "shp", "gram", "link", "copy", "adjoint")
 
 # Exported symbols of include/tcoh_b200.h.
 EXPORTS = (
@@ -367,9 +367,10 @@ class Backend:
 
     def stage_stats(self):
         """{stage: (device ms, launches)} of the last run with timing on."""
-        ms = (ctypes.c_float * 5)()
-        nl = (ctypes.c_int * 5)()
-        library().tc_stage_stats(self.handle, ms, nl, 5)
+        k = len(STAGES)
+        ms = (ctypes.c_float * k)()
+        nl = (ctypes.c_int * k)()
+        library().tc_stage_stats(self.handle, ms, nl, k)
         return {name: (ms[i], nl[i]) for i, name in enumerate(STAGES)}
 
     def set_geometry(self, geometry, grid):

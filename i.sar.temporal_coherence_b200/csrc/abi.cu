@@ -216,7 +216,7 @@ static cudaError_t ensure(DevBuf &b, size_t size)
     return e;
 }
 
-enum { ST_PREP, ST_SHP, ST_GRAM, ST_LINK, ST_COPY, ST_COUNT };
+enum { ST_PREP, ST_SHP, ST_GRAM, ST_LINK, ST_COPY, ST_ADJOINT, ST_COUNT };
 
 /* tc_run_ex copies a strip in this many row blocks on a second stream, and
    each chunk waits only for the blocks holding its rows. */
@@ -708,8 +708,15 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
                                       (const unsigned short *)o->pair_tab.p,
                                       (double *)o->link_scratch.p, coh, pairs, adj->gbar,
                                       o->sms, st));
-            CK(tc_launch_adjoint_scatter(s, c, o->wr / 2, adj->gbar, (const uint32_t *)o->mask.p,
-                                         slc, adj->dtheta, st));
+            tm.end(t);
+            t = tm.begin(ST_ADJOINT);
+            if (o->opt.gram == TC_GRAM_TENSOR && tc_gram_adjoint_tensor_supported(o->n, o->wa, o->wr))
+                CK(tc_launch_adjoint_scatter_tensor(s, c, o->wr / 2, adj->gbar,
+                                                    (const uint32_t *)o->mask.p, slc, adj->dtheta,
+                                                    st));
+            else
+                CK(tc_launch_adjoint_scatter(s, c, o->wr / 2, adj->gbar,
+                                             (const uint32_t *)o->mask.p, slc, adj->dtheta, st));
         }
         tm.end(t);
         if (mark_chunks)

@@ -275,8 +275,12 @@ __device__ __forceinline__ double grid_phase(const TcGeo &g, const double *grid,
     return ph;
 }
 
+/* One thread per strip cell; the outputs are pixel-major ([pixel][date]),
+   so each warp stages its 32 pixels' amplitudes, then their samples, in
+   shared memory (row stride n | 1, conflict-free for the 4-byte
+   amplitudes) and writes them out as one contiguous run. */
 template <int NP>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, NP <= 32 ? 3 : 1)
 tc_prep_raw_kernel(int n, const float *__restrict__ re, const float *__restrict__ im,
                    const double *__restrict__ elev, int row0, int region_rows, int padded_rows,
                    int cols, int halo, int use_geo, TcGeo g, const double *__restrict__ grid,
@@ -284,19 +288,24 @@ tc_prep_raw_kernel(int n, const float *__restrict__ re, const float *__restrict_
                    float2 *__restrict__ slc, float *__restrict__ amp,
                    unsigned char *__restrict__ valid)
 {
-    const int W = cols + 2 * halo;
+    extern __shared__ float2 prep_stage[];
+    const int W = cols + 2 * halo, ld = n | 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long total = (long long)padded_rows * W;
     const long long pix = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-
-    if (pix >= (long long)padded_rows * W)
-        return;
+    const long long wpix = pix - lane;
+    const int wcount = (int)min(32LL, total - wpix);
+    float2 *wb = prep_stage + warp * 32 * ld;
+    float *wa = (float *)wb;
+    const bool live = pix < total;
     const int r = (int)(pix / W), c = (int)(pix - (long long)r * W) - halo, row = row0 + r;
     const size_t plane = (size_t)padded_rows * cols;
     const size_t at = (size_t)r * cols + c;
-    float2 *s = slc + pix * n;
-    float *a_out = amp + pix * n;
-    bool ok = row >= 0 && row < region_rows && c >= 0 && c < cols;
+    bool ok = live && row >= 0 && row < region_rows && c >= 0 && c < cols;
     float a[NP];
 
+    if (wcount <= 0)
+        return; /* the whole warp lies past the strip */
     if (ok && elev && isnan(elev[at]))
         ok = false;
 #pragma unroll
@@ -311,51 +320,83 @@ tc_prep_raw_kernel(int n, const float *__restrict__ re, const float *__restrict_
             a[k] = sqrtf(__fadd_rn(__fmul_rn(vi, vi), __fmul_rn(vq, vq)));
         }
     }
-    valid[pix] = ok ? 1 : 0;
-    if (!ok) {
-        for (int k = 0; k < n; k++) {
-            s[k] = make_float2(0.f, 0.f);
-            a_out[k] = 0.f;
-        }
-        return;
-    }
-    bitonic<NP>(a);
+    if (live)
+        valid[pix] = ok ? 1 : 0;
+    if (ok)
+        bitonic<NP>(a);
 #pragma unroll
     for (int k = 0; k < NP; k++)
         if (k < n)
-            a_out[k] = a[k];
-    if (!use_geo && !psi) {
+            wa[lane * ld + k] = ok ? a[k] : 0.f;
+    __syncwarp();
+    for (int e = lane; e < wcount * n; e += 32) {
+        const int p = e / n;
+
+        amp[wpix * n + e] = wa[p * ld + (e - p * n)];
+    }
+    __syncwarp();
+    if (!ok) {
         for (int k = 0; k < n; k++)
-            s[k] = make_float2(re[k * plane + at], im[k * plane + at]);
-        return;
+            wb[lane * ld + k] = make_float2(0.f, 0.f);
     }
-    const int gr = row / GEO_STEP, gc = c / GEO_STEP;
-    const double fr = (double)(row - gr * GEO_STEP) / GEO_STEP;
-    const double fc = (double)(c - gc * GEO_STEP) / GEO_STEP;
-    /* the adjoint's variables: a height error and a phase screen */
-    const double h = (elev ? elev[at] : g.h0) + (dh ? dh[at] : 0.0);
-    double wh[3] = {1.0, 0.0, 0.0};
-
-    if (use_geo && g.nheights == 3) {
-        const double *x = g.heights;
-
-        wh[0] = (h - x[1]) * (h - x[2]) / ((x[0] - x[1]) * (x[0] - x[2]));
-        wh[1] = (h - x[0]) * (h - x[2]) / ((x[1] - x[0]) * (x[1] - x[2]));
-        wh[2] = (h - x[0]) * (h - x[1]) / ((x[2] - x[0]) * (x[2] - x[1]));
+    else if (!use_geo && !psi) {
+        for (int k = 0; k < n; k++)
+            wb[lane * ld + k] = make_float2(re[k * plane + at], im[k * plane + at]);
     }
-    for (int k = 0; k < n; k++) {
-        const double ph = (use_geo ? grid_phase(g, grid, gr, gc, fr, fc, wh, k) : 0.0) +
-                          (psi ? (double)psi[k * plane + at] : 0.0);
-        double sn, cs;
+    else {
+        const int gr = row / GEO_STEP, gc = c / GEO_STEP;
+        const double fr = (double)(row - gr * GEO_STEP) / GEO_STEP;
+        const double fc = (double)(c - gc * GEO_STEP) / GEO_STEP;
+        /* the adjoint's variables: a height error and a phase screen */
+        const double h = (elev ? elev[at] : g.h0) + (dh ? dh[at] : 0.0);
+        double wh[3] = {1.0, 0.0, 0.0};
 
-        sincos(ph, &sn, &cs);
-        const double vr = re[k * plane + at], vi = im[k * plane + at];
+        if (use_geo && g.nheights == 3) {
+            const double *x = g.heights;
 
-        /* (vr cs - vi sn, vr sn + vi cs) in double without contraction, as
-           main.c:117-121, then rounded to float */
-        s[k] = make_float2((float)__dadd_rn(__dmul_rn(vr, cs), -__dmul_rn(vi, sn)),
-                           (float)__dadd_rn(__dmul_rn(vr, sn), __dmul_rn(vi, cs)));
+            wh[0] = (h - x[1]) * (h - x[2]) / ((x[0] - x[1]) * (x[0] - x[2]));
+            wh[1] = (h - x[0]) * (h - x[2]) / ((x[1] - x[0]) * (x[1] - x[2]));
+            wh[2] = (h - x[0]) * (h - x[1]) / ((x[2] - x[0]) * (x[2] - x[1]));
+        }
+        for (int k = 0; k < n; k++) {
+            const double ph = (use_geo ? grid_phase(g, grid, gr, gc, fr, fc, wh, k) : 0.0) +
+                              (psi ? (double)psi[k * plane + at] : 0.0);
+            double sn, cs;
+
+            sincos(ph, &sn, &cs);
+            const double vr = re[k * plane + at], vi = im[k * plane + at];
+
+            /* (vr cs - vi sn, vr sn + vi cs) in double without contraction,
+               as main.c:117-121, then rounded to float */
+            wb[lane * ld + k] = make_float2((float)__dadd_rn(__dmul_rn(vr, cs), -__dmul_rn(vi, sn)),
+                                            (float)__dadd_rn(__dmul_rn(vr, sn), __dmul_rn(vi, cs)));
+        }
     }
+    __syncwarp();
+    for (int e = lane; e < wcount * n; e += 32) {
+        const int p = e / n;
+
+        slc[wpix * n + e] = wb[p * ld + (e - p * n)];
+    }
+}
+
+template <int NP>
+cudaError_t launch_prep_raw(unsigned blocks, int n, const float *re, const float *im,
+                            const double *elev, int row0, int region_rows, int padded_rows,
+                            int cols, int halo, int use, const TcGeo &g, const double *grid,
+                            const double *dh, const float *psi, float2 *s, float *amp,
+                            unsigned char *valid, cudaStream_t st)
+{
+    const int bytes = 8 * 32 * (n | 1) * (int)sizeof(float2);
+    cudaError_t e = cudaFuncSetAttribute(tc_prep_raw_kernel<NP>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+
+    if (e != cudaSuccess)
+        return e;
+    tc_prep_raw_kernel<NP><<<blocks, 256, bytes, st>>>(n, re, im, elev, row0, region_rows,
+                                                      padded_rows, cols, halo, use, g, grid, dh,
+                                                      psi, s, amp, valid);
+    return cudaGetLastError();
 }
 
 } // namespace
@@ -497,20 +538,14 @@ cudaError_t tc_launch_prep_raw(int n, const float *re, const float *im, const do
     float2 *s = (float2 *)slc;
 
     if (n <= 8)
-        tc_prep_raw_kernel<8><<<blocks, 256, 0, st>>>(n, re, im, elev, row0, region_rows,
-                                                      padded_rows, cols, halo, use, gg, grid, dh, psi, s,
-                                                      amp, valid);
-    else if (n <= 16)
-        tc_prep_raw_kernel<16><<<blocks, 256, 0, st>>>(n, re, im, elev, row0, region_rows,
-                                                       padded_rows, cols, halo, use, gg, grid, dh, psi, s,
-                                                       amp, valid);
-    else if (n <= 32)
-        tc_prep_raw_kernel<32><<<blocks, 256, 0, st>>>(n, re, im, elev, row0, region_rows,
-                                                       padded_rows, cols, halo, use, gg, grid, dh, psi, s,
-                                                       amp, valid);
-    else
-        tc_prep_raw_kernel<64><<<blocks, 256, 0, st>>>(n, re, im, elev, row0, region_rows,
-                                                       padded_rows, cols, halo, use, gg, grid, dh, psi, s,
-                                                       amp, valid);
-    return cudaGetLastError();
+        return launch_prep_raw<8>(blocks, n, re, im, elev, row0, region_rows, padded_rows, cols,
+                                  halo, use, gg, grid, dh, psi, s, amp, valid, st);
+    if (n <= 16)
+        return launch_prep_raw<16>(blocks, n, re, im, elev, row0, region_rows, padded_rows, cols,
+                                   halo, use, gg, grid, dh, psi, s, amp, valid, st);
+    if (n <= 32)
+        return launch_prep_raw<32>(blocks, n, re, im, elev, row0, region_rows, padded_rows, cols,
+                                   halo, use, gg, grid, dh, psi, s, amp, valid, st);
+    return launch_prep_raw<64>(blocks, n, re, im, elev, row0, region_rows, padded_rows, cols,
+                               halo, use, gg, grid, dh, psi, s, amp, valid, st);
 }

@@ -476,6 +476,294 @@ tc_gram_tc_kernel(TcStrip s, TcChunk c, int terms, const float2 *__restrict__ sl
                      ::"r"(tmem), "r"(TMEM_COLS) : "memory");
 }
 
+/* ------------------------------------------------------------------------
+ * The transpose: the adjoint's scatter of the Gram gradient onto the
+ * candidates (the CUDA-core form is tc_adjoint_scatter_kernel in
+ * adjoint.cu). With G_p the Hermitian gradient of pixel p, every candidate
+ * u of a tile needs
+ *
+ *   H_u = sum over the tile's pixels p that took u as an SHP of G_p,
+ *   dL/dtheta_u,i += 2 Im(conj(a_u,i) (H_u a_u)_i)
+ *
+ * and H = A' G is again one GEMM per tile: A'[u][p] = the SHP bit (the
+ * forward's A transposed, candidates as M, the 128 pixels as K) and G's
+ * columns the real and imaginary parts of G_p,ij for one row i at a time,
+ * j = 0 .. J - 1 (J = n rounded up to 16; G_ji = conj(G_ij); the diagonal
+ * adds nothing to Im(conj(a_i) G_ii a_i) and is left out). G is split into
+ * two truncated BF16 terms (relative error below 2^-16 per value, products
+ * with the 0/1 of A' exact). One CTA of 512 threads per tile: thread t owns
+ * candidate t (up to 4 blocks of 128, K <= 512), builds its A' row once
+ * and keeps its samples in registers; row i's G columns are staged in one
+ * of two buffers while the MMAs of row i - 1 run into the other half of
+ * TMEM, and the epilogue of row i - 1 forms (H_u a_u)_{i-1} from the
+ * accumulator and adds the candidate's dL/dtheta atomically (a candidate
+ * lies in the windows of several tiles). Waits are bounded as in the
+ * forward kernel; one that runs out sets the same fault flag.
+ * ------------------------------------------------------------------------ */
+constexpr int ADJ_THREADS = 512;
+constexpr int ADJ_MB = 4;                            /* candidate blocks of 128 */
+constexpr int ADJ_KCH = TC_TILE_PIX / 8;             /* 16-byte pixel chunks: 16 */
+constexpr int ADJ_A_BYTES = ADJ_MB * ADJ_KCH * 128 * 16;   /* 128 KB */
+constexpr int ADJ_TERM_BYTES = ADJ_KCH * 64 * 16;    /* 16 chunks x 2J <= 64 rows x 16 B */
+constexpr int ADJ_BUF_BYTES = 2 * ADJ_TERM_BYTES;    /* two terms */
+constexpr int ADJ_TMEM_COLS = 512;                   /* 2 buffers x 4 blocks x 64 */
+
+struct AdjSmem {
+    int a, b, rows, expand, bar, bytes;
+};
+
+__host__ __device__ inline AdjSmem adj_smem(int wa)
+{
+    AdjSmem g;
+
+    g.a = 0;
+    g.b = g.a + ADJ_A_BYTES;
+    g.rows = g.b + 2 * ADJ_BUF_BYTES;
+    g.expand = g.rows + wa * TC_TILE_PIX * 4;
+    g.bar = g.expand + 16 * 8;
+    g.bytes = g.bar + 32;
+    return g;
+}
+
+/* 8 FP32 values -> two truncated BF16 terms, 16 bytes each. */
+__device__ __forceinline__ void split2_store(const float (&v)[8], unsigned char *dst)
+{
+    uint32_t hi[4], lo[4];
+
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const uint32_t a = __float_as_uint(v[2 * k]), b = __float_as_uint(v[2 * k + 1]);
+        const float ra = v[2 * k] - __uint_as_float(a & 0xffff0000u);
+        const float rb = v[2 * k + 1] - __uint_as_float(b & 0xffff0000u);
+
+        hi[k] = __byte_perm(a, b, 0x7632);
+        lo[k] = __byte_perm(__float_as_uint(ra), __float_as_uint(rb), 0x7632);
+    }
+    *(uint4 *)dst = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+    *(uint4 *)(dst + ADJ_TERM_BYTES) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+}
+
+__global__ void __launch_bounds__(ADJ_THREADS, 1)
+tc_gram_adjoint_tc_kernel(TcStrip s, TcChunk c, int halo, const float2 *__restrict__ gbar,
+                          const uint32_t *__restrict__ mask, const float2 *__restrict__ slc,
+                          float *__restrict__ dtheta)
+{
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const int n = s.n, J = up16(n), NC = 2 * J;
+    const AdjSmem L = adj_smem(s.wa);
+    unsigned char *sA = sm + L.a, *sB = sm + L.b;
+    uint32_t *s_rows = (uint32_t *)(sm + L.rows);
+    uint2 *s_expand = (uint2 *)(sm + L.expand);
+    uint32_t *s_taddr = (uint32_t *)(sm + L.bar + 16);
+    const uint32_t bar0 = smem_u32(sm + L.bar);
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int tile = blockIdx.x;
+    const int ty = tile / c.tiles_x, tx = tile - ty * c.tiles_x;
+    const int y0 = c.row0 + ty * TC_TILE_H, x0 = tx * TC_TILE_W;
+    const int UW = TC_TILE_W + s.wr - 1, K = (TC_TILE_H + s.wa - 1) * UW;
+    const int MB = (K + 127) >> 7;
+    const uint32_t wr_mask = (1u << s.wr) - 1u;
+    const long long pix0 = (long long)tile * TC_TILE_PIX;
+
+    for (int e = t; e < s.wa * TC_TILE_PIX; e += ADJ_THREADS) {
+        const int dy = e >> 7, m = e & 127;
+        const int y = y0 + (m >> 3), x = x0 + (m & 7);
+        uint32_t f = 0u;
+
+        if (y < c.row0 + c.nrows && y < s.rows && x < s.cols) {
+            const int b = dy * s.wr, w = b >> 5, o = b & 31;
+            const uint32_t lo = mask[(long long)w * c.npix + pix0 + m];
+            const uint32_t hi = o + s.wr > 32 ? mask[(long long)(w + 1) * c.npix + pix0 + m] : 0u;
+
+            f = (uint32_t)(((unsigned long long)hi << 32 | lo) >> o) & wr_mask;
+        }
+        s_rows[e] = f;
+    }
+    if (t < 16)
+        s_expand[t] = make_uint2((t & 1 ? 0x3f80u : 0u) | (t & 2 ? 0x3f800000u : 0u),
+                                 (t & 4 ? 0x3f80u : 0u) | (t & 8 ? 0x3f800000u : 0u));
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(s_taddr)), "r"(ADJ_TMEM_COLS) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar0), "r"(1) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar0 + 8), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *s_taddr;
+
+    /* This thread's candidate: its A' row, its samples, its output cell. */
+    const int u = t, mb = u >> 7;
+    const int uy = u / UW, ux = u - uy * UW;
+    const int py = y0 + uy, px = x0 + ux, col = px - halo;
+    const bool in_strip = u < K && py < s.padded_rows && px < s.W;
+    uint32_t any = 0u;
+
+    if (mb < MB)
+        for (int g = 0; g < ADJ_KCH; g++) {
+            const int dy = uy - g; /* chunk g = tile row g, pixels 8g .. 8g + 7 */
+            uint32_t bits = 0u;
+
+            if (u < K && dy >= 0 && dy < s.wa)
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    const int dx = ux - k;
+
+                    if (dx >= 0 && dx < s.wr)
+                        bits |= ((s_rows[dy * TC_TILE_PIX + g * 8 + k] >> dx) & 1u) << k;
+                }
+            any |= bits;
+            const uint2 lo = s_expand[bits & 15u], hi = s_expand[bits >> 4];
+
+            *(uint4 *)(sA + ((mb * ADJ_KCH + g) * 128 + (u & 127)) * 16) =
+                make_uint4(lo.x, lo.y, hi.x, hi.y);
+        }
+    float2 a[32];
+
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+        float2 v = make_float2(0.f, 0.f);
+
+        if (k < n && in_strip && any) {
+            v = slc[((long long)py * s.W + px) * n + k];
+            if (!isfinite(v.x) || !isfinite(v.y))
+                v = make_float2(0.f, 0.f);
+        }
+        a[k] = v;
+    }
+    const bool emit = in_strip && any && col >= 0 && col < s.cols;
+    const size_t plane = (size_t)s.padded_rows * s.cols;
+    float *out = dtheta + (size_t)(emit ? py : 0) * s.cols + (emit ? col : 0);
+
+    /* staging items: J / 8 warps per group of four pixel chunks; a quarter
+       warp writes 8 consecutive 16-byte rows (conflict-free) */
+    const int jw = J >> 3;
+    const int sj = (lane & 7) + 8 * (warp % jw), sg = (lane >> 3) + 4 * (warp / jw);
+    const bool stager = sg < ADJ_KCH;
+    const uint32_t idesc = instr_desc(NC);
+    const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + mb * 64;
+    bool ok = true;
+    int issued = 0; /* rows whose MMAs were issued */
+
+    for (int i = 0; i <= n && ok; i++) {
+        const int b = i & 1;
+
+        if (i < n) {
+            /* (a) row i of G into buffer b (its last reader, the MMAs of
+               row i - 2, completed before the epilogue of row i - 2) */
+            if (stager) {
+                float re[8], im[8];
+                const bool zero = sj == i || sj >= n;
+
+                if (!zero) {
+                    const int lo = min(i, sj), hi = max(i, sj);
+                    const float sign = sj < i ? -1.f : 1.f;
+                    const float4 *src = (const float4 *)(gbar + (long long)tc_pidx(n, lo, hi) *
+                                                                    c.npix + pix0 + sg * 8);
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        const float4 v = __ldg(src + k);
+
+                        re[2 * k] = v.x;
+                        im[2 * k] = sign * v.y;
+                        re[2 * k + 1] = v.z;
+                        im[2 * k + 1] = sign * v.w;
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 8; k++)
+                        re[k] = im[k] = 0.f;
+                }
+                unsigned char *dst = sB + b * ADJ_BUF_BYTES + (sg * NC + sj) * 16;
+
+                split2_store(re, dst);
+                split2_store(im, dst + J * 16);
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+            /* (b) the MMAs of row i: M-block m of A' x both terms of G */
+            if (t == 0) {
+                fence_after();
+                for (int m = 0; m < MB; m++)
+#pragma unroll
+                    for (int ks = 0; ks < ADJ_KCH / 2; ks++) {
+                        const uint64_t adesc = smem_desc(
+                            smem_u32(sA + (m * ADJ_KCH + 2 * ks) * 128 * 16), 128 * 16, 128);
+#pragma unroll
+                        for (int term = 0; term < 2; term++) {
+                            const uint64_t bdesc = smem_desc(
+                                smem_u32(sB + b * ADJ_BUF_BYTES + term * ADJ_TERM_BYTES +
+                                         ks * 2 * NC * 16),
+                                NC * 16, 128);
+
+                            mma_bf16(tmem + b * 256 + m * 64, adesc, bdesc, idesc,
+                                     (ks | term) != 0);
+                        }
+                    }
+                mma_commit(bar0 + 8 * b);
+            }
+            issued = i + 1;
+        }
+        if (i == 0)
+            continue;
+        /* (c) epilogue of row r = i - 1 */
+        const int r = i - 1, rb = r & 1;
+
+        ok = mbar_wait(bar0 + 8 * rb, (r >> 1) & 1);
+        if (!__syncthreads_and(ok)) {
+            ok = false;
+            break;
+        }
+        fence_after();
+        if (mb < MB) {
+            float2 bsum = make_float2(0.f, 0.f), ar = make_float2(0.f, 0.f);
+
+#pragma unroll
+            for (int h = 0; h < 2; h++)
+                if (h * 16 < J) {
+                    uint32_t vr[16], vi[16];
+
+                    tmem_ld16(lane_addr + rb * 256 + h * 16, vr);
+                    tmem_ld16(lane_addr + rb * 256 + J + h * 16, vi);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                    for (int k = 0; k < 16; k++) {
+                        const float hr = __uint_as_float(vr[k]), hi = __uint_as_float(vi[k]);
+                        const float2 aj = a[h * 16 + k];
+
+                        bsum.x = fmaf(hr, aj.x, fmaf(-hi, aj.y, bsum.x));
+                        bsum.y = fmaf(hr, aj.y, fmaf(hi, aj.x, bsum.y));
+                    }
+                }
+#pragma unroll
+            for (int k = 0; k < 32; k++)
+                if (k == r)
+                    ar = a[k];
+            if (emit)
+                atomicAdd(out + r * plane, 2.f * (ar.x * bsum.y - ar.y * bsum.x));
+        }
+        fence_before();
+    }
+    if (!ok) {
+        if (t == 0)
+            atomicOr(&g_gram_fault, 1);
+        /* the MMAs issued last may still run: wait for both buffers' last
+           commits before the TMEM is freed */
+        for (int r = max(0, issued - 2); r < issued; r++)
+            mbar_wait(bar0 + 8 * (r & 1), (r >> 1) & 1);
+    }
+    __syncthreads();
+    fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     ::"r"(tmem), "r"(ADJ_TMEM_COLS) : "memory");
+}
+
 } // namespace
 
 bool tc_gram_tensor_supported(int n, int wa, int wr)
@@ -521,4 +809,26 @@ int tc_gram_tensor_fault(void)
         cudaMemcpyToSymbol(g_gram_fault, &zero, sizeof(zero));
     }
     return v;
+}
+
+bool tc_gram_adjoint_tensor_supported(int n, int wa, int wr)
+{
+    return n <= 32 && (TC_TILE_H + wa - 1) * (TC_TILE_W + wr - 1) <= ADJ_MB * 128 &&
+           tc_gram_tensor_supported(n, wa, wr);
+}
+
+cudaError_t tc_launch_adjoint_scatter_tensor(const TcStrip &s, const TcChunk &c, int halo,
+                                             const float2 *gbar, const uint32_t *mask,
+                                             const float *slc, float *dtheta, cudaStream_t st)
+{
+    const AdjSmem L = adj_smem(s.wa);
+    cudaError_t e;
+
+    if ((e = cudaFuncSetAttribute(tc_gram_adjoint_tc_kernel,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, L.bytes)) !=
+        cudaSuccess)
+        return e;
+    tc_gram_adjoint_tc_kernel<<<c.npix / TC_TILE_PIX, ADJ_THREADS, L.bytes, st>>>(
+        s, c, halo, gbar, mask, (const float2 *)slc, dtheta);
+    return cudaGetLastError();
 }

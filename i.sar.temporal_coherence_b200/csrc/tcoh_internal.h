@@ -132,6 +132,12 @@ bool tc_gram_tensor_supported(int n, int wa, int wr);
 /* 1 if a tensor-core Gram wait ran out since the last call (and clears it),
    0 if not, -1 if the flag cannot be read. Synchronous. */
 int tc_gram_tensor_fault(void);
+/* The adjoint's scatter as the transposed tensor-core Gram (n <= 32, at most
+   512 candidates in a tile's union window); faults set the flag above. */
+bool tc_gram_adjoint_tensor_supported(int n, int wa, int wr);
+cudaError_t tc_launch_adjoint_scatter_tensor(const TcStrip &s, const TcChunk &c, int halo,
+                                             const float2 *gbar, const uint32_t *mask,
+                                             const float *slc, float *dtheta, cudaStream_t st);
 int tc_gram_block_for(int n);
 cudaError_t tc_launch_link(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
                            const float2 *gram, const int *count,

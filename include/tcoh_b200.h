@@ -235,8 +235,10 @@ int tc_adjoint_raw(struct ocl *o, const float *re, const float *im, const double
    bracketed by CUDA events on its stream, and tc_stage_stats gives, per
    stage, the device milliseconds summed over the last run and the number
    of kernel launches: [0] strip preparation, [1] SHP selection,
-   [2] coherence matrices, [3] phase linking and coherence, [4] host<->device
-   copies (ms only). Returns the number of stages written (at most n). */
+   [2] coherence matrices, [3] phase linking and coherence (with the
+   adjoint: and its backward pass), [4] host<->device copies (ms only),
+   [5] the adjoint's scatter onto the samples. Returns the number of stages
+   written (at most n). */
 int tc_set_timing(struct ocl *o, int on);
 int tc_stage_stats(const struct ocl *o, float *ms, int *launches, int n);
 

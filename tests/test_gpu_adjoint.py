@@ -80,3 +80,51 @@ def test_adjoint_without_geometry_is_the_screen_gradient():
     compare(r1["grad_psi"], gpsi)
     # the candidates' sums are accumulated atomically: equal up to their order
     assert np.abs(r1["grad_psi"] - r2["grad_psi"]).max() <= 1e-5 * np.abs(gpsi).max()
+
+
+@pytest.mark.parametrize("gram", ["tensor", "fp32"])
+def test_adjoint_thirty_dates(gram):
+    """N = 30 on a synthetic acquisition over fractal heights (0 - 400 m),
+    through both forms of the scatter: the transposed tensor-core Gram
+    (gram "tensor") and the CUDA-core one (gram "fp32"). Two tiles across and
+    two down share candidates, so the atomic sums across tiles are covered."""
+    import tcoh_b200.scene as scene
+    import tcoh_b200.synthetic as syn
+
+    n, rows, cols, window = 30, 32, 16, (21, 7)
+    ha, hr = window[0] // 2, window[1] // 2
+    geo, orbits = scene.acquisition(n, rows, cols, seed=21)
+    h = scene.fbm_heights(rows, cols, hmax=400.0, seed=22)
+    geo.update(hmin=float(h.min()), hmax=float(h.max()), h0=0.0)
+    grid = oracle.geometry_grid(geo, orbits)
+    _gr, _gc, nh, hs = oracle.geometry_shape(geo)
+    assert nh == 3
+    stack = syn.generate(n, rows, cols, nregions=3, g0_max=0.95, seed=23, null_frac=0.02)
+    prow = rows + 2 * ha
+    re = np.full((n, prow, cols), np.nan, np.float32)
+    im = re.copy()
+    re[:, ha:ha + rows] = stack.real
+    im[:, ha:ha + rows] = stack.imag
+    elev = np.full((prow, cols), np.nan)
+    elev[ha:ha + rows] = h
+    rng = np.random.default_rng(24)
+    dh = rng.normal(0.0, 5.0, (prow, cols))
+    psi = rng.normal(0.0, 0.3, re.shape).astype(np.float32)
+    slc, amp, valid = oracle.prepare_strip(re, im, elev, -ha, rows, hr, geo, grid)
+    o = oracle.run_oracle(slc, amp, valid, rows, cols, window=window, min_shp=10,
+                          estimator="evd", shp_fp32=True, want_mask=True)
+    _L, gam, gdh, gpsi = adjoint_oracle.adjoint(
+        re, im, elev, dh, psi.astype(np.float64), row0=-ha, region_rows=rows, halo_cols=hr,
+        mask=o["mask"], count=o["count"], window=window, min_looks=max(10, n), estimator="evd",
+        bias=False, grid=grid, grid_heights=hs[:nh], h0=0.0)
+    s = tcoh_b200.make_settings(n, window=window, min_shp=10)
+    with tcoh_b200.Backend(s, cols + 2 * hr, gram=gram) as be:
+        be.set_geometry(tc_geometry(geo), grid)
+        r = be.adjoint_raw(re, im, elev, dh, psi, -ha, rows, rows, cols)
+    assert np.array_equal(r["count"], o["count"])
+    # a pixel needs max(min_shp, N) looks (main.c:585-587): some have fewer
+    assert np.isnan(gam).any() and not np.isnan(gam).all()
+    assert np.array_equal(np.isnan(r["coh"]), np.isnan(gam))
+    assert np.nanmax(np.abs(r["coh"] - gam)) < TOLERANCE
+    compare(r["grad_psi"], gpsi)
+    compare(r["grad_dh"], gdh)
