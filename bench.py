@@ -291,11 +291,21 @@ def adjoint_workload(args):
     stack = (stack * np.exp(-1j * phase)).astype(np.complex64)
     del phase
     prow = rows + 2 * ha
-    re = np.full((n, prow, cols), np.nan, np.float32)
-    im = re.copy()
+
+    def pinned(shape, dtype):
+        return torch.empty(shape, dtype=dtype, pin_memory=True).numpy()
+
+    # the samples and the gradients live in page-locked host memory
+    re = pinned((n, prow, cols), torch.float32)
+    im = pinned((n, prow, cols), torch.float32)
+    re[:] = np.nan
+    im[:] = np.nan
     re[:, ha:ha + rows] = stack.real
     im[:, ha:ha + rows] = stack.imag
     del stack
+    out = {"coh": pinned((rows, cols), torch.float32), "count": pinned((rows, cols), torch.int32),
+           "grad_dh": pinned((prow, cols), torch.float32),
+           "grad_psi": pinned((n, prow, cols), torch.float32)}
     elev = np.zeros((prow, cols))
     elev[ha:ha + rows] = h
     s = tcoh_b200.make_settings(n, window=(21, 7), shp_test="tlog", alpha=0.05, min_shp=20,
@@ -312,16 +322,16 @@ def adjoint_workload(args):
         e = d[inner] - dh_true
         return float(np.sqrt(np.mean((e - e.mean()) ** 2)))
 
-    r = be.adjoint_raw(re, im, elev, dh, None, -ha, rows, rows, cols)  # warm-up
+    r = be.adjoint_raw(re, im, elev, dh, None, -ha, rows, rows, cols, out=out)  # warm-up
     first = {"mean_gamma": float(np.nanmean(r["coh"])), "dh_rms_error_m": err(dh)}
     r = be.adjoint_raw(re, im, elev, np.pad(dh_true, ((ha, ha), (0, 0))), None, -ha, rows, rows,
-                       cols)
+                       cols, out=out)
     truth = float(np.nanmean(r["coh"]))
     times = []
     steps = 20
     for it in range(1, steps + 1):
         t = time.perf_counter()
-        r = be.adjoint_raw(re, im, elev, dh, None, -ha, rows, rows, cols)
+        r = be.adjoint_raw(re, im, elev, dh, None, -ha, rows, rows, cols, out=out)
         times.append(time.perf_counter() - t)
         gu = scene.smooth(r["grad_dh"].astype(np.float64), box)
         m_t = b1 * m_t + (1 - b1) * gu
@@ -329,7 +339,9 @@ def adjoint_workload(args):
         mh, vh = m_t / (1 - b1 ** it), v_t / (1 - b2 ** it)
         u = u + lr * mh / (np.sqrt(vh) + 1e-12)
         dh = scene.smooth(u, box)
-    r = be.adjoint_raw(re, im, elev, dh, None, -ha, rows, rows, cols)
+    be.set_timing(True)
+    r = be.adjoint_raw(re, im, elev, dh, None, -ha, rows, rows, cols, out=out)
+    stages = {k: {"ms": v[0], "launches": v[1]} for k, v in be.stage_stats().items()}
     be.close()
     ms = 1e3 * float(np.median(times))
     line = {"metric": "Mpixel/s forward + adjoint of temporal coherence, N=30, 21x7 window",
@@ -338,7 +350,8 @@ def adjoint_workload(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "N=30 %dx%d tlog/evd window 21x7, geometry with fBm heights "
                                    "0-2000 m, dh_true 15 m RMS, phase screen 0-2 rad" % (rows, cols),
-                       "api": "tc_adjoint_raw (host buffers, strip preparation on the device)"},
+                       "api": "tc_adjoint_raw (page-locked host buffers, strip preparation on the device)"},
+            "stages": stages,
             "ascent": {"optimizer": "Adam on u, dh = %dx%d box average of u, lr %.1f m"
                                     % (box, box, lr), "steps": steps,
                        "mean_gamma_at_dh_true": truth, "before": first,

@@ -401,22 +401,32 @@ class Backend:
             _ptr(out.get("phases")), _ptr(out.get("status"))))
         return out
 
-    def adjoint_raw(self, re, im, elevation, dh, psi, row0, region_rows, rows, cols):
+    def adjoint_raw(self, re, im, elevation, dh, psi, row0, region_rows, rows, cols, out=None):
         """tc_adjoint_raw: gamma of a raw strip (as run_raw) and the gradient
         of the sum of gamma over its estimated pixels with respect to a
         height error dh (padded_rows, cols) and a phase screen psi (N,
         padded_rows, cols) added to the removed phase (either None for
-        zero). Returns a dict with coh, count, grad_dh and grad_psi."""
+        zero). Returns a dict with coh, count, grad_dh and grad_psi; `out`
+        may hold any of them as C-contiguous arrays of those shapes and types
+        (for instance in page-locked memory, which the copies read and write
+        at full speed)."""
         re = np.ascontiguousarray(re, np.float32)
         im = np.ascontiguousarray(im, np.float32)
         n, padded_rows, _ = re.shape
         elev = None if elevation is None else np.ascontiguousarray(elevation, np.float64)
         dh = None if dh is None else np.ascontiguousarray(dh, np.float64)
         psi = None if psi is None else np.ascontiguousarray(psi, np.float32)
-        out = {"coh": np.empty((rows, cols), np.float32),
-               "count": np.empty((rows, cols), np.int32),
-               "grad_dh": np.empty((padded_rows, cols), np.float32),
-               "grad_psi": np.empty((n, padded_rows, cols), np.float32)}
+        want = {"coh": ((rows, cols), np.float32), "count": ((rows, cols), np.int32),
+                "grad_dh": ((padded_rows, cols), np.float32),
+                "grad_psi": ((n, padded_rows, cols), np.float32)}
+        out = dict(out or {})
+        for name, (shape, dtype) in want.items():
+            a = out.get(name)
+            if a is None:
+                out[name] = np.empty(shape, dtype)
+            elif a.shape != shape or a.dtype != dtype or not a.flags.c_contiguous:
+                raise ValueError("out[%r] must be a C-contiguous %s array of shape %s"
+                                 % (name, np.dtype(dtype).name, shape))
         _check(library().tc_adjoint_raw(
             self.handle, re.ctypes.data, im.ctypes.data, _ptr(elev), _ptr(dh), _ptr(psi), row0,
             region_rows, padded_rows, rows, cols, _ptr(out["coh"]), _ptr(out["count"]),

@@ -128,3 +128,79 @@ def test_adjoint_thirty_dates(gram):
     assert np.nanmax(np.abs(r["coh"] - gam)) < TOLERANCE
     compare(r["grad_psi"], gpsi)
     compare(r["grad_dh"], gdh)
+
+
+class CoherenceSum:
+    """torch.autograd.Function over tc_adjoint_raw (test harness only): L =
+    sum of gamma over the estimated pixels as a function of the height error
+    dh and the phase screen psi; the backward returns the device adjoint."""
+
+    @staticmethod
+    def function(be, re, im, elev, row0, rows, cols):
+        import torch
+
+        class F(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, dh, psi):
+                r = be.adjoint_raw(re, im, elev, dh.detach().numpy(),
+                                   psi.detach().numpy().astype(np.float32), row0, rows, rows, cols)
+                ctx.save_for_backward(torch.from_numpy(r["grad_dh"].astype(np.float64)),
+                                      torch.from_numpy(r["grad_psi"].astype(np.float64)))
+                return torch.tensor(np.nansum(r["coh"].astype(np.float64)), dtype=torch.float64)
+
+            @staticmethod
+            def backward(ctx, gl):
+                gdh, gpsi = ctx.saved_tensors
+                return gl * gdh, gl * gpsi
+
+        return F.apply
+
+
+def test_autograd_function_matches_finite_differences():
+    """The Function's gradient against central differences of the device
+    forward at N = 30: along its own direction to 1e-3 relative (steps of
+    0.05 m and 0.01 rad in norm), and along random directions (steps of
+    0.01 m and 0.0005 rad per cell) to 1e-3 of |grad| |direction|."""
+    import torch
+
+    import tcoh_b200.scene as scene
+    import tcoh_b200.synthetic as syn
+
+    n, rows, cols, window = 30, 32, 16, (21, 7)
+    ha, hr = window[0] // 2, window[1] // 2
+    geo, orbits = scene.acquisition(n, rows, cols, seed=31)
+    h = scene.fbm_heights(rows, cols, hmax=800.0, seed=32)
+    geo.update(hmin=float(h.min()), hmax=float(h.max()), h0=0.0)
+    grid = oracle.geometry_grid(geo, orbits)
+    stack = syn.generate(n, rows, cols, nregions=2, g0_max=0.95, seed=33, null_frac=0.0)
+    prow = rows + 2 * ha
+    re = np.full((n, prow, cols), np.nan, np.float32)
+    im = re.copy()
+    re[:, ha:ha + rows] = stack.real
+    im[:, ha:ha + rows] = stack.imag
+    elev = np.full((prow, cols), np.nan)
+    elev[ha:ha + rows] = h
+    rng = np.random.default_rng(34)
+    x0 = {"dh": rng.normal(0.0, 5.0, (prow, cols)), "psi": rng.normal(0.0, 0.2, re.shape)}
+    s = tcoh_b200.make_settings(n, window=window, min_shp=20)
+    with tcoh_b200.Backend(s, cols + 2 * hr) as be:
+        be.set_geometry(tc_geometry(geo), grid)
+        f = CoherenceSum.function(be, re, im, elev, -ha, rows, cols)
+        x = {k: torch.tensor(v, requires_grad=True) for k, v in x0.items()}
+        loss = f(x["dh"], x["psi"])
+        loss.backward()
+        assert loss.item() > 0
+
+        def along(name, d, eps):
+            with torch.no_grad():
+                lp = f(*(torch.tensor(x0[k] + (eps * d if k == name else 0.0)) for k in x0)).item()
+                lm = f(*(torch.tensor(x0[k] - (eps * d if k == name else 0.0)) for k in x0)).item()
+            return (lp - lm) / (2 * eps)
+
+        for name, step, cell_step in (("dh", 0.05, 0.01), ("psi", 0.01, 5e-4)):
+            g = x[name].grad.numpy()
+            gn = np.linalg.norm(g)
+            assert along(name, g / gn, step) == pytest.approx(gn, rel=1e-3)
+            d = rng.normal(0.0, 1.0, g.shape)
+            fd = along(name, d, cell_step)
+            assert abs(fd - (g * d).sum()) <= 1e-3 * gn * np.linalg.norm(d), (name, fd, (g * d).sum())
