@@ -321,6 +321,88 @@ __device__ void householder(float2 (&r0)[32], float2 (&r1)[32], int n, const HWs
 /* Tridiagonal eigenvector.                                            */
 /* ------------------------------------------------------------------ */
 
+/* x <- Q^H x (adjoint) or Q x, Q = H_0 H_1 .. H_{n-2}, H_k = I - tau_k v_k v_k^H
+   (v_k in T's lower triangle, column k), on the group's rows (i0, i1).
+   The reflectors go in blocks of four in application order; per block the
+   four products v^H x and the six v_m^H v_j within the block are reduced
+   over the group at once, then
+       s_m = v_m^H x - sum_{j<m} (v_m^H v_j) h_j,  h_m = tau'_m s_m,
+       x  -= sum_m v_m h_m
+   (tau' = conj(tau) for Q^H), which is the sequential application
+   rearranged. */
+__device__ void apply_q(int n, int ld, const HWs &w, const Grp &g, bool adjoint, float2 &x0,
+                        float2 &x1)
+{
+    const int i0 = g.gl, i1 = g.gl + 16, nk = n - 1;
+
+    for (int b = 0; b < nk; b += 4) {
+        float2 v0[4], v1[4], ta[4];
+
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            const int pos = b + m, k = adjoint ? pos : nk - 1 - pos;
+            const bool ok = pos < nk;
+            const float2 t = ok ? w.tau[k] : make_float2(0.f, 0.f);
+
+            ta[m] = adjoint ? make_float2(t.x, -t.y) : t;
+            v0[m] = ok && i0 > k && i0 < n ? w.T[i0 * ld + k] : make_float2(0.f, 0.f);
+            v1[m] = ok && i1 > k && i1 < n ? w.T[i1 * ld + k] : make_float2(0.f, 0.f);
+        }
+        /* r[2m], r[2m+1]: v_m^H x; r[8 + 2p], r[9 + 2p]: v_m^H v_j, pairs
+           p = (1,0), (2,0), (2,1), (3,0), (3,1), (3,2) */
+        float r[20];
+
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            r[2 * m] = v0[m].x * x0.x + v0[m].y * x0.y + v1[m].x * x1.x + v1[m].y * x1.y;
+            r[2 * m + 1] = v0[m].x * x0.y - v0[m].y * x0.x + v1[m].x * x1.y - v1[m].y * x1.x;
+        }
+        {
+            int p = 0;
+
+#pragma unroll
+            for (int m = 1; m < 4; m++)
+#pragma unroll
+                for (int j = 0; j < m; j++, p++) {
+                    r[8 + 2 * p] = v0[m].x * v0[j].x + v0[m].y * v0[j].y + v1[m].x * v1[j].x +
+                                   v1[m].y * v1[j].y;
+                    r[9 + 2 * p] = v0[m].x * v0[j].y - v0[m].y * v0[j].x + v1[m].x * v1[j].y -
+                                   v1[m].y * v1[j].x;
+                }
+        }
+#pragma unroll
+        for (int e = 0; e < 20; e++)
+            r[e] = gsum(r[e], g);
+        float2 h[4];
+
+        {
+            int p = 0;
+
+#pragma unroll
+            for (int m = 0; m < 4; m++) {
+                float sx = r[2 * m], sy = r[2 * m + 1];
+
+#pragma unroll
+                for (int j = 0; j < m; j++, p++) {
+                    const float gx = r[8 + 2 * p], gy = r[9 + 2 * p];
+
+                    sx -= gx * h[j].x - gy * h[j].y;
+                    sy -= gx * h[j].y + gy * h[j].x;
+                }
+                h[m] = make_float2(ta[m].x * sx - ta[m].y * sy, ta[m].x * sy + ta[m].y * sx);
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < 4; m++) {
+            x0.x -= v0[m].x * h[m].x - v0[m].y * h[m].y;
+            x0.y -= v0[m].x * h[m].y + v0[m].y * h[m].x;
+            x1.x -= v1[m].x * h[m].x - v1[m].y * h[m].y;
+            x1.y -= v1[m].x * h[m].y + v1[m].y * h[m].x;
+        }
+    }
+}
+
+
 __device__ __forceinline__ int sturm16(const float *d, const float *e2, int n, float x,
                                        float pivmin)
 {
@@ -516,25 +598,7 @@ __device__ unsigned eigvec(int n, int index, const HWs &w, int ld, const Grp &g,
     z0 = make_float2(i0 < n ? y0 : 0.f, 0.f);
     z1 = make_float2(i1 < n ? y1 : 0.f, 0.f);
     /* z = H_0 .. H_{n-2} y */
-    for (int k = n - 2; k >= 0; k--) {
-        const float2 ta = w.tau[k];
-
-        if (ta.x == 0.f && ta.y == 0.f)
-            continue;
-        const float2 v0 = i0 > k && i0 < n ? w.T[i0 * ld + k] : make_float2(0.f, 0.f);
-        const float2 v1 = i1 > k && i1 < n ? w.T[i1 * ld + k] : make_float2(0.f, 0.f);
-        float sr = v0.x * z0.x + v0.y * z0.y + v1.x * z1.x + v1.y * z1.y;
-        float si = v0.x * z0.y - v0.y * z0.x + v1.x * z1.y - v1.y * z1.x;
-
-        sr = gsum(sr, g);
-        si = gsum(si, g);
-        const float hr = ta.x * sr - ta.y * si, hi = ta.x * si + ta.y * sr;
-
-        z0.x -= v0.x * hr - v0.y * hi;
-        z0.y -= v0.x * hi + v0.y * hr;
-        z1.x -= v1.x * hr - v1.y * hi;
-        z1.y -= v1.x * hi + v1.y * hr;
-    }
+    apply_q(n, ld, w, g, false, z0, z1);
     return status;
 }
 
@@ -857,27 +921,7 @@ __device__ void solve_off(int n, int ld, const HWs &w, const Grp &g, const float
     const int i0 = g.gl, i1 = g.gl + 16;
 
     /* b = Q^H b = H_{n-2} .. H_0 b */
-    for (int k = 0; k < n - 1; k++) {
-        const float2 ta = w.tau[k];
-
-        if (ta.x == 0.f && ta.y == 0.f)
-            continue;
-        const float2 v0 = i0 > k && i0 < n ? w.T[i0 * ld + k] : make_float2(0.f, 0.f);
-        const float2 v1 = i1 > k && i1 < n ? w.T[i1 * ld + k] : make_float2(0.f, 0.f);
-        float sr = v0.x * b0.x + v0.y * b0.y + v1.x * b1.x + v1.y * b1.y;
-        float si = v0.x * b0.y - v0.y * b0.x + v1.x * b1.y - v1.y * b1.x;
-
-        sr = gsum(sr, g);
-        si = gsum(si, g);
-        /* H^H b = b - conj(tau) v (v^H b) */
-        const float hr = ta.x * sr + ta.y * si;
-        const float hi = ta.x * si - ta.y * sr;
-
-        b0.x -= v0.x * hr - v0.y * hi;
-        b0.y -= v0.x * hi + v0.y * hr;
-        b1.x -= v1.x * hr - v1.y * hi;
-        b1.y -= v1.x * hi + v1.y * hr;
-    }
+    apply_q(n, ld, w, g, true, b0, b1);
     /* b is in the real-tridiagonal basis but complex-valued: solve the real
        and imaginary parts with the float LU of (tri - lambda), off y. */
     float2 *bs = (float2 *)w.x;
@@ -906,8 +950,21 @@ __device__ void solve_off(int n, int ld, const HWs &w, const Grp &g, const float
         tr_[k] = fmaf(-cr, yr[k], tr_[k]);
         ti_[k] = fmaf(-ci, yr[k], ti_[k]);
     }
-    tri_solve(tr_, n, piv, w);
-    tri_solve(ti_, n, piv, w);
+    /* one solve per lane: the real parts in lanes 0-7, the imaginary parts
+       in lanes 8-15, exchanged afterwards */
+    {
+        float v[32];
+
+#pragma unroll
+        for (int k = 0; k < 32; k++)
+            v[k] = g.gl >= 8 ? ti_[k] : tr_[k];
+        tri_solve(v, n, piv, w);
+#pragma unroll
+        for (int k = 0; k < 32; k++) {
+            tr_[k] = __shfl_sync(g.mask, v[k], g.base);
+            ti_[k] = __shfl_sync(g.mask, v[k], g.base | 8);
+        }
+    }
     float dr = 0.f, di = 0.f;
 
 #pragma unroll
@@ -928,26 +985,7 @@ __device__ void solve_off(int n, int ld, const HWs &w, const Grp &g, const float
             t1 = make_float2(fmaf(-dr, yr[k], tr_[k]), fmaf(-di, yr[k], ti_[k]));
     }
     /* t = Q t = H_0 .. H_{n-2} t */
-    for (int k = n - 2; k >= 0; k--) {
-        const float2 ta = w.tau[k];
-
-        if (ta.x == 0.f && ta.y == 0.f)
-            continue;
-        const float2 v0 = i0 > k && i0 < n ? w.T[i0 * ld + k] : make_float2(0.f, 0.f);
-        const float2 v1 = i1 > k && i1 < n ? w.T[i1 * ld + k] : make_float2(0.f, 0.f);
-        float sr = v0.x * t0.x + v0.y * t0.y + v1.x * t1.x + v1.y * t1.y;
-        float si = v0.x * t0.y - v0.y * t0.x + v1.x * t1.y - v1.y * t1.x;
-
-        sr = gsum(sr, g);
-        si = gsum(si, g);
-        const float hr = ta.x * sr - ta.y * si;
-        const float hi = ta.x * si + ta.y * sr;
-
-        t0.x -= v0.x * hr - v0.y * hi;
-        t0.y -= v0.x * hi + v0.y * hr;
-        t1.x -= v1.x * hr - v1.y * hi;
-        t1.y -= v1.x * hi + v1.y * hr;
-    }
+    apply_q(n, ld, w, g, false, t0, t1);
 }
 
 /* One refinement step of the eigenpair of M for the eigenvector (z0, z1)
@@ -1026,37 +1064,19 @@ __device__ void refine(int n, int ld, const HWs &w, const Grp &g, double2 &x0, d
 /* Common stages.                                                      */
 /* ------------------------------------------------------------------ */
 
-/* T of the group's pixel from its packed Gram sums (tcoh.cl:611-636);
-   identity for an inactive group. The group's 16 lanes first issue all
-   their loads. */
-__device__ void load_T(const TcStrip &s, const TcChunk &c, const TcLinkConst &k, int p, bool active,
-                       int looks, const float2 *__restrict__ gram,
-                       const unsigned short *__restrict__ upper_tab, const HWs &w, int ld,
-                       const Grp &g)
+/* One batch of the packed entries q = gl + 16 t (t = t0 .. t0 + B - 1):
+   T_ij = C_ij / (nrm_i nrm_j), bias-corrected, both triangles. */
+template <int B>
+__device__ __forceinline__ void load_T_batch(const float2 (&gv)[B], int t0, int n, int npu, bool active,
+                                             int looks, const TcLinkConst &k,
+                                             const unsigned short *upper_tab, const HWs &w,
+                                             int ld, const Grp &g)
 {
-    const int n = s.n, npu = tc_npu(n);
-    const int i0 = g.gl, i1 = g.gl + 16;
-    float2 gv[33];
-
-    /* every load issued before any use */
-    const float d0 = (active && i0 < n) ? gram[tc_gram_at(npu, p, tc_pidx(n, i0, i0))].x : 1.f;
-    const float d1 = (active && i1 < n) ? gram[tc_gram_at(npu, p, tc_pidx(n, i1, i1))].x : 1.f;
-#pragma unroll
-    for (int t = 0; t < 33; t++) {
-        const int q = g.gl + 16 * t;
-
-        gv[t] = (active && q < npu) ? gram[tc_gram_at(npu, p, q)] : make_float2(0.f, 0.f);
-    }
-    if (i0 < n)
-        w.nrm[i0] = __fsqrt_rn(d0);
-    if (i1 < n)
-        w.nrm[i1] = __fsqrt_rn(d1);
-    gsync(g);
     const float fl = (float)looks;
 
 #pragma unroll
-    for (int t = 0; t < 33; t++) {
-        const int q = g.gl + 16 * t;
+    for (int t = 0; t < B; t++) {
+        const int q = g.gl + 16 * (t0 + t);
 
         if (q >= npu)
             continue;
@@ -1090,6 +1110,42 @@ __device__ void load_T(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
         w.T[i * ld + j] = make_float2(re, im);
         w.T[j * ld + i] = make_float2(re, -im);
     }
+}
+
+/* T of the group's pixel from its packed Gram sums (tcoh.cl:611-636);
+   identity for an inactive group. The entries come in two batches of 17
+   and 16 per lane, each batch's loads issued before any use (one batch
+   of 33 held 66 registers through the processing and spilled); upper_tab
+   is the CTA's shared-memory copy of the packed-entry table. */
+__device__ void load_T(const TcStrip &s, const TcChunk &c, const TcLinkConst &k, int p, bool active,
+                       int looks, const float2 *__restrict__ gram,
+                       const unsigned short *upper_tab, const HWs &w, int ld, const Grp &g)
+{
+    const int n = s.n, npu = tc_npu(n);
+    const int i0 = g.gl, i1 = g.gl + 16;
+    float2 ga[17], gb[16];
+
+    const float d0 = (active && i0 < n) ? gram[tc_gram_at(npu, p, tc_pidx(n, i0, i0))].x : 1.f;
+    const float d1 = (active && i1 < n) ? gram[tc_gram_at(npu, p, tc_pidx(n, i1, i1))].x : 1.f;
+#pragma unroll
+    for (int t = 0; t < 17; t++) {
+        const int q = g.gl + 16 * t;
+
+        ga[t] = (active && q < npu) ? gram[tc_gram_at(npu, p, q)] : make_float2(0.f, 0.f);
+    }
+    if (i0 < n)
+        w.nrm[i0] = __fsqrt_rn(d0);
+    if (i1 < n)
+        w.nrm[i1] = __fsqrt_rn(d1);
+    gsync(g);
+    load_T_batch<17>(ga, 0, n, npu, active, looks, k, upper_tab, w, ld, g);
+#pragma unroll
+    for (int t = 0; t < 16; t++) {
+        const int q = g.gl + 16 * (17 + t);
+
+        gb[t] = (active && q < npu) ? gram[tc_gram_at(npu, p, q)] : make_float2(0.f, 0.f);
+    }
+    load_T_batch<16>(gb, 17, n, npu, active, looks, k, upper_tab, w, ld, g);
     gsync(g);
 }
 
@@ -1526,6 +1582,12 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
     const long long plane = (long long)s.rows * s.cols;
     double *V = scratch + ((size_t)blockIdx.x * wpb * 2 + grp) * (size_t)(2 * n * ld + 32);
     const int i0 = g.gl, i1 = g.gl + 16;
+    /* the packed-entry table, read in every stage, from shared memory */
+    unsigned short *s_upper = (unsigned short *)(smem + (size_t)wpb * 2 * L.per_group);
+
+    for (int e = threadIdx.x; e < tc_npu(n); e += blockDim.x)
+        s_upper[e] = upper_tab[e];
+    __syncthreads();
 
     /* The warps of a CTA take pixel pairs qb + warp and run each stage
        together, separated by CTA barriers: the stages' code is far larger
@@ -1562,7 +1624,7 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
 
         /* stage 1: coherence matrix, pair coherences, connectivity */
         if (run) {
-            load_T(s, c, k, p, active, looks, gram, upper_tab, w, ld, g);
+            load_T(s, c, k, p, active, looks, gram, s_upper, w, ld, g);
             if (active)
                 for (int t = g.gl; t < k.npairs; t += 16) {
                     const int i = pair_tab[t] >> 8, j = pair_tab[t] & 255;
@@ -1661,7 +1723,7 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
         float2 ssum = make_float2(0.f, 0.f);
 
         if (run) {
-            const float gamma = gamma16(n, ld, w, g, z0, z1, upper_tab, &ssum);
+            const float gamma = gamma16(n, ld, w, g, z0, z1, s_upper, &ssum);
 
             if (active) {
                 if (g.gl == 0)
@@ -1686,7 +1748,7 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
                 backward16<EMI>(n, ld, w, g, z0, z1, ssum, yr, piv, looks, k.bias != 0, active,
                                 (float2 *)(smem + (size_t)grp * L.per_group + L.off_Tb),
                                 (double *)(smem + (size_t)grp * L.per_group + L.off_Db),
-                                upper_tab, gbar, c.npix, p);
+                                s_upper, gbar, c.npix, p);
             else
                 for (int t = g.gl; t < tc_npu(n); t += 16)
                     gbar[(long long)t * c.npix + p] = make_float2(0.f, 0.f);
@@ -1752,14 +1814,15 @@ static cudaError_t launch_half(const TcStrip &s, const TcChunk &c, const TcLinkC
 {
     const HalfLayout L = half_layout(s.n, EMI, ADJ);
     const size_t per_warp = 2 * (size_t)L.per_group;
+    const size_t tab = ((size_t)tc_npu(s.n) * 2 + 15) & ~(size_t)15;
     const int max_warps = EMI || ADJ ? 8 : 12;
-    int wpb = (int)((227 * 1024) / per_warp);
+    int wpb = (int)((227 * 1024 - tab) / per_warp);
 
     if (wpb > max_warps)
         wpb = max_warps;
     if (wpb < 1)
         return cudaErrorInvalidConfiguration;
-    const size_t smem = per_warp * wpb;
+    const size_t smem = per_warp * wpb + tab;
     const int want = (c.npix / 2 + wpb - 1) / wpb;
     const int blocks = want < sms ? want : sms;
     cudaError_t e = cudaFuncSetAttribute(tc_link_half_kernel<EMI, ADJ>,
