@@ -234,7 +234,7 @@ def accuracy(slc, amp, valid, coh_gpu, count_gpu, rows, cols, kw, size=48):
     cnt = count_gpu[r0:r0 + size, c0:c0 + size]
     m = ~np.isnan(o32["coh"]) & ~np.isnan(g)
     err = np.abs(g[m] - o32["coh"][m])
-    return {
+    out = {
         "pixels": int(size * size),
         "max_abs": float(err.max()) if err.size else None,
         "rms": float(np.sqrt(np.mean(err ** 2))) if err.size else None,
@@ -242,6 +242,27 @@ def accuracy(slc, amp, valid, coh_gpu, count_gpu, rows, cols, kw, size=48):
         "null_mask_mismatch": int((np.isnan(g) != np.isnan(o32["coh"])).sum()),
         "shp_count_flips_float_vs_fp64": int((o32["count"] != o64["count"]).sum()),
     }
+    # The other outputs on the same crop: all pair coherences |T_ij| and the
+    # per-date phases (wrapped difference, radians).
+    import tcoh_b200
+
+    n = amp.shape[2]
+    s = tcoh_b200.make_settings(n, pairs=True, pairs_all=True, **kw)
+    with tcoh_b200.Backend(s, size + 2 * hr) as be:
+        r = be.run(*crop, size, size, phases=True)
+    o = oracle.run_oracle(*crop, size, size, shp_fp32=True, npairs=s.npairs, pairs_all=True,
+                          want_phases=True, **kw)
+    pm = ~np.isnan(o["pairs"]) & ~np.isnan(r["pairs"])
+    perr = np.abs(r["pairs"][pm].astype(np.float64) - o["pairs"][pm])
+    ph = ~np.isnan(o["phases"]) & ~np.isnan(r["phases"])
+    d = np.angle(np.exp(1j * (r["phases"][ph].astype(np.float64) - o["phases"][ph])))
+    out["pairs"] = {"planes": int(s.npairs), "max_abs": float(perr.max()) if perr.size else None,
+                    "rms": float(np.sqrt(np.mean(perr ** 2))) if perr.size else None,
+                    "null_mask_mismatch": int((np.isnan(o["pairs"]) != np.isnan(r["pairs"])).sum())}
+    out["phases_rad"] = {"max_abs": float(np.abs(d).max()) if d.size else None,
+                         "rms": float(np.sqrt(np.mean(d ** 2))) if d.size else None,
+                         "p999": float(np.quantile(np.abs(d), 0.999)) if d.size else None}
+    return out
 
 
 # ---------------------------------------------------------------------------
