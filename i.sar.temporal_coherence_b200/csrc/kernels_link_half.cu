@@ -1301,18 +1301,19 @@ __device__ __forceinline__ float2 t_full(const HWs &w, int ld, int i, int j)
    |T|-bar = -|T|^-1 Re(conj(M-bar) o T) |T|^-1 (double); the bias correction
    |T| = sqrt((L |t|^2 - 1) / (L - 1)); the normalization
    t_ij = C_ij / sqrt(C_ii C_jj) (C_ii does not depend on the phases).
-   z0, z1: the final eigenvector rows; S: the sum of gamma16; Tb: n x ld
-   float2 scratch, Db: n x ld double scratch (EMI). An inactive pixel gets
-   G = 0. */
+   z0, z1: the final eigenvector rows; S: the sum of gamma16. The rows
+   (i0, i1) of T-bar stay in registers (those of the reduction are free by
+   now); once solve_off, the last reader of the Householder vectors, is
+   done, their strictly lower parts go to T's lower triangle so that the
+   owner of row i forms G_ij = (T-bar_ij + conj(T-bar_ji)) / 2 for j > i.
+   Db: n x ld double scratch (EMI). An inactive pixel gets G = 0. */
 template <bool EMI>
 __device__ void backward16(int n, int ld, const HWs &w, const Grp &g, double2 z0d, double2 z1d,
                            float2 S, const float (&yr)[32], unsigned long long piv, int looks,
-                           bool bias, bool active, float2 *Tb, double *Db,
-                           const unsigned short *__restrict__ upper_tab, float2 *gbar,
-                           long long npix, long long p)
+                           bool bias, bool active, double *Db, float2 *gbar, long long npix,
+                           long long p)
 {
     const int i0 = g.gl, i1 = g.gl + 16;
-    const int npu = tc_npu(n);
 
     /* unit-norm z in float; the phasor decisions (reference date, floor)
        are those of gamma16, from the double rows */
@@ -1348,46 +1349,47 @@ __device__ void backward16(int n, int ld, const HWs &w, const Grp &g, double2 z0
     const float P = 0.5f * n * (n - 1), sm = hypotf(S.x, S.y);
     const float2 Sb = sm > 0.f ? make_float2(S.x / (sm * P), S.y / (sm * P)) : make_float2(0.f, 0.f);
     const float2 Sc = make_float2(Sb.x, -Sb.y);
+    float2 tb0[32], tb1[32]; /* T-bar rows i0, i1 */
     float2 vb[2];
 
 #pragma unroll
     for (int t = 0; t < 2; t++) {
         const int r = t ? i1 : i0;
         float2 eb = make_float2(0.f, 0.f);
+        const float2 er = r < n ? w.zs[r] : make_float2(1.f, 0.f);
 
-        if (r < n) {
-            const float2 er = w.zs[r];
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+            float2 tb = make_float2(0.f, 0.f);
 
-            for (int j = 0; j < n; j++) {
-                float2 tb = make_float2(0.f, 0.f);
+            if (r < n && j < n && j != r) {
+                const float2 tv = t_full(w, ld, r, j);
+                const float m2 = tv.x * tv.x + tv.y * tv.y;
+                const float im = m2 > 0.f ? rsqrtf(m2) : 0.f;
+                const float2 wv = m2 > 0.f ? make_float2(tv.x * im, tv.y * im)
+                                           : make_float2(1.f, 0.f);
+                const float2 ej = w.zs[j];
+                /* j > r: e-bar_r += conj(S-bar) w_rj e_j; j < r: e-bar_r +=
+                   S-bar conj(w_jr) e_j = S-bar w_rj e_j */
+                const float2 c = cmul(cmul(j > r ? Sc : Sb, wv), ej);
 
-                if (j != r) {
-                    const float2 tv = t_full(w, ld, r, j);
-                    const float m2 = tv.x * tv.x + tv.y * tv.y;
-                    const float im = m2 > 0.f ? rsqrtf(m2) : 0.f;
-                    const float2 wv = m2 > 0.f ? make_float2(tv.x * im, tv.y * im)
-                                               : make_float2(1.f, 0.f);
-                    const float2 ej = w.zs[j];
-                    /* j > r: e-bar_r += conj(S-bar) w_rj e_j; j < r: e-bar_r +=
-                       S-bar conj(w_jr) e_j = S-bar w_rj e_j */
-                    const float2 c = cmul(cmul(j > r ? Sc : Sb, wv), ej);
+                eb = make_float2(eb.x + c.x, eb.y + c.y);
+                if (j > r && m2 > 0.f) {
+                    /* w-bar_rj = S-bar e_r conj(e_j), through w = T / |T| */
+                    const float2 wb = cmul(Sb, cmulc(er, ej));
+                    const float rr = wv.x * wb.x + wv.y * wb.y;
 
-                    eb = make_float2(eb.x + c.x, eb.y + c.y);
-                    if (j > r && m2 > 0.f) {
-                        /* w-bar_rj = S-bar e_r conj(e_j), through w = T / |T| */
-                        const float2 wb = cmul(Sb, cmulc(er, ej));
-                        const float rr = wv.x * wb.x + wv.y * wb.y;
-
-                        tb = make_float2((wb.x - wv.x * rr) * im, (wb.y - wv.y * rr) * im);
-                    }
+                    tb = make_float2((wb.x - wv.x * rr) * im, (wb.y - wv.y * rr) * im);
                 }
-                Tb[r * ld + j] = tb;
             }
+            if (t)
+                tb1[j] = tb;
+            else
+                tb0[j] = tb;
         }
         /* v-bar_r = (e-bar - e Re(conj(e) e-bar)) / |v_r| */
         vb[t] = make_float2(0.f, 0.f);
         if (t ? big1 : big0) {
-            const float2 er = w.zs[r];
             const float2 zv = t ? z1 : z0;
             const float vm = hypotf(zv.x, zv.y) * hypotf(zr.x, zr.y);
             const float rr = er.x * eb.x + er.y * eb.y;
@@ -1433,78 +1435,92 @@ __device__ void backward16(int n, int ld, const HWs &w, const Grp &g, double2 z0
     gsync(g);
     if (!EMI) {
 #pragma unroll
-        for (int t = 0; t < 2; t++) {
-            const int r = t ? i1 : i0;
-            const float2 yv = t ? y1 : y0;
+        for (int j = 0; j < 32; j++) {
+            const float2 zj = j < n ? zb[j] : make_float2(0.f, 0.f);
+            const float2 x0 = cmulc(y0, zj), x1 = cmulc(y1, zj);
 
-            if (r < n)
-                for (int j = 0; j < n; j++) {
-                    const float2 xb = cmulc(yv, zb[j]);
-
-                    Tb[r * ld + j].x += xb.x;
-                    Tb[r * ld + j].y += xb.y;
-                }
+            tb0[j].x += x0.x;
+            tb0[j].y += x0.y;
+            tb1[j].x += x1.x;
+            tb1[j].y += x1.y;
         }
     }
     else {
         /* M = A o T with A = |T|^-1 (packed, double): T-bar += A o M-bar,
-           A-bar = Re(conj(M-bar) o T) */
+           A-bar = Re(conj(M-bar) o T) (rows to Db) */
 #pragma unroll
         for (int t = 0; t < 2; t++) {
             const int r = t ? i1 : i0;
             const float2 yv = t ? y1 : y0;
 
-            if (r < n)
-                for (int j = 0; j < n; j++) {
+#pragma unroll
+            for (int j = 0; j < 32; j++)
+                if (r < n && j < n) {
                     const float2 mb = cmulc(yv, zb[j]);
                     const double a = w.G[sym_idx(n, r, j)];
                     const float2 tv = t_full(w, ld, r, j);
 
-                    Tb[r * ld + j].x += (float)a * mb.x;
-                    Tb[r * ld + j].y += (float)a * mb.y;
+                    if (t) {
+                        tb1[j].x += (float)a * mb.x;
+                        tb1[j].y += (float)a * mb.y;
+                    } else {
+                        tb0[j].x += (float)a * mb.x;
+                        tb0[j].y += (float)a * mb.y;
+                    }
                     Db[r * ld + j] = (double)mb.x * tv.x + (double)mb.y * tv.y;
                 }
         }
-        gsync(g);
-        /* |T|-bar = -A A-bar A, rows (i0, i1): P = A A-bar in registers */
-        double p0[32], p1[32];
-
-#pragma unroll
-        for (int j = 0; j < 32; j++)
-            p0[j] = p1[j] = 0.0;
-        for (int l = 0; l < n; l++) {
-            const double a0 = i0 < n ? w.G[sym_idx(n, i0, l)] : 0.0;
-            const double a1 = i1 < n ? w.G[sym_idx(n, i1, l)] : 0.0;
-
-#pragma unroll
-            for (int j = 0; j < 32; j++)
-                if (j < n) {
-                    const double ab = Db[l * ld + j];
-
-                    p0[j] = fma(a0, ab, p0[j]);
-                    p1[j] = fma(a1, ab, p1[j]);
-                }
-        }
+        /* |T|-bar = -A (A-bar A): first Q = A-bar A, each lane's rows in
+           place (it reads only its own rows of A-bar) */
 #pragma unroll
         for (int t = 0; t < 2; t++) {
             const int r = t ? i1 : i0;
 
-            if (r < n)
-                for (int j = 0; j < n; j++) {
-                    double bb = 0.0;
+            if (r < n) {
+                double q[32];
 
 #pragma unroll
-                    for (int k = 0; k < 32; k++)
-                        if (k < n)
-                            bb = fma(t ? p1[k] : p0[k], w.G[sym_idx(n, k, j)], bb);
-                    bb = -bb;
-                    if (j != r) {
-                        const float2 tv = t_full(w, ld, r, j);
-                        const float m = hypotf(tv.x, tv.y);
+                for (int j = 0; j < 32; j++)
+                    q[j] = 0.0;
+                for (int l = 0; l < n; l++) {
+                    const double ab = Db[r * ld + l];
 
-                        if (m > 0.f) {
-                            Tb[r * ld + j].x += (float)bb * tv.x / m;
-                            Tb[r * ld + j].y += (float)bb * tv.y / m;
+#pragma unroll
+                    for (int j = 0; j < 32; j++)
+                        if (j < n)
+                            q[j] = fma(ab, w.G[sym_idx(n, l, j)], q[j]);
+                }
+#pragma unroll
+                for (int j = 0; j < 32; j++)
+                    if (j < n)
+                        Db[r * ld + j] = q[j];
+            }
+        }
+        gsync(g);
+        /* then |T|-bar_rj = -(A Q)_rj, into T-bar through |T| */
+#pragma unroll
+        for (int t = 0; t < 2; t++) {
+            const int r = t ? i1 : i0;
+
+#pragma unroll
+            for (int j = 0; j < 32; j++)
+                if (r < n && j < n && j != r) {
+                    double bb = 0.0;
+
+                    for (int k = 0; k < n; k++)
+                        bb = fma(w.G[sym_idx(n, r, k)], Db[k * ld + j], bb);
+                    const float2 tv = t_full(w, ld, r, j);
+                    const float m = hypotf(tv.x, tv.y);
+
+                    if (m > 0.f) {
+                        const float b = (float)-bb;
+
+                        if (t) {
+                            tb1[j].x += b * tv.x / m;
+                            tb1[j].y += b * tv.y / m;
+                        } else {
+                            tb0[j].x += b * tv.x / m;
+                            tb0[j].y += b * tv.y / m;
                         }
                     }
                 }
@@ -1517,45 +1533,75 @@ __device__ void backward16(int n, int ld, const HWs &w, const Grp &g, double2 z0
     for (int t = 0; t < 2; t++) {
         const int r = t ? i1 : i0;
 
-        if (r < n)
-            for (int j = 0; j < n; j++) {
-                float2 tb = Tb[r * ld + j];
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+            float2 tb = t ? tb1[j] : tb0[j];
 
-                if (j == r)
-                    tb = make_float2(0.f, 0.f);
-                else if (bias && looks > 1) {
-                    const float2 tv = t_full(w, ld, r, j);
-                    const float mT = hypotf(tv.x, tv.y);
+            if (r >= n || j >= n || j == r)
+                tb = make_float2(0.f, 0.f);
+            else if (bias && looks > 1) {
+                const float2 tv = t_full(w, ld, r, j);
+                const float mT = hypotf(tv.x, tv.y);
 
-                    if (mT > 0.f) {
-                        /* t = unit(T) |t|, |t|^2 = ((L - 1) |T|^2 + 1) / L */
-                        const float m2 = ((L - 1.f) * mT * mT + 1.f) / L;
-                        const float mt = sqrtf(m2), c = mT / mt;
-                        const float2 tt = make_float2(tv.x / c, tv.y / c);
-                        const float kap = (tb.x * tt.x + tb.y * tt.y) / (c * (L - 1.f) * m2 * m2);
+                if (mT > 0.f) {
+                    /* t = unit(T) |t|, |t|^2 = ((L - 1) |T|^2 + 1) / L */
+                    const float m2 = ((L - 1.f) * mT * mT + 1.f) / L;
+                    const float mt = sqrtf(m2), c = mT / mt;
+                    const float2 tt = make_float2(tv.x / c, tv.y / c);
+                    const float kap = (tb.x * tt.x + tb.y * tt.y) / (c * (L - 1.f) * m2 * m2);
 
-                        tb = make_float2(c * tb.x + kap * tt.x, c * tb.y + kap * tt.y);
-                    }
-                    else
-                        tb = make_float2(0.f, 0.f);
+                    tb = make_float2(c * tb.x + kap * tt.x, c * tb.y + kap * tt.y);
                 }
+                else
+                    tb = make_float2(0.f, 0.f);
+            }
+            if (r < n && j < n) {
                 const float sc = 1.f / (w.nrm[r] * w.nrm[j]);
 
-                Tb[r * ld + j] = make_float2(tb.x * sc, tb.y * sc);
+                tb = make_float2(tb.x * sc, tb.y * sc);
             }
+            if (t)
+                tb1[j] = tb;
+            else
+                tb0[j] = tb;
+        }
+    }
+    /* the strictly lower parts of the rows to T's lower triangle (the
+       Householder vectors were last read by solve_off) */
+    gsync(g);
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+        const int r = t ? i1 : i0;
+
+#pragma unroll
+        for (int j = 0; j < 32; j++)
+            if (r < n && j < r)
+                w.T[r * ld + j] = t ? tb1[j] : tb0[j];
     }
     gsync(g);
-    /* G_ij = (C-bar_ij + conj(C-bar_ji)) / 2, upper triangle */
-    for (int q = g.gl; q < npu; q += 16) {
-        const int i = upper_tab[q] >> 8, j = upper_tab[q] & 255;
-        float2 v = make_float2(0.f, 0.f);
+    /* G_rj = (C-bar_rj + conj(C-bar_jr)) / 2 for j >= r (zero on the
+       diagonal), by the owner of row r */
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+        const int r = t ? i1 : i0;
 
-        if (active && i != j) {
-            const float2 a = Tb[i * ld + j], b = Tb[j * ld + i];
+        if (r < n) {
+            float2 *row = gbar + (long long)tc_pidx(n, r, r) * npix + p;
 
-            v = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
+            row[0] = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int j = 1; j < 32; j++)
+                if (j > r && j < n) {
+                    float2 v = make_float2(0.f, 0.f);
+
+                    if (active) {
+                        const float2 a = t ? tb1[j] : tb0[j], b = w.T[j * ld + r];
+
+                        v = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
+                    }
+                    row[(long long)(j - r) * npix] = v;
+                }
         }
-        gbar[(long long)q * npix + p] = v;
     }
     gsync(g);
 }
@@ -1746,9 +1792,8 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
         if (ADJ && q < nq) {
             if (run)
                 backward16<EMI>(n, ld, w, g, z0, z1, ssum, yr, piv, looks, k.bias != 0, active,
-                                (float2 *)(smem + (size_t)grp * L.per_group + L.off_Tb),
-                                (double *)(smem + (size_t)grp * L.per_group + L.off_Db),
-                                s_upper, gbar, c.npix, p);
+                                (double *)(smem + (size_t)grp * L.per_group + L.off_Db), gbar,
+                                c.npix, p);
             else
                 for (int t = g.gl; t < tc_npu(n); t += 16)
                     gbar[(long long)t * c.npix + p] = make_float2(0.f, 0.f);
@@ -1787,7 +1832,7 @@ HalfLayout half_layout(int n, int emi, int adj = 0)
     L.off_nrm = take(4 * 32);
     L.off_zs = take(8 * 32);
     L.off_lam = 0;
-    L.off_Tb = take(adj ? 8 * n * L.ld : 0);
+    L.off_Tb = 0; /* the backward keeps T-bar in registers */
     L.off_Db = take(adj && emi ? 8 * n * L.ld : 0);
     L.per_group = off;
     return L;
