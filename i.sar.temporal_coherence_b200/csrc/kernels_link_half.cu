@@ -107,7 +107,7 @@ struct HWs {
     float4 *vw;
     float4 *lu;
     float2 *tau;
-    float *d, *e, *df, *e2f, *y, *nrm;
+    float *d, *e, *df, *e2f, *y, *nrm; /* nrm: 1 / sqrt(C_ii) */
     float2 *zs;
     double *rs, *lam;
     double2 *x; /* double vectors of the refinement (2 x 32) */
@@ -1073,6 +1073,8 @@ __device__ __forceinline__ void load_T_batch(const float2 (&gv)[B], int t0, int 
                                              int ld, const Grp &g)
 {
     const float fl = (float)looks;
+    const bool debias = k.bias && looks > 1;
+    const float ilm1 = debias ? __frcp_rn(fl - 1.0f) : 0.f;
 
 #pragma unroll
     for (int t = 0; t < B; t++) {
@@ -1089,18 +1091,19 @@ __device__ __forceinline__ void load_T_batch(const float2 (&gv)[B], int t0, int 
         float re = 0.f, im = 0.f;
 
         if (active) {
+            /* w.nrm holds 1 / sqrt(C_ii) (0 for an empty date) */
             const float2 gq = gv[t];
-            const float dd = __fmul_rn(w.nrm[i], w.nrm[j]);
+            const float rd = w.nrm[i] * w.nrm[j];
 
-            if (dd > 0.f) {
-                const float rd = __frcp_rn(dd);
-
+            if (rd > 0.f) {
                 re = gq.x * rd;
                 im = gq.y * rd;
-                if (k.bias && looks > 1) {
+                if (debias) {
+                    /* f^2 = m2c / m2, m2c = (L m2 - 1) / (L - 1) */
                     const float m2 = re * re + im * im;
-                    const float m2c = (fl * m2 - 1.0f) * __frcp_rn(fl - 1.0f);
-                    const float f = (m2 > 0.f && m2c > 0.f) ? sqrtf(m2c * __frcp_rn(m2)) : 0.f;
+                    const float m2c = fmaf(fl, m2, -1.0f) * ilm1;
+                    const float f2 = m2 > 0.f && m2c > 0.f ? m2c * __fdividef(1.0f, m2) : 0.f;
+                    const float f = f2 > 0.f ? f2 * rsqrtf(f2) : 0.f;
 
                     re *= f;
                     im *= f;
@@ -1134,9 +1137,9 @@ __device__ void load_T(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
         ga[t] = (active && q < npu) ? gram[tc_gram_at(npu, p, q)] : make_float2(0.f, 0.f);
     }
     if (i0 < n)
-        w.nrm[i0] = __fsqrt_rn(d0);
+        w.nrm[i0] = d0 > 0.f ? __frcp_rn(__fsqrt_rn(d0)) : 0.f;
     if (i1 < n)
-        w.nrm[i1] = __fsqrt_rn(d1);
+        w.nrm[i1] = d1 > 0.f ? __frcp_rn(__fsqrt_rn(d1)) : 0.f;
     gsync(g);
     load_T_batch<17>(ga, 0, n, npu, active, looks, k, upper_tab, w, ld, g);
 #pragma unroll
@@ -1556,7 +1559,7 @@ __device__ void backward16(int n, int ld, const HWs &w, const Grp &g, double2 z0
                     tb = make_float2(0.f, 0.f);
             }
             if (r < n && j < n) {
-                const float sc = 1.f / (w.nrm[r] * w.nrm[j]);
+                const float sc = w.nrm[r] * w.nrm[j];
 
                 tb = make_float2(tb.x * sc, tb.y * sc);
             }
