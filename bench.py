@@ -42,9 +42,9 @@ WORKLOAD = dict(n=30, rows=4096, cols=4096, window=(21, 7), shp_test="ad", alpha
 METRIC = "Mpixel/s temporal coherence at N=30, 21x7 window, <=1e-4 vs FP64"
 # DRAM bytes (read + write) per pixel of one phase-linking launch, from an
 # ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of one
-# 65,536-pixel chunk at N=30, AD / EMI / bias correction: 244.4 MB read (the
-# packed Gram, 465 x 8 B per pixel, read once) + 7.1 MB written.
-LINK_DRAM_BYTES_PER_PIXEL = 251.5e6 / 65536
+# 65,536-pixel chunk at N=30, AD / EMI / bias correction: 232.2 MB read (the
+# packed Gram, 465 x 8 B per pixel, read at most once) + 7.3 MB written.
+LINK_DRAM_BYTES_PER_PIXEL = 239.4e6 / 65536
 
 
 def parse():

@@ -96,7 +96,7 @@ __device__ __forceinline__ void gsync(const Grp &g) { __syncwarp(g.mask); }
 struct HalfLayout {
     int n, ld;
     int off_T, off_G, off_vw, off_lu, off_tau, off_d, off_e, off_df, off_e2f, off_y,
-        off_nrm, off_zs, off_rs, off_lam, off_x, off_Tb, off_Db;
+        off_nrm, off_zs, off_rs, off_lam, off_x, off_Db;
     int per_group;
 };
 
@@ -479,7 +479,6 @@ __device__ float tri_eigenvalue(int n, int index, const HWs &w, const Grp &g, fl
 }
 
 __device__ __forceinline__ float rcpx(float x) { return __frcp_rn(x); }
-__device__ __forceinline__ double rcpx(double x) { return 1.0 / x; }
 
 /* Partially pivoted LU of tri - lambda I, into w.lu (written by the first
    lane of the group); returns the pivot bits. Every lane computes it. */
@@ -606,6 +605,21 @@ __device__ unsigned eigvec(int n, int index, const HWs &w, int ld, const Grp &g,
 /* EMI: |T|^-1 in double.                                              */
 /* ------------------------------------------------------------------ */
 
+/* 1 / d by two Newton-Raphson steps y <- y + y (1 - d y) from the hardware's
+   approximate FP64 reciprocal (within an ulp of the quotient; |d| here is a
+   pivot above the sweep's floor, never denormal or zero). */
+__device__ __forceinline__ double rcp_newton(double d)
+{
+    double y;
+
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(d));
+    double e = fma(-d, y, 1.0);
+
+    y = fma(y, e, y);
+    e = fma(-d, y, 1.0);
+    return fma(y, e, y);
+}
+
 /* Symmetric sweep (Gauss-Jordan elimination without pivoting in the form
    that keeps the matrix symmetric; Goodnight, The American Statistician 33,
    1979) of the group's matrix: rows i0, i1 in g0, g1, columns >= n zero.
@@ -635,7 +649,7 @@ __device__ bool sweep16(double (&g0)[32], double (&g1)[32], int n, double floor,
 
         if (!(fabs(d) > floor))
             return false;
-        const double id = 1.0 / d;
+        const double id = rcp_newton(d);
         const bool piv0 = i0 == k, piv1 = i1 == k;
         /* the pivot row scales by 1 / a_kk: a_kj - (1 - 1 / a_kk) a_kj, with
            a_kj from rs (equal to the row's own value up to rounding) */
@@ -1835,7 +1849,6 @@ HalfLayout half_layout(int n, int emi, int adj = 0)
     L.off_nrm = take(4 * 32);
     L.off_zs = take(8 * 32);
     L.off_lam = 0;
-    L.off_Tb = 0; /* the backward keeps T-bar in registers */
     L.off_Db = take(adj && emi ? 8 * n * L.ld : 0);
     L.per_group = off;
     return L;
