@@ -39,7 +39,27 @@ sys.path.insert(0, ROOT)
 
 WORKLOAD = dict(n=30, rows=4096, cols=4096, window=(21, 7), shp_test="ad", alpha=0.05,
                 min_shp=20, estimator="emi", bias=True, nregions=32, g0_max=0.99, spacing=12.0)
+# The other configurations of the path, as bench lines of their own (not the
+# metric's): N=10 KS/EVD on 512 x 512; N=60 KS with six-day dates (its
+# 8192 x 16384 scene as a 2048 x 2048 proxy unless --rows / --cols).
+WORKLOADS = {
+    "emi": WORKLOAD,
+    "ks10": dict(n=10, rows=512, cols=512, window=(21, 7), shp_test="ks", alpha=0.05,
+                 min_shp=10, estimator="evd", bias=False, nregions=8, g0_max=0.95, spacing=12.0),
+    "n60": dict(n=60, rows=2048, cols=2048, window=(21, 7), shp_test="ks", alpha=0.05,
+                min_shp=20, estimator="evd", bias=False, nregions=32, g0_max=0.99, spacing=6.0),
+    "n60emi": dict(n=60, rows=2048, cols=2048, window=(21, 7), shp_test="ks", alpha=0.05,
+                   min_shp=20, estimator="emi", bias=False, nregions=32, g0_max=0.99,
+                   spacing=6.0),
+}
 METRIC = "Mpixel/s temporal coherence at N=30, 21x7 window, <=1e-4 vs FP64"
+
+
+def metric_name(w):
+    if w is WORKLOAD:
+        return METRIC
+    return "Mpixel/s temporal coherence at N=%d, %dx%d window, <=1e-4 vs FP64" % (
+        w["n"], w["window"][0], w["window"][1])
 # DRAM bytes (read + write) per pixel of one phase-linking launch, from an
 # ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of one
 # 65,536-pixel chunk at N=30, AD / EMI / bias correction: 232.2 MB read (the
@@ -53,22 +73,25 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--rows", type=int, default=WORKLOAD["rows"])
-    p.add_argument("--cols", type=int, default=WORKLOAD["cols"])
+    p.add_argument("--rows", type=int, default=None, help="output rows (default: the workload's)")
+    p.add_argument("--cols", type=int, default=None, help="output columns (default: the workload's)")
     p.add_argument("--gram", default="tensor", choices=["tensor", "fp32"],
                    help="arithmetic of the coherence matrices (the tensor cores, else plain FP32)")
-    p.add_argument("--workload", default="emi", choices=["emi", "adjoint"],
+    p.add_argument("--workload", default="emi",
+                   choices=["emi", "adjoint", "geometry-pairs"] + [k for k in WORKLOADS if k != "emi"],
                    help="emi: the metric's configuration (default); adjoint: forward + "
                         "adjoint with geometry, a height error and a phase screen, and 20 "
                         "steps of gradient ascent on the height error (2048 x 2048 unless "
-                        "--rows / --cols)")
+                        "--rows / --cols); geometry-pairs: N=30 tlog with all pair "
+                        "coherences and the phase removed on the device from orbits and an "
+                        "elevation map (1024 x 2048 unless --rows / --cols); ks10, n60, "
+                        "n60emi: the other configurations")
     p.add_argument("--no-extras", action="store_true",
                    help="skip the e2e, plain-FP32, CPU and accuracy legs")
     return p.parse_args()
 
 
-def workload_name(rows, cols):
-    w = WORKLOAD
+def workload_name(rows, cols, w=WORKLOAD):
     return "N=%d %dx%d %s/%s%s window %dx%d, %d regions, coherence <= %.2f" % (
         w["n"], rows, cols, w["shp_test"], w["estimator"], "/-b" if w["bias"] else "",
         w["window"][0], w["window"][1], w["nregions"], w["g0_max"])
@@ -293,8 +316,8 @@ def adjoint_workload(args):
     import tcoh_b200.synthetic as syn
 
     n = 30
-    rows = args.rows if args.rows != WORKLOAD["rows"] else 2048
-    cols = args.cols if args.cols != WORKLOAD["cols"] else 2048
+    rows = args.rows or 2048
+    cols = args.cols or 2048
     ha, hr = 10, 3
     geo, orbits = scene.acquisition(n, rows, cols, seed=11)
     h = scene.fbm_heights(rows, cols, hurst=0.8, hmax=2000.0, seed=12)
@@ -381,15 +404,154 @@ def adjoint_workload(args):
     print(json.dumps(line))
 
 
+def geometry_pairs_workload(args):
+    """The configuration with geometry and all pair coherences, N=30 tlog /
+    EVD, window 21x7, min_shp 20, as a 1024 x 2048 proxy of its 4096 x 8192
+    scene (unless --rows / --cols): synthetic orbits (700 km, 7.6 km/s,
+    perpendicular baselines uniform in +-150 m, C band, 12-day dates) over a
+    fractal elevation map (H = 0.8, 0 - 2000 m); the raw I/Q planes carry
+    the geometric phase at each cell's height, which tc_run_raw removes on
+    the device before the path runs, with all 435 pair-coherence planes as
+    outputs. value: device-resident planes and outputs (tc_run_raw_device);
+    e2e: page-locked host planes in, all outputs back (tc_run_raw).
+    Accuracy on a 48 x 48 crop against the FP64 oracle (oracle strip
+    preparation from the same orbits)."""
+    import numpy as np
+    import torch
+
+    import tcoh_b200
+    import tcoh_b200.scene as scene
+    import tcoh_b200.synthetic as syn
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    n, window = 30, (21, 7)
+    rows, cols = args.rows or 1024, args.cols or 2048
+    ha, hr = window[0] // 2, window[1] // 2
+    prow = rows + 2 * ha
+    kw = dict(window=window, shp_test="tlog", alpha=0.05, min_shp=20, estimator="evd",
+              bias=False)
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    geo, orbits = scene.acquisition(n, rows, cols, seed=21)
+    h = scene.fbm_heights(rows, cols, hurst=0.8, hmax=2000.0, seed=22)
+    g = tcoh_b200.make_geometry(heights=h, h0=0.0, **geo)
+    grid = tcoh_b200.geometry_grid(g, orbits)
+    levels = ([g.hmin, 0.5 * (g.hmin + g.hmax), g.hmax] if grid.shape[2] == 3
+              else [0.5 * (g.hmin + g.hmax)])
+    stack = syn.generate(n, rows, cols, nregions=32, g0_max=0.99, seed=23, device=dev)
+    re = torch.full((n, prow, cols), float("nan"), dtype=torch.float32, device=dev)
+    im = torch.full_like(re, float("nan"))
+    for r0 in range(0, rows, 128):
+        r1 = min(rows, r0 + 128)
+        phi = torch.from_numpy(scene.grid_phases(grid, levels, h[r0:r1], row0=r0)).to(dev)
+        blk = stack[:, r0:r1] * torch.exp(-1j * phi).to(torch.complex64)
+        re[:, ha + r0:ha + r1] = blk.real
+        im[:, ha + r0:ha + r1] = blk.imag
+    del stack
+    elev_h = np.full((prow, cols), np.nan)
+    elev_h[ha:ha + rows] = h
+    elev = torch.from_numpy(elev_h).to(dev)
+    s = tcoh_b200.make_settings(n, pairs=True, pairs_all=True, **kw)
+    be = tcoh_b200.Backend(s, cols + 2 * hr, device=0)
+    be.set_geometry(g, grid)
+    coh = torch.empty((rows, cols), dtype=torch.float32, device=dev)
+    count = torch.empty((rows, cols), dtype=torch.int32, device=dev)
+    pairs = torch.empty((s.npairs, rows, cols), dtype=torch.float32, device=dev)
+    stream = torch.cuda.Stream(dev)
+
+    def step():
+        be.run_raw_device(re, im, elev, -ha, rows, rows, cols, coh, count, pairs=pairs,
+                          stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = Clocks(0)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    e1.synchronize()
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    npix = rows * cols
+    line = {"metric": "Mpixel/s temporal coherence at N=30, 21x7 window, all pair coherences, "
+                      "phase removed from orbits and elevation on the device",
+            "value": npix / (ms * 1e-3) / 1e6, "unit": "Mpixel/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "N=30 %dx%d tlog/evd window 21x7, pairs=all (%d planes), "
+                                   "fBm elevation 0-2000 m, synthetic orbits" % (rows, cols,
+                                                                                   s.npairs),
+                       "api": "tc_run_raw_device"},
+            "clocks": ck}
+    if not args.no_extras:
+        def pinned(t):
+            h_ = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+            h_.copy_(t)
+            return h_.numpy()
+
+        re_h, im_h = pinned(re), pinned(im)
+        out = {"coh": pinned(coh), "count": pinned(count), "pairs": pinned(pairs)}
+        be.run_raw(re_h, im_h, elev_h, -ha, rows, rows, cols, out=out)
+        t = time.perf_counter()
+        for _ in range(3):
+            be.run_raw(re_h, im_h, elev_h, -ha, rows, rows, cols, out=out)
+        dt = (time.perf_counter() - t) / 3
+        line["e2e"] = {"value": npix / dt / 1e6, "unit": "Mpixel/s",
+                       "h2d_bytes_per_step": int(re_h.nbytes + im_h.nbytes + elev_h.nbytes),
+                       "d2h_bytes_per_step": int(sum(v.nbytes for v in out.values())),
+                       "ms_per_step": dt * 1e3, "api": "tc_run_raw (page-locked buffers)"}
+        # accuracy on a crop: oracle strip preparation from the same grid
+        import oracle
+
+        size = 48
+        r0, c0 = rows // 2, cols // 2
+        sub = dict(geo, rows=rows, cols=cols, hmin=g.hmin, hmax=g.hmax, h0=0.0)
+        re_c = re_h[:, r0:r0 + size + 2 * ha].copy()
+        im_c = im_h[:, r0:r0 + size + 2 * ha].copy()
+        el_c = elev_h[r0:r0 + size + 2 * ha].copy()
+        # padded columns of output columns c0 .. c0 + size - 1
+        cs = slice(c0, c0 + size + 2 * hr)
+        slc_c, amp_c, valid_c = oracle.prepare_strip(re_c, im_c, el_c, r0 - ha, rows, hr, sub,
+                                                     grid)
+        slc_c, amp_c, valid_c = slc_c[:, cs], amp_c[:, cs], valid_c[:, cs]
+        o = oracle.run_oracle(np.ascontiguousarray(slc_c), np.ascontiguousarray(amp_c),
+                              np.ascontiguousarray(valid_c), size, size, npairs=s.npairs,
+                              pairs_all=True, shp_fp32=True, **kw)
+        gc = out["coh"][r0:r0 + size, c0:c0 + size].astype(np.float64)
+        gp = out["pairs"][:, r0:r0 + size, c0:c0 + size].astype(np.float64)
+        m = ~np.isnan(o["coh"]) & ~np.isnan(gc)
+        pm = ~np.isnan(o["pairs"]) & ~np.isnan(gp)
+        line["accuracy"] = {
+            "pixels": size * size,
+            "max_abs": float(np.abs(gc[m] - o["coh"][m]).max()) if m.any() else None,
+            "count_mismatch": int((out["count"][r0:r0 + size, c0:c0 + size] != o["count"]).sum()),
+            "null_mask_mismatch": int((np.isnan(gc) != np.isnan(o["coh"])).sum()),
+            "pairs_max_abs": float(np.abs(gp[pm] - o["pairs"][pm]).max()) if pm.any() else None}
+        line["mean_coherence"] = float(np.nanmean(out["coh"]))
+    be.close()
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     if args.workload == "adjoint" and args.impl != "reference":
         return adjoint_workload(args)
+    if args.workload == "geometry-pairs" and args.impl != "reference":
+        return geometry_pairs_workload(args)
+    if args.workload in ("adjoint", "geometry-pairs"):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the "
+                          "metric's configuration (--workload emi)"}))
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    w = dict(WORKLOAD)
-    rows, cols = args.rows, args.cols
+    w = WORKLOADS[args.workload]
+    rows, cols = args.rows or w["rows"], args.cols or w["cols"]
     ha, hr = w["window"][0] // 2, w["window"][1] // 2
     kw = dict(window=w["window"], shp_test=w["shp_test"], alpha=w["alpha"], min_shp=w["min_shp"],
               estimator=w["estimator"], bias=w["bias"])
@@ -429,11 +591,11 @@ def main():
             if i >= args.warmup:
                 vals.append(r["value"])
         v = float(np.mean(vals))
-        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Mpixel/s",
+        line = {"impl": "reference", "metric": metric_name(w), "value": v, "unit": "Mpixel/s",
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": workload_name(rows, cols), "parallelism": "host cores"},
+                "config": {"workload": workload_name(rows, cols, w), "parallelism": "host cores"},
                 "cpu_baseline": dict(r, value=v),
                 "e2e": {"value": v, "unit": "Mpixel/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
@@ -532,11 +694,11 @@ def main():
         roofline["algorithmic_bytes_per_launch"] = (8.0 * w["n"] * (w["n"] + 1) / 2 + 4) * px_launch
         roofline["traffic_source"] = ("ncu dram bytes of one 65,536-pixel launch, scaled by "
                                       "the pixels per launch")
-    line = {"metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": world,
+    line = {"metric": metric_name(w), "value": value, "unit": "Mpixel/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": workload_name(rows, cols), "gram": args.gram,
+            "config": {"workload": workload_name(rows, cols, w), "gram": args.gram,
                        "pixels_per_step": npix, "parallelism": "dp%d (independent strips)" % world,
                        "l2": "inputs %.1f GB per step > 126 MB L2, no flush" % (
                            (slc.numel() * 4 + amp.numel() * 4 + valid.numel()) / 1e9)},
