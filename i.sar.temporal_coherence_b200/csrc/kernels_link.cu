@@ -12,13 +12,13 @@
  *   EVD: eigenvector of the largest eigenvalue of T, in float (as
  *   tcoh.cl:649-656); EMI: eigenvector of the smallest eigenvalue of
  *   M = |T|^-1 o T (tcoh.cl:657-694), all in double: |T| is inverted by
- *   Gauss-Jordan when its pivots stay above 1e-5 (positive definite, the
- *   test of tcoh.cl:459), else through |T|^2 (an inverse of the symmetric
- *   indefinite matrix), and by its Jacobi eigen-pseudo-inverse with the
- *   absolute eigenvalue floor 1e-9 of tests/reference.py:151-156 when it is
- *   close to singular; the two differ only there, since the pseudo-inverse
- *   of a matrix whose eigenvalues all exceed 1e-9 in magnitude is its
- *   inverse;
+ *   the symmetric sweep (Gauss-Jordan without pivoting, which takes the
+ *   indefinite |T| of noisy stacks) when its pivots stay above 1e-5 in
+ *   magnitude and the inverse stays moderate, else by its Jacobi
+ *   eigen-pseudo-inverse with the absolute eigenvalue floor 1e-9 of
+ *   tests/reference.py:151-156; the two differ only near singularity,
+ *   since the pseudo-inverse of a matrix whose eigenvalues all exceed 1e-9
+ *   in magnitude is its inverse;
  *   the eigenvector is one Householder reduction to a real tridiagonal
  *   (LAPACK zhetd2 form), a 33-way multisection on Sturm counts for the
  *   wanted eigenvalue, inverse iteration on the tridiagonal and the
@@ -28,8 +28,11 @@
  *   (tcoh.cl:696-744).
  *
  * This file holds the path for 33 to 64 dates, where the matrices stay in
- * shared memory, two rows per lane, and the EMI inverse of |T| is a double
- * Cholesky with the Jacobi pseudo-inverse as fallback. Up to 32 dates the
+ * shared memory, two rows per lane. With EMI, |T| and its inverse occupy
+ * the first half of the working matrix's region (the Jacobi fallback's
+ * eigenvectors the second half) until M is formed over them, so that a
+ * warp needs T plus one complex double matrix: two warps per SM at 60
+ * dates. Up to 32 dates the
  * faster register path of kernels_link_half.cu runs instead (same stages,
  * same numerics, two pixels per warp).
  */
@@ -589,57 +592,61 @@ __device__ unsigned heig_smem(int n, int ld, typename Cx<R>::T *A, int index, co
     return status;
 }
 
-/* In-place inverse of the symmetric positive definite W (double, full
-   storage, shared memory) by Cholesky, X workspace. False when a pivot is
-   not above 1e-5 (tcoh.cl:449-492, in double precision). */
-__device__ bool chol_inverse_smem(int n, int ld, double *W, double *X, int lane)
+/* In-place inverse of the symmetric W (double, full storage, shared
+   memory) by the symmetric sweep (Gauss-Jordan elimination without
+   pivoting in the form that keeps the matrix symmetric; Goodnight, The
+   American Statistician 33, 1979): sweeping pivot k maps
+       a_ij -> a_ij - a_ik a_kj / a_kk,  a_ik, a_kj -> a_ik / a_kk,
+       a_kk -> -1 / a_kk,
+   and sweeping every pivot leaves -W^-1. It takes indefinite matrices. row
+   is n doubles of scratch (the pivot row before the step). False when a
+   pivot's magnitude is not above 1e-5, or when the inverse is not finite or
+   so large (n max|inv| >= 1e8) that an eigenvalue may lie below the
+   pseudo-inverse floor 1e-9; W is then undefined. */
+__device__ bool sweep_inverse_smem(int n, int ld, double *W, double *row, int lane)
 {
-    for (int j = 0; j < n; j++) {
-        const double djj = W[j * ld + j];
+    for (int k = 0; k < n; k++) {
+        const double d = W[k * ld + k];
 
-        if (!(djj > 1.0e-5))
+        if (!(fabs(d) > 1.0e-5))
             return false;
-        const double ljj = sqrt(djj);
+        const double id = 1.0 / d;
 
+        for (int j = lane; j < n; j += 32)
+            row[j] = W[k * ld + j];
         __syncwarp();
-        for (int r = lane; r < n; r += 32)
-            if (r > j)
-                W[r * ld + j] /= ljj;
-        if (lane == 0)
-            W[j * ld + j] = ljj;
-        __syncwarp();
-        for (int r = lane; r < n; r += 32)
-            if (r > j) {
-                const double lrj = W[r * ld + j];
+        for (int r = lane; r < n; r += 32) {
+            double *wr = W + r * ld;
 
-                for (int c = j + 1; c <= r; c++)
-                    W[r * ld + c] -= lrj * W[c * ld + j];
+            if (r == k)
+                for (int j = 0; j < n; j++)
+                    wr[j] = j == k ? -id : row[j] * id;
+            else {
+                const double f = wr[k] * id;
+
+                for (int j = 0; j < n; j++)
+                    wr[j] = j == k ? f : fma(-f, row[j], wr[j]);
             }
+        }
         __syncwarp();
     }
-    for (int c = lane; c < n; c += 32)
-        for (int i = 0; i < n; i++) {
-            if (i < c) {
-                X[i * ld + c] = 0.0;
-                continue;
-            }
-            double s = i == c ? 1.0 : 0.0;
+    double mx = 0.0;
+    bool bad = false;
 
-            for (int k = c; k < i; k++)
-                s -= W[i * ld + k] * X[k * ld + c];
-            X[i * ld + c] = s / W[i * ld + i];
-        }
-    __syncwarp();
-    for (int i = lane; i < n; i += 32)
+    for (int r = lane; r < n; r += 32)
         for (int j = 0; j < n; j++) {
-            double s = 0.0;
+            const double v = -W[r * ld + j];
 
-            for (int k = max(i, j); k < n; k++)
-                s += X[k * ld + i] * X[k * ld + j];
-            W[i * ld + j] = s;
+            W[r * ld + j] = v;
+            bad |= !(fabs(v) <= 1.0e300);
+            mx = fmax(mx, fabs(v));
         }
+#pragma unroll
+    for (int o = 16; o; o >>= 1)
+        mx = fmax(mx, __shfl_xor_sync(FULL, mx, o));
+    bad = __any_sync(FULL, bad);
     __syncwarp();
-    return true;
+    return !bad && n * mx < 1.0e8;
 }
 
 /* Pseudo-inverse of the symmetric W (double, full storage) in place, from
@@ -996,8 +1003,11 @@ tc_link_smem_kernel(TcStrip s, TcChunk c, TcLinkConst k, LinkLayout L,
             gamma = phasors_and_gamma<float>(n, ld, w, z, upper_tab, lane);
         }
         else {
-            double *X = (double *)w.A;
+            /* |T| and its inverse in w.G, the first half of the working
+               matrix's region; the second half holds the Jacobi fallback's
+               eigenvectors */
             double2 *A = (double2 *)w.A;
+            double *V = w.G + n * ld;
 
             for (int r = lane; r < n; r += 32)
                 for (int j = 0; j < n; j++) {
@@ -1006,7 +1016,7 @@ tc_link_smem_kernel(TcStrip s, TcChunk c, TcLinkConst k, LinkLayout L,
                     w.G[r * ld + j] = hypot((double)t.x, (double)t.y);
                 }
             __syncwarp();
-            if (!chol_inverse_smem(n, ld, w.G, X, lane)) {
+            if (!sweep_inverse_smem(n, ld, w.G, (double *)w.vw, lane)) {
                 __syncwarp();
                 for (int r = lane; r < n; r += 32)
                     for (int j = 0; j < n; j++) {
@@ -1015,16 +1025,33 @@ tc_link_smem_kernel(TcStrip s, TcChunk c, TcLinkConst k, LinkLayout L,
                         w.G[r * ld + j] = hypot((double)t.x, (double)t.y);
                     }
                 __syncwarp();
-                st |= TC_STATUS_EMI_PINV | jacobi_pinv(n, ld, w.G, X, w.lam, lane);
+                st |= TC_STATUS_EMI_PINV | jacobi_pinv(n, ld, w.G, V, w.lam, lane);
             }
-            for (int r = lane; r < n; r += 32)
-                for (int j = 0; j < n; j++) {
-                    const float2 t = w.T[r * ld + j];
-                    const double gg = w.G[r * ld + j];
+            /* M = |T|^-1 o T over the same region, 32 entries at a time from
+               the last one down: complex entry q covers |T|^-1 entries 2q and
+               2q + 1, which are above the block being read (or in it, read
+               before the barrier) and so already consumed */
+            const int total = n * ld;
 
-                    A[r * ld + j] = make_double2(gg * (double)t.x, gg * (double)t.y);
+            for (int base = (total - 1) & ~31; base >= 0; base -= 32) {
+                const int q = base + lane;
+                double2 v = make_double2(0.0, 0.0);
+
+                if (q < total) {
+                    const int r = q / ld, j = q - r * ld;
+
+                    if (j < n) {
+                        const float2 t = w.T[r * ld + j];
+                        const double gg = w.G[q];
+
+                        v = make_double2(gg * (double)t.x, gg * (double)t.y);
+                    }
                 }
-            __syncwarp();
+                __syncwarp();
+                if (q < total)
+                    A[q] = v;
+                __syncwarp();
+            }
             double2 z[2];
 
             st |= heig_smem<double>(n, ld, A, 0, w, lane, z);
@@ -1052,9 +1079,17 @@ LinkLayout layout_for(int n, int emi, bool regs)
     L.ld = n | 1;
     L.nv = even(n > 32 ? n : 32);
     L.off_T = 0;
-    L.off_G = even(n * L.ld);
-    L.off_A = even(L.off_G + (emi ? n * L.ld : 0));
-    L.off_vec = even(L.off_A + (regs ? 0 : (emi ? 2 : 1) * n * L.ld));
+    if (emi && !regs) {
+        /* |T| and its inverse share the working matrix's region */
+        L.off_A = even(n * L.ld);
+        L.off_G = L.off_A;
+        L.off_vec = even(L.off_A + 2 * n * L.ld);
+    }
+    else {
+        L.off_G = even(n * L.ld);
+        L.off_A = even(L.off_G + (emi ? n * L.ld : 0));
+        L.off_vec = even(L.off_A + (regs ? 0 : (emi ? 2 : 1) * n * L.ld));
+    }
     L.per_warp = even(L.off_vec + VEC_UNITS(n, L.nv));
     return L;
 }
@@ -1077,7 +1112,7 @@ cudaError_t tc_launch_link(const TcStrip &s, const TcChunk &c, const TcLinkConst
                                    pairs, phases, status, sms, st);
     const LinkLayout L = layout_for(s.n, k.emi, false);
     const size_t per_warp = (size_t)L.per_warp * sizeof(double);
-    int wpb = (int)((200 * 1024) / per_warp);
+    int wpb = (int)((227 * 1024) / per_warp);
 
     if (wpb > 8)
         wpb = 8;

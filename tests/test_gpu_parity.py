@@ -110,6 +110,7 @@ CASES = [
     (33, "ks", 0.05, "evd", False, (21, 7), 0.95),
     (64, "ad", 0.05, "evd", False, (21, 7), 0.95),
     (64, "ks", 0.05, "emi", True, (15, 5), 0.99),
+    (48, "ks", 0.05, "emi", False, (21, 7), 0.99),
 ]
 
 
