@@ -34,7 +34,7 @@ import json
 import os
 import sys
 import types
-from datetime import datetime, timezone
+from datetime import datetime
 
 import numpy as np
 

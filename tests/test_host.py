@@ -1,7 +1,6 @@
 """Host-side logic and the C-ABI library, without a GPU."""
 
 import ctypes
-import os
 import subprocess
 import sys
 

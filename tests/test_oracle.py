@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import oracle
-from conftest import GOLDEN, TOLERANCE, Case, golden_names
+from conftest import GOLDEN, TOLERANCE, Case
 
 
 @pytest.mark.parametrize("shp_fp32", [False, True])
