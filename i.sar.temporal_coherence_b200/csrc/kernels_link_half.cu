@@ -449,6 +449,12 @@ __device__ float tri_eigenvalue(int n, int index, const HWs &w, const Grp &g, fl
     int round = 0;
 
     for (; round < 20; round++) {
+        /* 1e-7 of the spectrum's scale is all that the inverse iteration
+           and the solves off the eigenvector need (the eigenvector's
+           accuracy comes from those); the smallest eigenvalues of EMI would
+           otherwise take several more rounds down to their own ulp */
+        if (hi - lo <= 1.0e-7f * norm)
+            break;
         const float xq = lo + (hi - lo) * ((float)(g.gl + 1) * (1.0f / 17.0f));
         const int cnt = sturm16(w.d, w.e2f, n, xq, pivmin);
         const unsigned gt = (__ballot_sync(g.mask, cnt > index) >> g.base) & 0xFFFFu;
@@ -478,7 +484,9 @@ __device__ float tri_eigenvalue(int n, int index, const HWs &w, const Grp &g, fl
     return 0.5f * (lo + hi);
 }
 
-__device__ __forceinline__ float rcpx(float x) { return __frcp_rn(x); }
+/* The LU's reciprocals (pivots of a shifted tridiagonal) need no correct
+   rounding: the hardware approximation, within two ulps. */
+__device__ __forceinline__ float rcpx(float x) { return __fdividef(1.0f, x); }
 
 /* Partially pivoted LU of tri - lambda I, into w.lu (written by the first
    lane of the group); returns the pivot bits. Every lane computes it. */
