@@ -146,3 +146,22 @@ def test_synthetic_stack_is_deterministic():
     bad = np.isnan(a).any(axis=0) | (a == 0).any(axis=0)
     assert 0 < bad.sum() <= 8
     assert np.all(np.isnan(a) | (a.real == np.round(a.real)))
+
+
+def test_adjoint_output_buffers_are_checked_before_the_call():
+    """adjoint_raw's caller-supplied outputs must have the gradient shapes
+    and types; a mismatch is reported before anything reaches the device."""
+    n, prow, cols, rows = 4, 12, 8, 2
+    re = np.zeros((n, prow, cols), np.float32)
+
+    class NoDevice:
+        handle = None
+
+    bad = {"grad_psi": np.zeros((n, prow, cols + 1), np.float32)}
+    with pytest.raises(ValueError, match="grad_psi"):
+        tcoh_b200.Backend.adjoint_raw(NoDevice(), re, re, None, None, None, -5, rows, rows,
+                                      cols, out=bad)
+    bad = {"grad_dh": np.zeros((prow, cols), np.float64)}
+    with pytest.raises(ValueError, match="grad_dh"):
+        tcoh_b200.Backend.adjoint_raw(NoDevice(), re, re, None, None, None, -5, rows, rows,
+                                      cols, out=bad)
