@@ -231,9 +231,16 @@ def reference_rate(slc, amp, valid, rows, cols, kw, target_s=10.0, threads=0):
     run(*crop, nrows, ccols, threads=threads, **kw)
     dt = time.perf_counter() - t
     cores = oracle.reference_threads() if kind == "reference" else (threads or os.cpu_count())
-    return {"value": nrows * ccols / dt / 1e6, "unit": "Mpixel/s", "cores": cores, "kind": kind,
-            "sample": "%d x %d output pixels of the workload (rows %d.., %.1f s)" % (
-                nrows, ccols, rows // 4, dt)}
+    out = {"value": nrows * ccols / dt / 1e6, "unit": "Mpixel/s", "cores": cores, "kind": kind,
+           "sample": "%d x %d output pixels of the workload (rows %d.., %.1f s)" % (
+               nrows, ccols, rows // 4, dt)}
+    if kind == "reference":
+        # "specialised": tcoh.cl built with this configuration's -D constants,
+        # as the reference's OpenCL backend builds it (ocl.c:222-229)
+        out["build"] = oracle.ref_build(amp.shape[2], kw["window"], ccols + 2 * hr,
+                                        kw["shp_test"], kw["alpha"], kw["estimator"],
+                                        kw["bias"], kw["min_shp"], 0, False)
+    return out
 
 
 def accuracy(slc, amp, valid, coh_gpu, count_gpu, rows, cols, kw, size=48):

@@ -64,7 +64,7 @@ struct GramSmem {
     int rows;    /* wa x 128 u32: SHP bits of each window row of each pixel */
     int pair;    /* npu x u16 */
     int expand;  /* 16 x uint2: four mask bits -> four BF16 0/1 */
-    int bar;     /* mbarrier (8 B) + TMEM address (4 B) */
+    int bar;     /* mbarrier (8 B), TMEM address (4 B), drain mbarrier (8 B) */
     int bytes;
 };
 
@@ -83,7 +83,7 @@ __host__ __device__ inline GramSmem gram_smem(int n, int wa)
     g.pair = g.rows + wa * 128 * 4;
     g.expand = g.pair + up16(tc_npu(n) * 2);
     g.bar = g.expand + 16 * 8;
-    g.bytes = g.bar + 16;
+    g.bytes = g.bar + 24;
     return g;
 }
 
@@ -143,6 +143,26 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
 
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+/* Teardown after a bounded wait ran out, by the thread that issued every MMA
+   of the CTA: a commit to a fresh mbarrier tracks the completion of all the
+   thread's earlier tcgen05 operations, whatever phase the working barriers
+   were left in, so its arrival proves that no MMA still writes the
+   accumulator. Only then may the TMEM be freed. The wait is sixteen times
+   the working one; an MMA completes in bounded time once issued, so a drain
+   that still runs out means the tensor pipe itself has stopped (bit 2 of
+   the fault flag), and the TMEM is freed all the same: a CTA that exits
+   holding it would block every later allocation on its SM. */
+__device__ __forceinline__ bool drain_mmas(uint32_t bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    mma_commit(bar);
+    for (int k = 0; k < 16; k++)
+        if (mbar_wait(bar, 0))
+            return true;
+    return false;
+}
 
 /* 16 consecutive FP32 columns of this warp's 32 TMEM lanes. */
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16])
@@ -461,10 +481,12 @@ tc_gram_tc_kernel(TcStrip s, TcChunk c, int terms, const float2 *__restrict__ sl
         fence_before();
     }
     if (!ok) {
-        if (t == 0)
+        if (t == 0) {
             atomicOr(&g_gram_fault, 1);
-        if (pending)
-            mbar_wait(bar, parity);
+            if (!drain_mmas(smem_u32(sm + L.bar + 16)))
+                atomicOr(&g_gram_fault, 2);
+        }
+        __syncthreads();
         for (int e = t; e < npu * TC_TILE_PIX; e += THREADS)
             gram[tc_gram_at(npu, (long long)tile * TC_TILE_PIX + (e & 127), e >> 7)] =
                 make_float2(__int_as_float(0x7fc00000), __int_as_float(0x7fc00000));
@@ -648,7 +670,6 @@ tc_gram_adjoint_tc_kernel(TcStrip s, TcChunk c, int halo, const float2 *__restri
     const uint32_t idesc = instr_desc(NC);
     const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + mb * 64;
     bool ok = true;
-    int issued = 0; /* rows whose MMAs were issued */
 
     for (int i = 0; i <= n && ok; i++) {
         const int b = i & 1;
@@ -707,7 +728,6 @@ tc_gram_adjoint_tc_kernel(TcStrip s, TcChunk c, int halo, const float2 *__restri
                     }
                 mma_commit(bar0 + 8 * b);
             }
-            issued = i + 1;
         }
         if (i == 0)
             continue;
@@ -749,13 +769,10 @@ tc_gram_adjoint_tc_kernel(TcStrip s, TcChunk c, int halo, const float2 *__restri
         }
         fence_before();
     }
-    if (!ok) {
-        if (t == 0)
-            atomicOr(&g_gram_fault, 1);
-        /* the MMAs issued last may still run: wait for both buffers' last
-           commits before the TMEM is freed */
-        for (int r = max(0, issued - 2); r < issued; r++)
-            mbar_wait(bar0 + 8 * (r & 1), (r >> 1) & 1);
+    if (!ok && t == 0) {
+        atomicOr(&g_gram_fault, 1);
+        if (!drain_mmas(bar0 + 24))
+            atomicOr(&g_gram_fault, 2);
     }
     __syncthreads();
     fence_after();

@@ -23,50 +23,42 @@
  * arithmetic (TC_GRAM_FP32); results are those of tc_run_device with that
  * option.
  *
- * The first call on a device resolves the array's device address with
- * cudaGetSymbolAddress (once per device, under a lock); make that first
- * call before any stream capture.
+ * Every call looks up the array's device address with cudaGetSymbolAddress
+ * on the current device, so that the address stays right when the device's
+ * context is destroyed and created again (cudaDeviceReset reloads the
+ * library's device code, and the array may move). The first call on a
+ * device also loads that device code; make it before any stream capture.
  */
 #include "../../include/tcoh_b200.h"
 #include "tcoh_internal.h"
 
 #include <math.h>
-#include <mutex>
 #include <stdio.h>
 #include <stdlib.h>
 
 #define TC_API extern "C" __attribute__((visibility("default")))
 
 #define TC_STATIC_SCRATCH_BYTES ((size_t)64 << 20)
-#define TC_STATIC_MAX_DEVICES 64
-
 static __device__ __align__(256) unsigned char tc_static_scratch[TC_STATIC_SCRATCH_BYTES];
-
-static std::mutex g_static_mu;
-static unsigned char *g_static_addr[TC_STATIC_MAX_DEVICES];
 
 /* Device address of tc_static_scratch on the current device. In host code
    the symbol's name is only a host-side stand-in, never a device address. */
-static int static_scratch(int dev, unsigned char **out)
+static int static_scratch(unsigned char **out)
 {
-    std::lock_guard<std::mutex> lock(g_static_mu);
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, tc_static_scratch);
 
-    if (!g_static_addr[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, tc_static_scratch);
-
-        if (e != cudaSuccess)
-            return tc_error(TC_ERR_CUDA, "cudaGetSymbolAddress of the static scratch: %s",
-                            cudaGetErrorString(e));
-        g_static_addr[dev] = (unsigned char *)p;
-    }
-    *out = g_static_addr[dev];
+    if (e != cudaSuccess)
+        return tc_error(TC_ERR_CUDA, "cudaGetSymbolAddress of the static scratch: %s",
+                        cudaGetErrorString(e));
+    *out = (unsigned char *)p;
     return TC_OK;
 }
 
-/* The date pairs of the packed upper triangle and of the pair planes. */
-__global__ void tc_static_tables_kernel(int n, int pairs_all, unsigned short *upper,
-                                        unsigned short *planes)
+/* The date pairs of the packed upper triangle and of the first npairs pair
+   planes (none when npairs is 0: the planes' slot then holds one entry). */
+__global__ void tc_static_tables_kernel(int n, int npairs, int pairs_all,
+                                        unsigned short *upper, unsigned short *planes)
 {
     if (threadIdx.x != 0 || blockIdx.x != 0)
         return;
@@ -76,8 +68,8 @@ __global__ void tc_static_tables_kernel(int n, int pairs_all, unsigned short *up
         for (int j = i; j < n; j++)
             upper[q++] = (unsigned short)(i << 8 | j);
     q = 0;
-    for (int i = 0; i < n - 1; i++)
-        for (int j = i + 1; j < (pairs_all ? n : i + 2); j++)
+    for (int i = 0; i < n - 1 && q < npairs; i++)
+        for (int j = i + 1; j < (pairs_all ? n : i + 2) && q < npairs; j++)
             planes[q++] = (unsigned short)(i << 8 | j);
 }
 
@@ -127,9 +119,6 @@ TC_API int tc_run_device_static(const struct settings *s, int padded_cols, const
 
     if ((e = cudaGetDevice(&dev)) != cudaSuccess)
         return tc_error(TC_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
-    if (dev < 0 || dev >= TC_STATIC_MAX_DEVICES)
-        return tc_error(TC_ERR_DEVICE, "device %d beyond the %d supported", dev,
-                        TC_STATIC_MAX_DEVICES);
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
         return tc_error(TC_ERR_CUDA, "cudaDeviceGetAttribute: %s", cudaGetErrorString(e));
     const size_t link = s->emi ? up256(tc_link_scratch_bytes(n, sms)) : 256;
@@ -152,7 +141,7 @@ TC_API int tc_run_device_static(const struct settings *s, int padded_cols, const
 
     unsigned char *base;
 
-    if ((rc = static_scratch(dev, &base)) != TC_OK)
+    if ((rc = static_scratch(&base)) != TC_OK)
         return rc;
     unsigned short *upper = (unsigned short *)base;
     unsigned short *ptab = (unsigned short *)(base + up256(sizeof(unsigned short) * tc_npu(n)));
@@ -160,7 +149,7 @@ TC_API int tc_run_device_static(const struct settings *s, int padded_cols, const
     unsigned char *sub = base + fixed + link;
     cudaStream_t st = (cudaStream_t)stream;
 
-    tc_static_tables_kernel<<<1, 32, 0, st>>>(n, s->pairs_all, upper, ptab);
+    tc_static_tables_kernel<<<1, 32, 0, st>>>(n, s->npairs, s->pairs_all, upper, ptab);
     if ((e = cudaGetLastError()) != cudaSuccess)
         return tc_error(TC_ERR_CUDA, "table kernel: %s", cudaGetErrorString(e));
 

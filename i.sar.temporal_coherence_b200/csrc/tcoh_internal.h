@@ -129,8 +129,9 @@ cudaError_t tc_launch_gram_tensor(const TcStrip &s, const TcChunk &c, int split_
                                   float2 *gram, cudaStream_t st);
 /* Tensor-core Gram for n dates and a wa x wr window on the current device. */
 bool tc_gram_tensor_supported(int n, int wa, int wr);
-/* 1 if a tensor-core Gram wait ran out since the last call (and clears it),
-   0 if not, -1 if the flag cannot be read. Synchronous. */
+/* Non-zero if a tensor-core Gram wait ran out since the last call (and
+   clears it): bit 1 a working wait, bit 2 also the teardown's drain of the
+   issued MMAs; 0 if none, -1 if the flag cannot be read. Synchronous. */
 int tc_gram_tensor_fault(void);
 /* The adjoint's scatter as the transposed tensor-core Gram (n <= 32, at most
    512 candidates in a tile's union window); faults set the flag above. */

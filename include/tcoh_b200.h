@@ -256,9 +256,11 @@ int tc_fp32_peak(int device, double *tflops);
    which every GPU that loads the library holds until exit; a strip whose
    16-row sub-strip needs more (very wide strips with many dates) gets
    TC_ERR_ARG and a message with the limit. All calls share that array:
-   calls that overlap on the GPU race. The first call on a device looks up
-   the array's address (cudaGetSymbolAddress) and should come before any
-   stream capture. The coherence matrices use plain FP32 (TC_GRAM_FP32).
+   calls that overlap on the GPU race. Every call looks up the array's
+   address (cudaGetSymbolAddress), so it stays right after a device reset;
+   the first call on a device also loads the library's device code there
+   and should come before any stream capture. The coherence matrices use
+   plain FP32 (TC_GRAM_FP32).
    No counterpart in the reference, whose ocl_open always allocates. */
 int tc_run_device_static(const struct settings *s, int padded_cols,
                          const float *slc, const float *amp,

@@ -262,12 +262,32 @@ def reference_available():
     return os.path.exists(os.path.join(HERE, "_ref", "libtcoh_ref.so"))
 
 
-def _ref_lib(pairs):
+def ref_variant_name(n, window, padded_cols, shp_test, alpha, estimator, bias, min_shp,
+                     npairs, pairs_all):
+    """File name of the reference kernel built for one configuration with its
+    -D constants (oracle/build_ref_variants.py)."""
+    return "libtcoh_ref_n%d_%dx%d_W%d_%s_a%g_%s_b%d_m%d_p%d%s.so" % (
+        n, window[0], window[1], padded_cols, shp_test, alpha, estimator, int(bias),
+        max(int(min_shp), n), npairs, "all" if pairs_all else "")
+
+
+def ref_build(n, window, padded_cols, shp_test, alpha, estimator, bias, min_shp, npairs,
+              pairs_all):
+    """"specialised" when the reference kernel built for this configuration
+    exists (it is the one run_reference then runs), else "generic"."""
+    name = ref_variant_name(n, window, padded_cols, shp_test, alpha, estimator, bias, min_shp,
+                            npairs, pairs_all)
+    return "specialised" if os.path.exists(os.path.join(HERE, "_ref", name)) else "generic"
+
+
+def _ref_lib(pairs, variant=None):
     name = "libtcoh_ref_pairs.so" if pairs else "libtcoh_ref.so"
+    if variant and os.path.exists(os.path.join(HERE, "_ref", variant)):
+        name = variant
     if name not in _ref:
         path = os.path.join(HERE, "_ref", name)
         if not os.path.exists(path):
-            raise FileNotFoundError(path + " (build with: make -C oracle)")
+            raise FileNotFoundError(path + " (build with: make -C oracle REF=<reference>)")
         lib_ = ctypes.CDLL(path)
         lib_.ref_run.restype = ctypes.c_int
         lib_.ref_run.argtypes = [ctypes.c_int] * 8 + [ctypes.c_float] * 4 + [ctypes.c_int] + [
@@ -284,7 +304,9 @@ def reference_threads():
 def run_reference(slc, amp, valid, rows, cols, window=(21, 7), shp_test="ks", alpha=0.05,
                   min_shp=20, estimator="evd", bias=False, npairs=0, pairs_all=False,
                   threads=0):
-    """The reference kernel (tcoh.cl compiled as C) over a padded strip."""
+    """The reference kernel (tcoh.cl compiled as C) over a padded strip: the
+    build specialised for this configuration (its -D constants compiled in,
+    as ocl.c:222-229 builds it) when one exists, else the generic build."""
     slc = np.ascontiguousarray(slc, np.float32)
     amp = np.ascontiguousarray(amp, np.float32)
     valid = np.ascontiguousarray(valid, np.uint8)
@@ -293,7 +315,9 @@ def run_reference(slc, amp, valid, rows, cols, window=(21, 7), shp_test="ks", al
     coh = np.empty((rows, cols), np.float32)
     count = np.empty((rows, cols), np.int32)
     pairs = np.empty((max(npairs, 1), rows, cols), np.float32)
-    rc = _ref_lib(npairs > 0).ref_run(
+    variant = ref_variant_name(n, window, pcol, shp_test, alpha, estimator, bias, min_shp,
+                               npairs, pairs_all)
+    rc = _ref_lib(npairs > 0, variant).ref_run(
         n, window[0], window[1], TESTS[shp_test], int(estimator == "emi"), int(bias),
         max(int(min_shp), n), k.ks_max, k.ad_norm, k.ad_sigma, k.ad_crit, k.tlog_crit,
         int(pairs_all), _ptr(slc), _ptr(amp), _ptr(valid), prow, pcol, rows, cols,

@@ -3,7 +3,9 @@
  * TEST INFRASTRUCTURE ONLY: the reference's own per-pixel code, run over a
  * padded strip with one OpenMP thread per row block, in place of ocl.c's
  * NDRange launch (ocl.c:329-363). The kernel constants are given here as
- * the float values that ocl.c:222-229 writes into the OpenCL build options.
+ * the float values that ocl.c:222-229 writes into the OpenCL build options;
+ * a specialised build (TCOH_REF_SPECIALISED) has them compiled in and
+ * rejects (-2) a strip or options that are not its configuration.
  */
 #include <stddef.h>
 
@@ -33,6 +35,14 @@ int ref_run(int n, int wa, int wr, int test, int emi, int bias, int min_looks,
 {
     if (padded_rows != rows + wa - 1 || padded_cols != cols + wr - 1)
         return -1;
+#ifdef TCOH_REF_SPECIALISED
+    /* built for one configuration: the strip and the options must be it */
+    if (n != N || wa != WA || wr != WR || padded_cols != W || test != SHP_TEST ||
+        emi != EMI || bias != BIAS || min_looks != MIN_LOOKS || ks_max != KS_MAX ||
+        ad_norm != AD_NORM || ad_sigma != AD_SIGMA || ad_crit != AD_CRIT ||
+        tlog_crit != TLOG_CRIT || pairs_all != PAIRS_ALL)
+        return -2;
+#endif
     ref_N = n;
     ref_WA = wa;
     ref_WR = wr;

@@ -5,10 +5,14 @@
  * TEST INFRASTRUCTURE ONLY: used by oracle/Makefile to build oracle/_ref/,
  * never by the product.
  *
- * The OpenCL build constants that ocl.c:222-229 passes with -D become
- * run-time globals (set by ref_runner.c before each run), except NPAIRS,
- * which tcoh.cl tests with #if and is therefore given on the compiler command
- * line (one library per value). <tgmath.h> keeps log, sqrt, hypot, fabs,
+ * Two builds. Generic: the OpenCL build constants that ocl.c:222-229 passes
+ * with -D become run-time globals (set by ref_runner.c before each run),
+ * except NPAIRS, which tcoh.cl tests with #if and is therefore given on the
+ * compiler command line (one library per value). Specialised
+ * (TCOH_REF_SPECIALISED, oracle/build_ref_variants.py): every constant is
+ * given with -D on the command line, exactly as ocl.c builds the kernel for
+ * one configuration, so that the compiler sees constant trip counts and
+ * fixed-size private arrays, as the OpenCL JIT does. <tgmath.h> keeps log, sqrt, hypot, fabs,
  * fmin, fmax and copysign in single precision on float arguments, as in
  * OpenCL C; the compiler is run without floating-point contraction.
  */
@@ -29,6 +33,7 @@ extern int ref_N, ref_WA, ref_WR, ref_W, ref_SHP_TEST, ref_EMI, ref_BIAS,
 extern float ref_AD_NORM, ref_AD_SIGMA, ref_AD_CRIT, ref_TLOG_CRIT;
 extern __thread int ref_gid[2];
 
+#ifndef TCOH_REF_SPECIALISED
 #define N          ref_N
 #define WA         ref_WA
 #define WR         ref_WR
@@ -43,6 +48,7 @@ extern __thread int ref_gid[2];
 #define AD_CRIT    ref_AD_CRIT
 #define TLOG_CRIT  ref_TLOG_CRIT
 #define PAIRS_ALL  ref_PAIRS_ALL
+#endif
 
 #define __kernel
 #define __global

@@ -1,9 +1,9 @@
 """Generate the golden vectors of the phase-linking path from the reference.
 
 Run in a container that has the reference checkout (it is read, never
-copied):
+copied), naming its directory:
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference PATH_TO_REFERENCE
 
 For every numeric case of the reference's own test-suite
 (tests/i_sar_temporal_coherence_test.py), this imports the reference's
@@ -120,7 +120,8 @@ def geometry_extra(geometry, geometry_model, ref, heights, h0=0.0):
 
 def main():
     parser = argparse.ArgumentParser()
-    parser.add_argument("--reference", default="/root/reference")
+    parser.add_argument("--reference", required=True,
+                        help="directory of the reference checkout (i.sar.temporal_coherence)")
     args = parser.parse_args()
     reference, conftest, geometry_model = load_reference(args.reference)
     synthetic_stack = conftest.synthetic_stack

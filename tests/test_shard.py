@@ -48,16 +48,26 @@ def rank_main(rank, world, port, name, out_dir):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("world", [2, 3, 8])
 def test_row_bands_cover_the_region(world):
-    for rows in (1, 2, 16, 30, 31, 4096):
-        if rows < world:
-            continue
+    for rows in (1, 2, 5, 16, 30, 31, 4096):
         bands = [shard.row_band(rows, world, r) for r in range(world)]
-        assert bands[0][0] == 0 and bands[-1][1] == rows
-        assert all(a[1] == b[0] for a, b in zip(bands, bands[1:]))
-        sizes = [b[1] - b[0] for b in bands]
-        assert max(sizes) - min(sizes) <= 1
+        # with more ranks than rows, the surplus ranks (the last ones) get none
+        live = [b for b in bands if b is not None]
+        assert len(live) == min(rows, world)
+        assert all(b is None for b in bands[len(live):])
+        assert live[0][0] == 0 and live[-1][1] == rows
+        assert all(a[1] == b[0] for a, b in zip(live, live[1:]))
+        sizes = [b[1] - b[0] for b in live]
+        assert min(sizes) >= 1 and max(sizes) - min(sizes) <= 1
+
+
+def test_a_rank_without_rows_has_no_strip():
+    re = np.zeros((3, 2, 4), np.float32)
+    assert shard.row_band(2, 4, 3) is None
+    assert shard.band_strip(re, re, shard.row_band(2, 4, 3), (5, 3)) is None
+    slc, amp, valid = shard.band_strip(re, re, shard.row_band(2, 4, 1), (5, 3))
+    assert valid.shape == (1 + 4, 4 + 2)
 
 
 def test_two_gloo_ranks_reassemble_the_region(tmp_path):
