@@ -40,17 +40,13 @@ sys.path.insert(0, ROOT)
 WORKLOAD = dict(n=30, rows=4096, cols=4096, window=(21, 7), shp_test="ad", alpha=0.05,
                 min_shp=20, estimator="emi", bias=True, nregions=32, g0_max=0.99, spacing=12.0)
 # The other configurations of the path, as bench lines of their own (not the
-# metric's): N=10 KS/EVD on 512 x 512; N=60 KS with six-day dates (its
-# 8192 x 16384 scene as a 2048 x 2048 proxy unless --rows / --cols).
+# metric's): N=10 KS/EVD on 512 x 512 here; the scenes of N=30 with geometry
+# and all pair coherences (4096 x 8192) and of N=60 with six-day dates
+# (8192 x 16384) in SCENES below, processed in strips.
 WORKLOADS = {
     "emi": WORKLOAD,
     "ks10": dict(n=10, rows=512, cols=512, window=(21, 7), shp_test="ks", alpha=0.05,
                  min_shp=10, estimator="evd", bias=False, nregions=8, g0_max=0.95, spacing=12.0),
-    "n60": dict(n=60, rows=2048, cols=2048, window=(21, 7), shp_test="ks", alpha=0.05,
-                min_shp=20, estimator="evd", bias=False, nregions=32, g0_max=0.99, spacing=6.0),
-    "n60emi": dict(n=60, rows=2048, cols=2048, window=(21, 7), shp_test="ks", alpha=0.05,
-                   min_shp=20, estimator="emi", bias=False, nregions=32, g0_max=0.99,
-                   spacing=6.0),
 }
 METRIC = "Mpixel/s temporal coherence at N=30, 21x7 window, <=1e-4 vs FP64"
 
@@ -78,14 +74,20 @@ def parse():
     p.add_argument("--gram", default="tensor", choices=["tensor", "fp32"],
                    help="arithmetic of the coherence matrices (the tensor cores, else plain FP32)")
     p.add_argument("--workload", default="emi",
-                   choices=["emi", "adjoint", "geometry-pairs"] + [k for k in WORKLOADS if k != "emi"],
+                   choices=["emi", "adjoint", "geometry-pairs", "n60", "n60emi"] +
+                   [k for k in WORKLOADS if k != "emi"],
                    help="emi: the metric's configuration (default); adjoint: forward + "
                         "adjoint with geometry, a height error and a phase screen, and 20 "
                         "steps of gradient ascent on the height error (2048 x 2048 unless "
                         "--rows / --cols); geometry-pairs: N=30 tlog with all pair "
                         "coherences and the phase removed on the device from orbits and an "
-                        "elevation map (1024 x 2048 unless --rows / --cols); ks10, n60, "
-                        "n60emi: the other configurations")
+                        "elevation map, 4096 x 8192 in strips of 512 rows; n60, n60emi: N=60 "
+                        "KS with EVD or EMI, 8192 x 16384 in strips of 1024 rows; ks10: "
+                        "N=10 KS/EVD on 512 x 512")
+    p.add_argument("--strip-rows", type=int, default=None,
+                   help="output rows per strip of the scene workloads")
+    p.add_argument("--accuracy-size", type=int, default=256,
+                   help="side of the centred crop checked against the FP64 oracle")
     p.add_argument("--no-extras", action="store_true",
                    help="skip the e2e, plain-FP32, CPU and accuracy legs")
     return p.parse_args()
@@ -210,78 +212,91 @@ def cpu_crop(slc, amp, valid, rows, cols, r0, nrows, ncols, ha, hr):
             np.ascontiguousarray(valid[sl, cs]))
 
 
-def reference_rate(slc, amp, valid, rows, cols, kw, target_s=10.0, threads=0):
+def reference_rate(slc, amp, valid, rows, cols, kw, target_s=10.0, threads=0, ccols=512,
+                   npairs=0, max_rows=None):
     """Mpixel/s of the reference kernel (tcoh.cl as C) on the host cores,
-    on crops of the workload sized for about target_s seconds."""
+    on a crop of ccols columns of the strip, its rows sized for about
+    target_s seconds (at most max_rows, by default half the strip)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
     ha, hr = kw["window"][0] // 2, kw["window"][1] // 2
     kind = "reference" if oracle.reference_available() else "port"
     run = oracle.run_reference if kind == "reference" else oracle.run_oracle
-    ccols = min(cols, 512)
+    extra = dict(npairs=npairs, pairs_all=True) if npairs else {}
+    ccols = min(cols, ccols)
+    max_rows = max_rows or rows // 2
     # calibration on 4 rows
-    crop = cpu_crop(slc, amp, valid, rows, cols, rows // 2, 4, ccols, ha, hr)
+    crop = cpu_crop(slc, amp, valid, rows, cols, rows // 2 if rows >= 8 else 0, 4, ccols, ha, hr)
     t = time.perf_counter()
-    run(*crop, 4, ccols, threads=threads, **kw)
+    run(*crop, 4, ccols, threads=threads, **extra, **kw)
     rate = 4 * ccols / max(time.perf_counter() - t, 1e-6)
-    nrows = int(max(4, min(rows // 2, rate * target_s / ccols)))
-    crop = cpu_crop(slc, amp, valid, rows, cols, rows // 4, nrows, ccols, ha, hr)
+    nrows = int(max(4, min(max_rows, rate * target_s / ccols)))
+    r0 = min(rows // 4, rows - nrows)
+    crop = cpu_crop(slc, amp, valid, rows, cols, r0, nrows, ccols, ha, hr)
     t = time.perf_counter()
-    run(*crop, nrows, ccols, threads=threads, **kw)
+    run(*crop, nrows, ccols, threads=threads, **extra, **kw)
     dt = time.perf_counter() - t
     cores = oracle.reference_threads() if kind == "reference" else (threads or os.cpu_count())
     out = {"value": nrows * ccols / dt / 1e6, "unit": "Mpixel/s", "cores": cores, "kind": kind,
            "sample": "%d x %d output pixels of the workload (rows %d.., %.1f s)" % (
-               nrows, ccols, rows // 4, dt)}
+               nrows, ccols, r0, dt)}
     if kind == "reference":
         # "specialised": tcoh.cl built with this configuration's -D constants,
         # as the reference's OpenCL backend builds it (ocl.c:222-229)
         out["build"] = oracle.ref_build(amp.shape[2], kw["window"], ccols + 2 * hr,
                                         kw["shp_test"], kw["alpha"], kw["estimator"],
-                                        kw["bias"], kw["min_shp"], 0, False)
+                                        kw["bias"], kw["min_shp"], npairs, bool(npairs))
     return out
 
 
-def accuracy(slc, amp, valid, coh_gpu, count_gpu, rows, cols, kw, size=48):
-    """|coh - FP64 oracle| on a centred crop (oracle with the float SHP
-    decisions, so that both use the same masks), plus SHP decision flips of
-    the float statistics against the FP64 ones."""
+def accuracy(slc, amp, valid, coh_gpu, count_gpu, rows, cols, kw, size=256, flips_size=64):
+    """crop_accuracy on a centred size x size crop of a strip."""
+    size = min(size, rows, cols)
+    ha, hr = kw["window"][0] // 2, kw["window"][1] // 2
+    r0, c0 = (rows - size) // 2, (cols - size) // 2
+    crop = cpu_crop(slc[:, c0:], amp[:, c0:], valid[:, c0:], rows, cols, r0, size, size, ha, hr)
+    return crop_accuracy(crop, coh_gpu[r0:r0 + size, c0:c0 + size],
+                         count_gpu[r0:r0 + size, c0:c0 + size], size, amp.shape[2], kw,
+                         flips_size)
+
+
+def crop_accuracy(crop, coh_gpu, count_gpu, size, n, kw, flips_size=64):
+    """|coh - FP64 oracle| on a size x size padded crop (slc, amp, valid),
+    the oracle with the float SHP decisions, so that both use the same
+    masks: the timed run's coherence (coh_gpu, count_gpu over the crop),
+    and all pair coherences, per-date phases and status bits of a run on
+    the crop; plus the SHP decision flips of the float statistics against
+    the FP64 ones on a flips_size x flips_size part of it."""
     import numpy as np
 
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-
-    ha, hr = kw["window"][0] // 2, kw["window"][1] // 2
-    r0, c0 = rows // 2, cols // 2
-    sl = slice(r0, r0 + size + 2 * ha)
-    cs = slice(c0, c0 + size + 2 * hr)
-    crop = (np.ascontiguousarray(slc[sl, cs]), np.ascontiguousarray(amp[sl, cs]),
-            np.ascontiguousarray(valid[sl, cs]))
-    o32 = oracle.run_oracle(*crop, size, size, shp_fp32=True, **kw)
-    o64 = oracle.run_oracle(*crop, size, size, shp_fp32=False, **kw)
-    g = coh_gpu[r0:r0 + size, c0:c0 + size].astype(np.float64)
-    cnt = count_gpu[r0:r0 + size, c0:c0 + size]
-    m = ~np.isnan(o32["coh"]) & ~np.isnan(g)
-    err = np.abs(g[m] - o32["coh"][m])
-    out = {
-        "pixels": int(size * size),
-        "max_abs": float(err.max()) if err.size else None,
-        "rms": float(np.sqrt(np.mean(err ** 2))) if err.size else None,
-        "count_mismatch": int((cnt != o32["count"]).sum()),
-        "null_mask_mismatch": int((np.isnan(g) != np.isnan(o32["coh"])).sum()),
-        "shp_count_flips_float_vs_fp64": int((o32["count"] != o64["count"]).sum()),
-    }
-    # The other outputs on the same crop: all pair coherences |T_ij| and the
-    # per-date phases (wrapped difference, radians).
     import tcoh_b200
 
-    n = amp.shape[2]
+    ha, hr = kw["window"][0] // 2, kw["window"][1] // 2
     s = tcoh_b200.make_settings(n, pairs=True, pairs_all=True, **kw)
     with tcoh_b200.Backend(s, size + 2 * hr) as be:
-        r = be.run(*crop, size, size, phases=True)
+        r = be.run(*crop, size, size, phases=True, status=True)
+    t = time.perf_counter()
     o = oracle.run_oracle(*crop, size, size, shp_fp32=True, npairs=s.npairs, pairs_all=True,
                           want_phases=True, **kw)
+    t_oracle = time.perf_counter() - t
+    g = coh_gpu.astype(np.float64)
+    m = ~np.isnan(o["coh"]) & ~np.isnan(g)
+    err = np.abs(g[m] - o["coh"][m])
+    out = {
+        "pixels": int(size * size), "estimated": int(m.sum()),
+        "max_abs": float(err.max()) if err.size else None,
+        "rms": float(np.sqrt(np.mean(err ** 2))) if err.size else None,
+        "over_1e-4": int((err > 1e-4).sum()),
+        "count_mismatch": int((count_gpu != o["count"]).sum()),
+        "null_mask_mismatch": int((np.isnan(g) != np.isnan(o["coh"])).sum()),
+        "crop_run_equals_timed_run": bool(np.array_equal(r["coh"], coh_gpu, equal_nan=True)),
+        "fp64_tier_fraction": float(((r["status"][m] & tcoh_b200.STATUS_FP64) != 0).mean())
+        if m.any() else None,
+        "oracle_seconds": t_oracle,
+    }
     pm = ~np.isnan(o["pairs"]) & ~np.isnan(r["pairs"])
     perr = np.abs(r["pairs"][pm].astype(np.float64) - o["pairs"][pm])
     ph = ~np.isnan(o["phases"]) & ~np.isnan(r["phases"])
@@ -292,6 +307,11 @@ def accuracy(slc, amp, valid, coh_gpu, count_gpu, rows, cols, kw, size=48):
     out["phases_rad"] = {"max_abs": float(np.abs(d).max()) if d.size else None,
                          "rms": float(np.sqrt(np.mean(d ** 2))) if d.size else None,
                          "p999": float(np.quantile(np.abs(d), 0.999)) if d.size else None}
+    fs = min(flips_size, size)
+    fc = cpu_crop(*crop, size, size, 0, fs, fs, ha, hr)
+    o64 = oracle.run_oracle(*fc, fs, fs, shp_fp32=False, **kw)
+    out["shp_count_flips_float_vs_fp64"] = {
+        "pixels": fs * fs, "flips": int((o["count"][:fs, :fs] != o64["count"]).sum())}
     return out
 
 
@@ -411,18 +431,40 @@ def adjoint_workload(args):
     print(json.dumps(line))
 
 
-def geometry_pairs_workload(args):
-    """The configuration with geometry and all pair coherences, N=30 tlog /
-    EVD, window 21x7, min_shp 20, as a 1024 x 2048 proxy of its 4096 x 8192
-    scene (unless --rows / --cols): synthetic orbits (700 km, 7.6 km/s,
-    perpendicular baselines uniform in +-150 m, C band, 12-day dates) over a
-    fractal elevation map (H = 0.8, 0 - 2000 m); the raw I/Q planes carry
-    the geometric phase at each cell's height, which tc_run_raw removes on
-    the device before the path runs, with all 435 pair-coherence planes as
-    outputs. value: device-resident planes and outputs (tc_run_raw_device);
-    e2e: page-locked host planes in, all outputs back (tc_run_raw).
-    Accuracy on a 48 x 48 crop against the FP64 oracle (oracle strip
-    preparation from the same orbits)."""
+# ---------------------------------------------------------------------------
+# Configurations 2 and 4 at their stated sizes: scenes in strips.
+
+SCENES = {
+    # N=30 tlog / EVD, all 435 pair coherences, the geometric phase removed
+    # on the device from synthetic orbits and a fractal elevation map
+    "geometry-pairs": dict(n=30, rows=4096, cols=8192, window=(21, 7), shp_test="tlog",
+                           alpha=0.05, min_shp=20, estimator="evd", bias=False, nregions=32,
+                           g0_max=0.99, spacing=12.0, pairs=True, geometry=True, strip_rows=512),
+    # N=60 six-day dates, KS, EVD and EMI
+    "n60": dict(n=60, rows=8192, cols=16384, window=(21, 7), shp_test="ks", alpha=0.05,
+                min_shp=20, estimator="evd", bias=False, nregions=32, g0_max=0.99, spacing=6.0,
+                pairs=False, geometry=False, strip_rows=1024),
+    "n60emi": dict(n=60, rows=8192, cols=16384, window=(21, 7), shp_test="ks", alpha=0.05,
+                   min_shp=20, estimator="emi", bias=False, nregions=32, g0_max=0.99,
+                   spacing=6.0, pairs=False, geometry=False, strip_rows=1024),
+}
+
+
+def scene_workload(args, name):
+    """A scene at its stated size, processed as main.c:724-825 does: strips
+    of output rows, each read with WA/2 halo rows above and below (NULL
+    outside the region), raw I/Q planes in, the strip preparation (validity,
+    sorted amplitudes and, with geometry, the phase removal) on the device.
+
+    * value: device-resident raw planes, tc_run_raw_device per strip timed
+      with CUDA events (the synthetic generation of each strip, the scene's
+      raster reading, is outside the timed region), summed over the strips;
+    * e2e: page-locked host strip buffers reused from strip to strip,
+      tc_run_raw per strip: raw rows copied in row blocks on a side stream
+      while earlier chunks compute, outputs (with all the pair planes) back
+      into reused host buffers as each chunk completes; wall clock.
+    * accuracy on a centred 256 x 256 crop against the FP64 oracle, and the
+      reference kernel on the host cores on a crop of 1024 columns."""
     import numpy as np
     import torch
 
@@ -431,126 +473,254 @@ def geometry_pairs_workload(args):
     import tcoh_b200.synthetic as syn
 
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    n, window = 30, (21, 7)
-    rows, cols = args.rows or 1024, args.cols or 2048
+    w = SCENES[name]
+    n, window = w["n"], w["window"]
+    rows, cols = args.rows or w["rows"], args.cols or w["cols"]
+    S = min(args.strip_rows or w["strip_rows"], rows)
     ha, hr = window[0] // 2, window[1] // 2
-    prow = rows + 2 * ha
-    kw = dict(window=window, shp_test="tlog", alpha=0.05, min_shp=20, estimator="evd",
-              bias=False)
+    kw = dict(window=window, shp_test=w["shp_test"], alpha=w["alpha"], min_shp=w["min_shp"],
+              estimator=w["estimator"], bias=w["bias"])
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    geo, orbits = scene.acquisition(n, rows, cols, seed=21)
-    h = scene.fbm_heights(rows, cols, hurst=0.8, hmax=2000.0, seed=22)
-    g = tcoh_b200.make_geometry(heights=h, h0=0.0, **geo)
-    grid = tcoh_b200.geometry_grid(g, orbits)
-    levels = ([g.hmin, 0.5 * (g.hmin + g.hmax), g.hmax] if grid.shape[2] == 3
-              else [0.5 * (g.hmin + g.hmax)])
-    stack = syn.generate(n, rows, cols, nregions=32, g0_max=0.99, seed=23, device=dev)
-    re = torch.full((n, prow, cols), float("nan"), dtype=torch.float32, device=dev)
-    im = torch.full_like(re, float("nan"))
-    for r0 in range(0, rows, 128):
-        r1 = min(rows, r0 + 128)
-        phi = torch.from_numpy(scene.grid_phases(grid, levels, h[r0:r1], row0=r0)).to(dev)
-        blk = stack[:, r0:r1] * torch.exp(-1j * phi).to(torch.complex64)
-        re[:, ha + r0:ha + r1] = blk.real
-        im[:, ha + r0:ha + r1] = blk.imag
-    del stack
-    elev_h = np.full((prow, cols), np.nan)
-    elev_h[ha:ha + rows] = h
-    elev = torch.from_numpy(elev_h).to(dev)
-    s = tcoh_b200.make_settings(n, pairs=True, pairs_all=True, **kw)
+    g = grid = h = levels = None
+    grid_ms = None
+    if w["geometry"]:
+        geo, orbits = scene.acquisition(n, rows, cols, seed=21)
+        h = scene.fbm_heights(rows, cols, hurst=0.8, hmax=2000.0, seed=22)
+        g = tcoh_b200.make_geometry(heights=h, h0=0.0, **geo)
+        t = time.perf_counter()
+        grid = tcoh_b200.geometry_grid(g, orbits)
+        grid_ms = (time.perf_counter() - t) * 1e3
+        levels = ([g.hmin, 0.5 * (g.hmin + g.hmax), g.hmax] if grid.shape[2] == 3
+                  else [0.5 * (g.hmin + g.hmax)])
+    s = tcoh_b200.make_settings(n, pairs=w["pairs"], pairs_all=True, **kw)
     be = tcoh_b200.Backend(s, cols + 2 * hr, device=0)
-    be.set_geometry(g, grid)
-    coh = torch.empty((rows, cols), dtype=torch.float32, device=dev)
-    count = torch.empty((rows, cols), dtype=torch.int32, device=dev)
-    pairs = torch.empty((s.npairs, rows, cols), dtype=torch.float32, device=dev)
+    if w["geometry"]:
+        be.set_geometry(g, grid)
+    strips = [(r0, min(rows, r0 + S)) for r0 in range(0, rows, S)]
+
+    def region_rows(a, b):
+        """Raw I/Q of region rows a .. b - 1 on the device (complex64), with
+        the geometric phase the acquisition carries."""
+        st = syn.generate(n, rows, cols, nregions=w["nregions"], g0_max=w["g0_max"],
+                          spacing=w["spacing"], seed=31, device=dev, row_range=(a, b))
+        if w["geometry"]:
+            for q0 in range(a, b, 128):
+                q1 = min(b, q0 + 128)
+                phi = torch.from_numpy(scene.grid_phases(grid, levels, h[q0:q1], row0=q0)).to(dev)
+                st[:, q0 - a:q1 - a] *= torch.exp(-1j * phi).to(torch.complex64)
+        return st
+
+    def strip_planes(r0, r1):
+        """re, im (N, padded rows, cols) of the strip of output rows r0 .. r1
+        - 1 on the device, NULL outside the region, and its elevation rows
+        (host, None without geometry)."""
+        prow = r1 - r0 + 2 * ha
+        a, b = max(0, r0 - ha), min(rows, r1 + ha)
+        st = region_rows(a, b)
+        re = torch.full((n, prow, cols), float("nan"), dtype=torch.float32, device=dev)
+        im = torch.full_like(re, float("nan"))
+        o = a - (r0 - ha)
+        re[:, o:o + b - a] = st.real
+        im[:, o:o + b - a] = st.imag
+        elev = None
+        if w["geometry"]:
+            elev = np.full((prow, cols), np.nan)
+            elev[o:o + b - a] = h[a:b]
+        return re, im, elev
+
+    npairs = s.npairs
+    coh = np.empty((rows, cols), np.float32)
+    count = np.empty((rows, cols), np.int32)
     stream = torch.cuda.Stream(dev)
+    d_coh = torch.empty((S, cols), dtype=torch.float32, device=dev)
+    d_count = torch.empty((S, cols), dtype=torch.int32, device=dev)
+    d_pairs = (torch.empty((npairs, S, cols), dtype=torch.float32, device=dev)
+               if npairs else None)
 
-    def step():
-        be.run_raw_device(re, im, elev, -ha, rows, rows, cols, coh, count, pairs=pairs,
-                          stream=stream)
+    def strip_on_device(r0, r1):
+        re, im, elev = strip_planes(r0, r1)
+        el = torch.from_numpy(elev).to(dev) if elev is not None else None
+        m = r1 - r0
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        be.run_raw_device(re, im, el, r0 - ha, rows, m, cols, d_coh[:m], d_count[:m],
+                          pairs=d_pairs[:, :m] if npairs and m == S else
+                          (torch.empty((npairs, m, cols), dtype=torch.float32, device=dev)
+                           if npairs else None), stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        coh[r0:r1] = d_coh[:m].cpu().numpy()
+        count[r0:r1] = d_count[:m].cpu().numpy()
+        return e0.elapsed_time(e1)
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
+    # device-resident: one untimed strip, then the scene
+    strip_on_device(*strips[len(strips) // 2])
     clocks = Clocks(0)
     clocks.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
-    e1.synchronize()
+    ms_strips = [strip_on_device(r0, r1) for r0, r1 in strips]
     ck = clocks.stop()
-    ms = e0.elapsed_time(e1) / args.steps
+    ms = float(sum(ms_strips))
     npix = rows * cols
-    line = {"metric": "Mpixel/s temporal coherence at N=30, 21x7 window, all pair coherences, "
-                      "phase removed from orbits and elevation on the device",
-            "value": npix / (ms * 1e-3) / 1e6, "unit": "Mpixel/s", "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic",
-            "config": {"workload": "N=30 %dx%d tlog/evd window 21x7, pairs=all (%d planes), "
-                                   "fBm elevation 0-2000 m, synthetic orbits" % (rows, cols,
-                                                                                   s.npairs),
-                       "api": "tc_run_raw_device"},
-            "clocks": ck}
-    if not args.no_extras:
-        def pinned(t):
-            h_ = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
-            h_.copy_(t)
-            return h_.numpy()
+    # per-stage device time on the middle strip
+    be.set_timing(True)
+    strip_on_device(*strips[len(strips) // 2])
+    stages = be.stage_stats()
+    be.set_timing(False)
+    mid = strips[len(strips) // 2]
+    cnt_mid = count[mid[0]:mid[1]]
+    lbar = float(cnt_mid[cnt_mid >= 0].mean()) if (cnt_mid >= 0).any() else 0.0
+    est = int((cnt_mid >= s.min_looks).sum())
+    f_gram, f_link = flops_per_pixel(n, lbar, w["estimator"] == "emi")
+    exact = w["estimator"] == "emi" and n > 32
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    fp32_peak = tcoh_b200.fp32_peak_tflops(0)
+    fp64_peak = tcoh_b200.fp64_peak_tflops(0)
+    bf16_peak = peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops", 1381.5))
+    valid_mid = int((cnt_mid >= 0).sum())
+    work = {
+        "shp": (shp_ops_per_pixel(n, w["shp_test"], window[0] * window[1]) * valid_mid,
+                "fp32", fp32_peak),
+        "gram": (f_gram * valid_mid, "tensor", bf16_peak),
+        # above 32 dates EMI runs the exact tier: FP64 sums and chain
+        "link": ((f_link + f_gram) * est if exact else f_link * est,
+                 "fp64" if exact else "fp32", fp64_peak if exact else fp32_peak),
+    }
+    kernels = {}
+    for k, (flops, bound, peak) in work.items():
+        t_ms, nl = stages[k]
+        if t_ms <= 0 or nl == 0:
+            continue
+        achieved = flops / (t_ms * 1e-3) / 1e12
+        kernels[k] = {"ms_middle_strip": t_ms, "launches": nl, "achieved_tflops": achieved,
+                      "bound": bound, "peak_tflops": peak, "frac": achieved / peak}
+    dom = max(kernels, key=lambda k: kernels[k]["ms_middle_strip"])
+    d = kernels[dom]
+    roofline = {"kernel": dom, "bound": d["bound"], "achieved": d["achieved_tflops"],
+                "peak": d["peak_tflops"], "unit": "TFLOP/s", "frac": d["frac"],
+                "traffic": None,
+                "peak_source": {"fp32": "measured FP32 FMA microbenchmark (tc_fp32_peak)",
+                                "fp64": "measured FP64 FMA microbenchmark (tc_fp64_peak)",
+                                "tensor": "MEASURED_PEAKS.json bf16_tflops_sustained"}[d["bound"]]}
+    line = {"metric": "Mpixel/s temporal coherence at N=%d, %dx%d window%s" % (
+                n, window[0], window[1], ", all pair coherences, phase removed from orbits "
+                "and elevation on the device" if w["geometry"] else ""),
+            "value": npix / (ms * 1e-3) / 1e6, "unit": "Mpixel/s", "n_gpus": 1, "steps": 1,
+            "warmup": 1, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "N=%d %dx%d %s/%s window %dx%d, %d regions, coherence <= "
+                                   "%.2f%s%s, strips of %d rows" % (
+                                       n, rows, cols, w["shp_test"], w["estimator"], window[0],
+                                       window[1], w["nregions"], w["g0_max"],
+                                       ", pairs=all (%d planes)" % npairs if npairs else "",
+                                       ", fBm elevation 0-2000 m, synthetic orbits"
+                                       if w["geometry"] else "", S),
+                       "api": "tc_run_raw_device per strip",
+                       "strips": len(strips),
+                       "l2": "raw strips of %.1f GB > 126 MB L2, no flush" % (
+                           n * (S + 2 * ha) * cols * 8 / 1e9)},
+            "roofline": roofline, "stages_middle_strip": kernels,
+            "mean_shp_count": lbar, "clocks": ck,
+            "mean_coherence": float(np.nanmean(coh)) if np.isfinite(coh).any() else None}
+    if grid_ms is not None:
+        line["geometry_grid_ms"] = grid_ms
+    if args.no_extras:
+        be.close()
+        print(json.dumps(line))
+        return
 
-        re_h, im_h = pinned(re), pinned(im)
-        out = {"coh": pinned(coh), "count": pinned(count), "pairs": pinned(pairs)}
-        be.run_raw(re_h, im_h, elev_h, -ha, rows, rows, cols, out=out)
+    # end to end: page-locked strip buffers reused from strip to strip
+    def pinned(shape, dtype):
+        return torch.empty(shape, dtype=dtype, pin_memory=True).numpy()
+
+    prow = S + 2 * ha
+    h_re, h_im = pinned((n, prow, cols), torch.float32), pinned((n, prow, cols), torch.float32)
+    h_el = pinned((prow, cols), torch.float64) if w["geometry"] else None
+    out = {"coh": pinned((S, cols), torch.float32), "count": pinned((S, cols), torch.int32)}
+    if npairs:
+        out["pairs"] = pinned((npairs, S, cols), torch.float32)
+    wall = 0.0
+    h2d = d2h = 0
+    for r0, r1 in strips:
+        m = r1 - r0
+        re, im, elev = strip_planes(r0, r1)
+        p = m + 2 * ha
+        full = m == S
+        tre = h_re if full else pinned((n, p, cols), torch.float32)
+        tim = h_im if full else pinned((n, p, cols), torch.float32)
+        tel = (h_el if full else pinned((p, cols), torch.float64)) if w["geometry"] else None
+        o = out if full else {"coh": pinned((m, cols), torch.float32),
+                              "count": pinned((m, cols), torch.int32),
+                              **({"pairs": pinned((npairs, m, cols), torch.float32)}
+                                 if npairs else {})}
+        tre[...] = re.cpu().numpy()
+        tim[...] = im.cpu().numpy()
+        if tel is not None:
+            tel[...] = elev
+        del re, im
         t = time.perf_counter()
-        for _ in range(3):
-            be.run_raw(re_h, im_h, elev_h, -ha, rows, rows, cols, out=out)
-        dt = (time.perf_counter() - t) / 3
-        line["e2e"] = {"value": npix / dt / 1e6, "unit": "Mpixel/s",
-                       "h2d_bytes_per_step": int(re_h.nbytes + im_h.nbytes + elev_h.nbytes),
-                       "d2h_bytes_per_step": int(sum(v.nbytes for v in out.values())),
-                       "ms_per_step": dt * 1e3, "api": "tc_run_raw (page-locked buffers)"}
-        # accuracy on a crop: oracle strip preparation from the same grid
-        import oracle
-
-        size = 48
-        r0, c0 = rows // 2, cols // 2
-        sub = dict(geo, rows=rows, cols=cols, hmin=g.hmin, hmax=g.hmax, h0=0.0)
-        re_c = re_h[:, r0:r0 + size + 2 * ha].copy()
-        im_c = im_h[:, r0:r0 + size + 2 * ha].copy()
-        el_c = elev_h[r0:r0 + size + 2 * ha].copy()
-        # padded columns of output columns c0 .. c0 + size - 1
-        cs = slice(c0, c0 + size + 2 * hr)
-        slc_c, amp_c, valid_c = oracle.prepare_strip(re_c, im_c, el_c, r0 - ha, rows, hr, sub,
-                                                     grid)
-        slc_c, amp_c, valid_c = slc_c[:, cs], amp_c[:, cs], valid_c[:, cs]
-        o = oracle.run_oracle(np.ascontiguousarray(slc_c), np.ascontiguousarray(amp_c),
-                              np.ascontiguousarray(valid_c), size, size, npairs=s.npairs,
-                              pairs_all=True, shp_fp32=True, **kw)
-        gc = out["coh"][r0:r0 + size, c0:c0 + size].astype(np.float64)
-        gp = out["pairs"][:, r0:r0 + size, c0:c0 + size].astype(np.float64)
-        m = ~np.isnan(o["coh"]) & ~np.isnan(gc)
-        pm = ~np.isnan(o["pairs"]) & ~np.isnan(gp)
-        line["accuracy"] = {
-            "pixels": size * size,
-            "max_abs": float(np.abs(gc[m] - o["coh"][m]).max()) if m.any() else None,
-            "count_mismatch": int((out["count"][r0:r0 + size, c0:c0 + size] != o["count"]).sum()),
-            "null_mask_mismatch": int((np.isnan(gc) != np.isnan(o["coh"])).sum()),
-            "pairs_max_abs": float(np.abs(gp[pm] - o["pairs"][pm]).max()) if pm.any() else None}
-        line["mean_coherence"] = float(np.nanmean(out["coh"]))
+        be.run_raw(tre, tim, tel, r0 - ha, rows, m, cols, out=o)
+        wall += time.perf_counter() - t
+        h2d += tre.nbytes + tim.nbytes + (tel.nbytes if tel is not None else 0)
+        d2h += sum(v.nbytes for v in o.values())
+        assert np.array_equal(o["count"], count[r0:r1])
+    line["e2e"] = {"value": npix / wall / 1e6, "unit": "Mpixel/s", "h2d_bytes_per_step": int(h2d),
+                   "d2h_bytes_per_step": int(d2h), "ms_per_step": wall * 1e3,
+                   "api": "tc_run_raw per strip (page-locked strip buffers, reused)"}
     be.close()
-    print(json.dumps(line))
 
+    # accuracy on a centred crop, and the reference kernel on the host cores
+    import oracle
+
+    def prepared(r0, nr, c0, nc):
+        """Padded strip (slc, amp, valid) of output rows r0 .. r0 + nr - 1
+        and columns c0 .. c0 + nc - 1 of the scene, as main.c reads it."""
+        st = region_rows(max(0, r0 - ha), min(rows, r0 + nr + ha)).cpu().numpy()
+        if w["geometry"]:
+            pr = nr + 2 * ha
+            re_c = np.full((n, pr, cols), np.nan, np.float32)
+            im_c = re_c.copy()
+            el_c = np.full((pr, cols), np.nan)
+            o = max(0, r0 - ha) - (r0 - ha)
+            re_c[:, o:o + st.shape[1]] = st.real
+            im_c[:, o:o + st.shape[1]] = st.imag
+            el_c[o:o + st.shape[1]] = h[max(0, r0 - ha):min(rows, r0 + nr + ha)]
+            sg = dict(geo, hmin=g.hmin, hmax=g.hmax, h0=0.0)
+            full = oracle.prepare_strip(re_c, im_c, el_c, r0 - ha, rows, hr, sg, grid)
+            cs = slice(c0, c0 + nc + 2 * hr)
+            return tuple(np.ascontiguousarray(x[:, cs]) for x in full)
+        # interior crops: the halo rows and columns are pixels of the scene
+        assert r0 >= ha and r0 + nr + ha <= rows and c0 >= hr and c0 + nc + hr <= cols
+        st = st[:, :, c0 - hr:c0 + nc + hr]
+        return tcoh_b200.read_strip(np.ascontiguousarray(st.real), np.ascontiguousarray(st.imag),
+                                    0, nr + 2 * ha, 0)
+
+    size = min(args.accuracy_size, rows - 2 * ha, cols - 2 * hr)
+    r0, c0 = (rows - size) // 2, (cols - size) // 2
+    crop = prepared(r0, size, c0, size)
+    line["accuracy"] = crop_accuracy(crop, coh[r0:r0 + size, c0:c0 + size],
+                                     count[r0:r0 + size, c0:c0 + size], size, n, kw)
+    # a 1024 x 1024 crop at 60 dates; 512 columns with the pair planes
+    ccols = min(512 if npairs else 1024, cols - 2 * hr)
+    nrows = min(1024, rows - 2 * ha)
+    cr0, cc0 = (rows - nrows) // 2, (cols - ccols) // 2
+    cpu = prepared(cr0, nrows, cc0, ccols)
+    line["cpu_baseline"] = reference_rate(*cpu, nrows, ccols, kw, target_s=30.0, ccols=ccols,
+                                          npairs=npairs, max_rows=nrows)
+    print(json.dumps(line))
 
 def main():
     args = parse()
     if args.workload == "adjoint" and args.impl != "reference":
         return adjoint_workload(args)
-    if args.workload == "geometry-pairs" and args.impl != "reference":
-        return geometry_pairs_workload(args)
-    if args.workload in ("adjoint", "geometry-pairs"):
+    if args.workload in SCENES and args.impl != "reference":
+        return scene_workload(args, args.workload)
+    if args.workload == "adjoint" or args.workload in SCENES:
         print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the "
                           "metric's configuration (--workload emi)"}))
         return
@@ -763,7 +933,8 @@ def main():
                        "ms_per_step": dt * 1e3, "api": "tc_run_ex (the ocl_run path)"}
         # CPU baseline and accuracy on crops.
         line["cpu_baseline"] = reference_rate(sn, an, vn, rows, cols, kw, target_s=12.0)
-        line["accuracy"] = accuracy(sn, an, vn, coh_h, cnt, rows, cols, kw)
+        line["accuracy"] = accuracy(sn, an, vn, coh_h, cnt, rows, cols, kw,
+                                    size=args.accuracy_size)
     be.close()
     if rank == 0:
         print(json.dumps(line))

@@ -29,7 +29,7 @@ LIBRARY = os.path.join(HERE, "libtcoh_b200.so")
 
 SHP_TESTS = {"ks": 0, "ad": 1, "tlog": 2}
 GRAM_TENSOR, GRAM_FP32 = 0, 1
-STATUS_EMI_PINV, STATUS_UNLINKED, STATUS_ITER_CAP = 1, 2, 4
+STATUS_EMI_PINV, STATUS_UNLINKED, STATUS_ITER_CAP, STATUS_FP64 = 1, 2, 4, 8
 STAGES = ("prep", "shp", "gram", "link", "copy", "adjoint")
 
 # Exported symbols of include/tcoh_b200.h.
@@ -37,7 +37,7 @@ EXPORTS = (
     "ocl_list_devices", "ocl_open", "ocl_run", "ocl_close",
     "tc_last_error", "tc_set_fatal_handler", "tc_shp_constants", "tc_device_count",
     "tc_open", "tc_run_ex", "tc_run_device", "tc_set_timing", "tc_stage_stats",
-    "tc_close", "tc_fp32_peak", "tc_run_device_static", "tc_get_options",
+    "tc_close", "tc_fp32_peak", "tc_fp64_peak", "tc_run_device_static", "tc_get_options",
     "tc_geometry_grid_shape", "tc_geometry_init", "tc_set_geometry", "tc_run_raw",
     "tc_run_raw_device", "tc_adjoint_raw",
 )
@@ -173,6 +173,7 @@ def library():
         lib.tc_run_raw_device.argtypes = [vp, vp, vp, vp, i, i, i, i, i, vp, vp, vp, vp, vp, vp]
         lib.tc_adjoint_raw.argtypes = [vp, vp, vp, vp, vp, vp, i, i, i, i, i, vp, vp, vp, vp]
         lib.tc_fp32_peak.argtypes = [i, ctypes.POINTER(ctypes.c_double)]
+        lib.tc_fp64_peak.argtypes = [i, ctypes.POINTER(ctypes.c_double)]
         lib.tc_run_device_static.argtypes = [ctypes.POINTER(Settings), i, vp, vp, vp, i, i, i,
                                              vp, vp, vp, vp, vp, vp]
         lib.ocl_open.restype = vp
@@ -240,6 +241,13 @@ def fp32_peak_tflops(device=0):
     """Measured FP32 FMA throughput (TFLOP/s) of the device."""
     v = ctypes.c_double(0.0)
     _check(library().tc_fp32_peak(device, ctypes.byref(v)))
+    return v.value
+
+
+def fp64_peak_tflops(device=0):
+    """Measured FP64 FMA throughput (TFLOP/s) of the device."""
+    v = ctypes.c_double(0.0)
+    _check(library().tc_fp64_peak(device, ctypes.byref(v)))
     return v.value
 
 

@@ -236,13 +236,19 @@ struct ocl {
     cudaStream_t out_stream;  /* device -> host copies of the outputs, by chunks */
     std::vector<cudaEvent_t> chunk_done;
     DevBuf slc, amp, valid, coh, count, pairs, phases, status;
-    DevBuf soa, logstat, mask, gram, upper_tab, pair_tab, link_scratch;
+    DevBuf soa, logstat, mask, gram, upper_tab, pair_tab, link_scratch, exact_list;
     DevBuf raw_re, raw_im, raw_elev, geo_grid, adj_dh, adj_psi, adj_gbar, adj_dtheta, adj_gdh;
     bool has_geo;
     TcGeo geo;
     bool timing;
     float stage_ms[ST_COUNT];
     int stage_launches[ST_COUNT];
+    /* Host-side fault injection for tests of the error paths: with the
+       environment variable TCOH_FAIL_AT_CHUNK=k when the context opens,
+       every run fails before launching its chunk k (0-based), as a CUDA
+       error would, without touching the GPU: tc_run_* return TC_ERR_CUDA
+       and ocl_run calls the fatal handler (ocl.c:44-48). -1: off. */
+    int fail_chunk;
 };
 
 static int check_settings(const struct settings *s, int padded_cols)
@@ -306,7 +312,8 @@ static void free_bufs(struct ocl *o)
 {
     DevBuf *b[] = {&o->slc, &o->amp, &o->valid, &o->coh, &o->count, &o->pairs,
                    &o->phases, &o->status, &o->soa, &o->logstat, &o->mask, &o->gram,
-                   &o->upper_tab, &o->pair_tab, &o->link_scratch, &o->raw_re, &o->raw_im,
+                   &o->upper_tab, &o->pair_tab, &o->link_scratch, &o->exact_list,
+                   &o->raw_re, &o->raw_im,
                    &o->raw_elev, &o->geo_grid, &o->adj_dh, &o->adj_psi, &o->adj_gbar,
                    &o->adj_dtheta, &o->adj_gdh};
 
@@ -389,6 +396,11 @@ TC_API int tc_open(int device, const struct settings *s, int padded_cols,
     o->gram_block = tc_gram_block_for(o->n);
     o->timing = false;
     o->has_geo = false;
+    {
+        const char *env = getenv("TCOH_FAIL_AT_CHUNK");
+
+        o->fail_chunk = env && *env ? atoi(env) : -1;
+    }
     memset(o->stage_ms, 0, sizeof(o->stage_ms));
     memset(o->stage_launches, 0, sizeof(o->stage_launches));
 
@@ -629,6 +641,8 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
     CK(ensure(o->mask, sizeof(uint32_t) * s.mask_words * max_npix));
     CK(ensure(o->gram, sizeof(float2) * tc_npu(o->n) * max_npix));
     CK(ensure(o->link_scratch, tc_link_scratch_bytes(o->n, o->sms)));
+    if (o->emi)
+        CK(ensure(o->exact_list, sizeof(int) * (max_npix + 1)));
     if (o->opt.gram == TC_GRAM_FP32)
         CK(ensure(o->soa, sizeof(float2) * s.planes * s.npad));
     if (o->test == SHP_TLOG)
@@ -666,8 +680,12 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
             o->chunk_done.push_back(ev);
         }
     }
-    for (int row0 = 0; row0 < rows; row0 += crows) {
+    for (int row0 = 0, chunk = 0; row0 < rows; row0 += crows, chunk++) {
         TcChunk c;
+
+        if (chunk == o->fail_chunk)
+            return set_error(TC_ERR_CUDA, "injected failure before chunk %d "
+                             "(TCOH_FAIL_AT_CHUNK)", chunk);
 
         c.row0 = row0;
         c.nrows = rows - row0 < crows ? rows - row0 : crows;
@@ -687,17 +705,20 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
         CK(tc_launch_shp(s, c, o->shp, amp, valid, (const float2 *)o->logstat.p,
                          (uint32_t *)o->mask.p, count, o->sms, st));
         tm.end(t);
-        t = tm.begin(ST_GRAM);
-        if (o->opt.gram == TC_GRAM_FP32)
-            CK(tc_launch_gram_fp32(s, c, o->gram_block, (const float2 *)o->soa.p,
-                                   (const uint32_t *)o->mask.p, (float2 *)o->gram.p, st));
-        else
-            CK(tc_launch_gram_tensor(s, c, o->opt.split_terms, slc, (const uint32_t *)o->mask.p,
-                                     (float2 *)o->gram.p, st));
-        tm.end(t);
+        if (adj || tc_link_needs_gram(o->n, o->emi)) {
+            t = tm.begin(ST_GRAM);
+            if (o->opt.gram == TC_GRAM_FP32)
+                CK(tc_launch_gram_fp32(s, c, o->gram_block, (const float2 *)o->soa.p,
+                                       (const uint32_t *)o->mask.p, (float2 *)o->gram.p, st));
+            else
+                CK(tc_launch_gram_tensor(s, c, o->opt.split_terms, slc,
+                                         (const uint32_t *)o->mask.p, (float2 *)o->gram.p, st));
+            tm.end(t);
+        }
         t = tm.begin(ST_LINK);
         if (!adj)
-            CK(tc_launch_link(s, c, lk, (const float2 *)o->gram.p, count,
+            CK(tc_launch_link(s, c, lk, (const float2 *)o->gram.p, slc,
+                              (const uint32_t *)o->mask.p, count, (int *)o->exact_list.p,
                               (const unsigned short *)o->upper_tab.p,
                               (const unsigned short *)o->pair_tab.p,
                               (double *)o->link_scratch.p, coh, pairs, phases, status, o->sms,
@@ -948,12 +969,22 @@ TC_API int tc_set_geometry(struct ocl *o, const struct tc_geometry *g, const dou
         return rc;
     if (d.ndates != o->n)
         return set_error(TC_ERR_ARG, "geometry of %d dates for a context of %d", d.ndates, o->n);
-    const size_t bytes = (size_t)d.grid_rows * d.grid_cols * d.nheights * d.ndates * sizeof(double);
+    const size_t nodes = (size_t)d.grid_rows * d.grid_cols * d.ndates;
+    const size_t bytes = nodes * d.nheights * sizeof(double);
+    DevBuf raw;
 
+    /* the grid as given, then its coefficient form (TcGridCell) */
     CK(cudaSetDevice(o->device));
-    CK(ensure(o->geo_grid, bytes));
-    CK(cudaMemcpyAsync(o->geo_grid.p, grid, bytes, cudaMemcpyHostToDevice, o->stream));
-    CK(cudaStreamSynchronize(o->stream));
+    CK(ensure(o->geo_grid, nodes * 3 * sizeof(double)));
+    CK(ensure(raw, bytes));
+    cudaError_t e = cudaMemcpyAsync(raw.p, grid, bytes, cudaMemcpyHostToDevice, o->stream);
+
+    if (e == cudaSuccess)
+        e = tc_launch_geometry_coef(d, (const double *)raw.p, (double *)o->geo_grid.p, o->stream);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(o->stream);
+    cudaFree(raw.p);
+    CK(e);
     o->geo = d;
     o->has_geo = true;
     return TC_OK;
@@ -991,7 +1022,8 @@ static int prepare_raw(struct ocl *o, const float *re, const float *im, const do
     const int t = tm.begin(ST_PREP);
 
     CK(tc_launch_prep_raw(o->n, re, im, elev, row0, region_rows, padded_rows, cols, o->wr / 2,
-                          o->has_geo ? &o->geo : nullptr, (const double *)o->geo_grid.p, dh, psi,
+                          0, padded_rows, o->has_geo ? &o->geo : nullptr,
+                          (const double *)o->geo_grid.p, dh, psi,
                           (float *)o->slc.p, (float *)o->amp.p, (unsigned char *)o->valid.p,
                           st));
     tm.end(t);
@@ -1010,7 +1042,8 @@ TC_API int tc_run_raw(struct ocl *o, const float *re, const float *im, const dou
     CK(cudaSetDevice(o->device));
     const size_t plane = (size_t)padded_rows * cols;
     const size_t n = o->n;
-    cudaStream_t st = o->stream;
+    const size_t npad = (size_t)padded_rows * o->padded_cols;
+    cudaStream_t st = o->stream, cs = o->copy_stream;
     Timer tm(o, st);
 
     memset(o->stage_ms, 0, sizeof(o->stage_ms));
@@ -1019,22 +1052,49 @@ TC_API int tc_run_raw(struct ocl *o, const float *re, const float *im, const dou
     CK(ensure(o->raw_im, n * plane * sizeof(float)));
     if (elevation)
         CK(ensure(o->raw_elev, plane * sizeof(double)));
+    CK(ensure(o->slc, npad * n * 2 * sizeof(float)));
+    CK(ensure(o->amp, npad * n * sizeof(float)));
+    CK(ensure(o->valid, npad));
     if ((rc = ensure_outputs(o, (size_t)rows * cols, phases != nullptr, status != nullptr)) !=
         TC_OK)
         return rc;
-    const int t = tm.begin(ST_COPY);
+    /* The raw rows go over in row blocks on the copy stream (one strided
+       copy per block for all the date planes), each block prepared there
+       as soon as its rows have arrived, and each chunk of the path waits
+       only for the blocks that hold its rows: the copies and the
+       preparation overlap the path (and are not timed as stages here). */
+    const int block_rows = (padded_rows + TC_COPY_BLOCKS - 1) / TC_COPY_BLOCKS;
+    RowsReady ready;
 
-    CK(cudaMemcpyAsync(o->raw_re.p, re, n * plane * sizeof(float), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(o->raw_im.p, im, n * plane * sizeof(float), cudaMemcpyHostToDevice, st));
-    if (elevation)
-        CK(cudaMemcpyAsync(o->raw_elev.p, elevation, plane * sizeof(double),
-                           cudaMemcpyHostToDevice, st));
-    tm.end(t);
-    if ((rc = prepare_raw(o, (const float *)o->raw_re.p, (const float *)o->raw_im.p,
-                          elevation ? (const double *)o->raw_elev.p : nullptr, row0, region_rows,
-                          padded_rows, cols, st, tm)) != TC_OK)
-        return rc;
-    return run_context_buffers(o, padded_rows, rows, cols, coh, count, pairs, phases, status, tm);
+    ready.block_rows = block_rows;
+    ready.nblocks = (padded_rows + block_rows - 1) / block_rows;
+    ready.done = o->block_done;
+    /* work already queued on the context's stream may still read the
+       buffers */
+    CK(cudaEventRecord(o->block_done[0], st));
+    CK(cudaStreamWaitEvent(cs, o->block_done[0], 0));
+    for (int b = 0; b < ready.nblocks; b++) {
+        const int r0 = b * block_rows;
+        const int nr = b + 1 < ready.nblocks ? block_rows : padded_rows - r0;
+        const size_t at = (size_t)r0 * cols, bytes = (size_t)nr * cols * sizeof(float);
+
+        CK(cudaMemcpy2DAsync((float *)o->raw_re.p + at, plane * sizeof(float), re + at,
+                             plane * sizeof(float), bytes, n, cudaMemcpyHostToDevice, cs));
+        CK(cudaMemcpy2DAsync((float *)o->raw_im.p + at, plane * sizeof(float), im + at,
+                             plane * sizeof(float), bytes, n, cudaMemcpyHostToDevice, cs));
+        if (elevation)
+            CK(cudaMemcpyAsync((double *)o->raw_elev.p + at, elevation + at,
+                               (size_t)nr * cols * sizeof(double), cudaMemcpyHostToDevice, cs));
+        CK(tc_launch_prep_raw(o->n, (const float *)o->raw_re.p, (const float *)o->raw_im.p,
+                              elevation ? (const double *)o->raw_elev.p : nullptr, row0,
+                              region_rows, padded_rows, cols, o->wr / 2, r0, r0 + nr,
+                              o->has_geo ? &o->geo : nullptr, (const double *)o->geo_grid.p,
+                              nullptr, nullptr, (float *)o->slc.p, (float *)o->amp.p,
+                              (unsigned char *)o->valid.p, cs));
+        CK(cudaEventRecord(o->block_done[b], cs));
+    }
+    return run_context_buffers(o, padded_rows, rows, cols, coh, count, pairs, phases, status, tm,
+                               &ready);
 }
 
 TC_API int tc_run_raw_device(struct ocl *o, const float *re, const float *im,

@@ -18,8 +18,8 @@
  * dL/dtheta (atomically: a candidate lies in the windows of several tiles).
  *
  * dL/dpsi_q,k = dL/dtheta_q,k; dL/ddh_q = sum_k dL/dtheta_q,k dphi_k/dh at the
- * cell's height (the derivative of the quadratic interpolation in height of
- * geometry.c:273-281; zero with a single height level).
+ * cell's height (the derivative of the quadratic in height of the grid's
+ * coefficient form, TcGridCell; zero with a single height level).
  */
 #include "tcoh_internal.h"
 
@@ -148,7 +148,8 @@ tc_adjoint_scatter_kernel(TcStrip s, TcChunk c, int halo, const float2 *__restri
     }
 }
 
-/* dL/ddh from dL/dtheta (grad_psi) and the grid's height derivative. */
+/* dL/ddh from dL/dtheta (grad_psi) and the height derivative of the phase
+   grid (coefficient form). */
 __global__ void tc_adjoint_height_kernel(int n, int padded_rows, int cols, int row0,
                                          int region_rows, const double *__restrict__ elev,
                                          const double *__restrict__ dh, TcGeo g,
@@ -165,28 +166,14 @@ __global__ void tc_adjoint_height_kernel(int n, int padded_rows, int cols, int r
 
     if (grid && g.nheights == 3 && row >= 0 && row < region_rows) {
         const double h = (elev ? elev[cell] : g.h0) + (dh ? dh[cell] : 0.0);
-        const double *x = g.heights;
-        const double dw[3] = {((h - x[1]) + (h - x[2])) / ((x[0] - x[1]) * (x[0] - x[2])),
-                              ((h - x[0]) + (h - x[2])) / ((x[1] - x[0]) * (x[1] - x[2])),
-                              ((h - x[0]) + (h - x[1])) / ((x[2] - x[0]) * (x[2] - x[1]))};
-        const int gr = row / 16, gc = col / 16;
-        const double fr = (double)(row - gr * 16) / 16, fc = (double)(col - gc * 16) / 16;
-        const size_t stride = (size_t)3 * n;
+        const TcGridCell gc = tc_grid_cell(g, grid, row, col, h);
         const size_t plane = (size_t)padded_rows * cols;
         double acc = 0.0;
 
         for (int k = 0; k < n; k++) {
-            double d = 0.0;
+            double d;
 
-            for (int hl = 0; hl < 3; hl++) {
-                const double *p00 = grid + (((size_t)gr * g.grid_cols + gc) * 3 + hl) * n;
-                const double *p01 = p00 + stride;
-                const double *p10 = p00 + (size_t)g.grid_cols * stride;
-                const double *p11 = p10 + stride;
-
-                d += dw[hl] * ((1.0 - fr) * ((1.0 - fc) * p00[k] + fc * p01[k]) +
-                               fr * ((1.0 - fc) * p10[k] + fc * p11[k]));
-            }
+            gc.phase(k, &d);
             acc += d * dtheta[k * plane + cell];
         }
         out = (float)acc;

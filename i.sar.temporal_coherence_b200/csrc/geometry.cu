@@ -1,17 +1,35 @@
 /* Flat-earth / topographic phase and the strip preparation, on the device.
  *
- * Phase grid (geometry.c:161-254): for every node of a grid every 16 lines
- * and samples of the region, and every height level (one, or hmin, mid,
- * hmax), the ground point seen by the reference date is located on the
- * WGS84 ellipsoid raised by the height (Newton on the range-Doppler
- * equations, geometry.c:100-148), then every date's zero-Doppler time of
- * that point is found by Newton from its closest state vector
- * (geometry.c:33-71), orbits being interpolated by 8-point Lagrange
- * polynomials (orbit.c:324-346); the phase of date k is
- * 4 pi / lambda (R_k - R_ref). All FP64, one thread per grid node (its
- * height levels in turn, each starting from the previous level's point as
- * the reference does). The grid is small (a few thousand nodes for a large
- * region) and computed once per run.
+ * Phase grid (what geometry.c:161-254 computes): for every node of a grid
+ * every 16 lines and samples of the region and every height level (one, or
+ * hmin, mid, hmax), the ground point that the reference date sees at the
+ * node's azimuth time and slant range on the WGS84 ellipsoid raised by the
+ * height, then every date's slant range to that point at its own
+ * zero-Doppler time; the phase of date k is 4 pi / lambda (R_k - R_ref).
+ * All in double precision, one warp per grid node:
+ *
+ * - orbits: each date's state vectors, interpolated by the polynomial of
+ *   degree 7 through the 8 vectors around the time (the window of
+ *   orbit.c:326-346), evaluated by Neville's scheme on the offsets from
+ *   the window's middle vector, with the time derivative of the velocity;
+ * - ground point (lanes 0 .. nheights - 1, one height level each): in the
+ *   zero-Doppler plane of the reference orbit the point is
+ *   s + R (cos a e1 + sin a e2), e1 pointing down, e2 to the right of the
+ *   track, so that the Doppler and range equations hold by construction;
+ *   the look angle a solves the ellipsoid equation by Newton's method from
+ *   the law-of-cosines angle of a spherical Earth of the local radius;
+ * - zero-Doppler times (the lanes over height levels x dates): the root of
+ *   f(t) = v(t) . (p - s(t)) lies between the state vector nearest to p and
+ *   its neighbour across the sign change of f; Newton's method from the
+ *   secant point of that bracket, with f'(t) = v'(t) . (p - s(t)) - |v(t)|^2,
+ *   converges quadratically. A point whose root is not bracketed inside the
+ *   orbit is outside its coverage (the reference's fatal error).
+ *
+ * The grid is small (a few thousand nodes for a large region) and computed
+ * once per run. For the strip preparation it is turned into coefficient
+ * form (tc_launch_geometry_coef): per node and date the quadratic in height
+ * through the three levels, so that a cell's phase is one bilinear blend of
+ * three coefficients and a Horner step (TcGridCell).
  *
  * Strip preparation (main.c:52-127), one thread per padded-strip cell, from
  * raw I/Q planes of the strip's rows: a cell is valid when it lies in the
@@ -20,9 +38,8 @@
  * are rounded exactly as the reference's C (no contraction) and sorted
  * ascending (a bitonic network in registers; any correct sort gives the
  * same floats); with a geometry, date k is rotated by exp(i phase_k) in
- * double, phase_k interpolated from the grid bilinearly in line and sample
- * and quadratically in height (geometry.c:256-291), and rounded to float.
- * Invalid cells are zero.
+ * double, phase_k interpolated from the grid at the cell's line, sample and
+ * height, and rounded to float. Invalid cells are zero.
  */
 #include "tcoh_internal.h"
 
@@ -31,202 +48,297 @@
 
 namespace {
 
-constexpr int GEO_STEP = 16;
-constexpr int LAGRANGE = 8;
+constexpr int LAGRANGE = 8;       /* state vectors per interpolation window */
+constexpr int GRID_WARPS = 4;     /* grid nodes per CTA */
 constexpr double SPEED_OF_LIGHT = 299792458.0;
 constexpr double WGS84_A = 6378137.0;
 constexpr double WGS84_B = 6356752.314245;
+constexpr unsigned FULL = 0xffffffffu;
 
 __device__ int g_geo_fault;
 
-__device__ __forceinline__ double dot3(const double *a, const double *b)
-{
-    return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
-}
-
-struct DevOrbit {
-    int n;
-    const double *t, *pos, *vel;
+struct V3 {
+    double x, y, z;
 };
 
-__device__ DevOrbit dev_orbit(const TcOrbitSet &o, int k)
+__host__ __device__ __forceinline__ V3 v3(double x, double y, double z) { return {x, y, z}; }
+__host__ __device__ __forceinline__ V3 operator+(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__host__ __device__ __forceinline__ V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__host__ __device__ __forceinline__ V3 operator*(double k, V3 a) { return v3(k * a.x, k * a.y, k * a.z); }
+__host__ __device__ __forceinline__ double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__host__ __device__ __forceinline__ V3 cross(V3 a, V3 b)
 {
-    DevOrbit d;
+    return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__host__ __device__ __forceinline__ V3 unit(V3 a) { return (1.0 / sqrt(dot(a, a))) * a; }
+
+/* One date's orbit: nsv state vectors, times increasing. */
+struct Orbit {
+    int nsv;
+    const double *t, *pos, *vel; /* [nsv], [nsv][3], [nsv][3] */
+};
+
+__host__ __device__ __forceinline__ Orbit orbit_of(const TcOrbitSet &o, int k)
+{
     const int off = o.offset[k];
 
-    d.n = o.count[k];
-    d.t = o.t + off;
-    d.pos = o.pos + 3 * off;
-    d.vel = o.vel + 3 * off;
-    return d;
+    return {o.count[k], o.t + off, o.pos + 3 * off, o.vel + 3 * off};
 }
 
-__device__ void orbit_state(const DevOrbit &o, double t, double *pos, double *vel)
+__host__ __device__ __forceinline__ V3 row3(const double *a, int i)
 {
-    int first = 0;
+    return v3(a[3 * i], a[3 * i + 1], a[3 * i + 2]);
+}
 
-    while (first + LAGRANGE < o.n && o.t[first + LAGRANGE / 2] < t)
-        first++;
-    for (int k = 0; k < 3; k++)
-        pos[k] = vel[k] = 0.0;
-    for (int i = first; i < first + LAGRANGE; i++) {
-        double w = 1.0;
+struct State {
+    V3 pos, vel, acc; /* acc: time derivative of the interpolated velocity */
+};
 
-        for (int j = first; j < first + LAGRANGE; j++)
-            if (j != i)
-                w *= (t - o.t[j]) / (o.t[i] - o.t[j]);
-        for (int k = 0; k < 3; k++) {
-            pos[k] += w * o.pos[3 * i + k];
-            vel[k] += w * o.vel[3 * i + k];
+/* First state vector of the interpolation window at time tt: LAGRANGE / 2
+   vectors before the first one at or after tt, kept inside the orbit. */
+__host__ __device__ int window_start(const Orbit &o, double tt)
+{
+    int lo = 0, hi = o.nsv;
+
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+
+        if (o.t[mid] < tt)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    const int f = lo - LAGRANGE / 2;
+
+    return f < 0 ? 0 : (f > o.nsv - LAGRANGE ? o.nsv - LAGRANGE : f);
+}
+
+/* Neville's scheme on the window's 8 points (times dt[i] relative to the
+   evaluation time) for the values y, and the derivative when d is set. */
+__host__ __device__ __forceinline__ double neville(const double (&dt)[LAGRANGE], double (&y)[LAGRANGE],
+                                          double *d)
+{
+    double dy[LAGRANGE];
+
+#pragma unroll
+    for (int i = 0; i < LAGRANGE; i++)
+        dy[i] = 0.0;
+#pragma unroll
+    for (int m = 1; m < LAGRANGE; m++)
+#pragma unroll
+        for (int i = 0; i + m < LAGRANGE; i++) {
+            /* P_i,i+m(t) = ((t - t_i+m) P_i,i+m-1 + (t_i - t) P_i+1,i+m) / (t_i - t_i+m) */
+            const double r = 1.0 / (dt[i] - dt[i + m]);
+
+            if (d)
+                dy[i] = (y[i] - y[i + 1] - dt[i + m] * dy[i] + dt[i] * dy[i + 1]) * r;
+            y[i] = (dt[i] * y[i + 1] - dt[i + m] * y[i]) * r;
         }
-    }
+    if (d)
+        *d = dy[0];
+    return y[0];
 }
 
-/* false when the time falls outside the orbit */
-__device__ bool zero_doppler(const DevOrbit &o, const double *p, double &tz)
+__host__ __device__ State orbit_state(const Orbit &o, double tt)
 {
-    double t = o.t[0], best = -1.0;
+    const int f = window_start(o, tt), c = f + LAGRANGE / 2;
+    double dt[LAGRANGE], y[LAGRANGE], out[6], der[3] = {0.0, 0.0, 0.0};
 
-    for (int i = 0; i < o.n; i++) {
-        double d[3];
+#pragma unroll
+    for (int i = 0; i < LAGRANGE; i++)
+        dt[i] = o.t[f + i] - tt;
+#pragma unroll
+    for (int comp = 0; comp < 6; comp++) {
+        const double *src = comp < 3 ? o.pos : o.vel;
+        const int q = comp % 3;
+        /* offsets from the window's middle vector */
+        const double base = src[3 * c + q];
 
-        for (int k = 0; k < 3; k++)
-            d[k] = p[k] - o.pos[3 * i + k];
-        const double dist = dot3(d, d);
-
-        if (best < 0 || dist < best) {
-            best = dist;
-            t = o.t[i];
-        }
+#pragma unroll
+        for (int i = 0; i < LAGRANGE; i++)
+            y[i] = src[3 * (f + i) + q] - base;
+        out[comp] = base + neville(dt, y, comp < 3 ? nullptr : der + q);
     }
-    for (int it = 0; it < 30; it++) {
-        double s[3], v[3], d[3];
-
-        orbit_state(o, t, s, v);
-        for (int k = 0; k < 3; k++)
-            d[k] = p[k] - s[k];
-        const double dt = dot3(v, d) / dot3(v, v);
-
-        t += dt;
-        if (fabs(dt) < 1e-10)
-            break;
-    }
-    tz = t;
-    return !(t < o.t[0] || t > o.t[o.n - 1]);
+    return {v3(out[0], out[1], out[2]), v3(out[3], out[4], out[5]), v3(der[0], der[1], der[2])};
 }
 
-__device__ double det3(const double (&m)[3][3])
-{
-    return m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) -
-           m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
-           m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
-}
-
-/* Cramer's rule; false when singular */
-__device__ bool solve3(const double (&a)[3][3], const double *b, double *x)
-{
-    const double det = det3(a);
-
-    if (det == 0.0)
-        return false;
-    for (int c = 0; c < 3; c++) {
-        double m[3][3];
-
-        for (int r = 0; r < 3; r++)
-            for (int q = 0; q < 3; q++)
-                m[r][q] = q == c ? b[r] : a[r][q];
-        x[c] = det3(m) / det;
-    }
-    return true;
-}
-
-/* false when singular or not converged */
-__device__ bool geolocate(const DevOrbit &o, double t, double range, double h, bool have_guess,
-                          double *p)
+/* Ground point at height h seen at slant range R from the state st (the
+   reference orbit at the node's azimuth time), right-looking; false when
+   Newton's method on the look angle does not settle. */
+__host__ __device__ bool ground_point(const State &st, double R, double h, V3 &p)
 {
     const double a = WGS84_A + h, b = WGS84_B + h;
-    double s[3], v[3];
+    const double ia2 = 1.0 / (a * a), ib2 = 1.0 / (b * b);
+    const V3 s = st.pos, v = st.vel;
+    const V3 e1 = unit((dot(s, v) / dot(v, v)) * v - s); /* down, in the plane */
+    const V3 e2 = unit(cross(v, s));                       /* right of the track */
+    const double rho2 = dot(s, s);
+    /* a sphere of the ellipsoid's radius below the satellite */
+    const double z2 = s.z * s.z / rho2;
+    const double re2 = a * a * b * b / (b * b * (1.0 - z2) + a * a * z2);
+    const double c0 = (rho2 + R * R - re2) / (2.0 * sqrt(rho2) * R);
+    double ang = acos(fmin(fmax(c0, -1.0), 1.0));
 
-    orbit_state(o, t, s, v);
-    if (!have_guess) {
-        double right[3];
-        const double rs = sqrt(dot3(s, s));
+    for (int it = 0; it < 40; it++) {
+        double sn, cs;
 
-        right[0] = v[1] * s[2] - v[2] * s[1];
-        right[1] = v[2] * s[0] - v[0] * s[2];
-        right[2] = v[0] * s[1] - v[1] * s[0];
-        const double nr = sqrt(dot3(right, right));
-        const double ground = sqrt(fmax(range * range - (rs - a) * (rs - a), 0.0));
+        sincos(ang, &sn, &cs);
+        p = s + R * (cs * e1 + sn * e2);
+        const V3 dp = R * (cs * e2 - sn * e1);
+        const double F = (p.x * p.x + p.y * p.y) * ia2 + p.z * p.z * ib2 - 1.0;
+        const double dF = 2.0 * ((p.x * dp.x + p.y * dp.y) * ia2 + p.z * dp.z * ib2);
 
-        for (int k = 0; k < 3; k++)
-            p[k] = s[k] * a / rs + right[k] / nr * ground;
-    }
-    for (int it = 0; it < 50; it++) {
-        double d[3], jac[3][3], f[3], dx[3];
-
-        for (int k = 0; k < 3; k++)
-            d[k] = p[k] - s[k];
-        const double dist = sqrt(dot3(d, d));
-
-        f[0] = -dot3(v, d);
-        f[1] = -(dist - range);
-        f[2] = -((p[0] * p[0] + p[1] * p[1]) / (a * a) + p[2] * p[2] / (b * b) - 1.0);
-        for (int k = 0; k < 3; k++) {
-            jac[0][k] = v[k];
-            jac[1][k] = d[k] / dist;
-        }
-        jac[2][0] = 2.0 * p[0] / (a * a);
-        jac[2][1] = 2.0 * p[1] / (a * a);
-        jac[2][2] = 2.0 * p[2] / (b * b);
-        if (!solve3(jac, f, dx))
+        if (!(dF != 0.0))
             return false;
-        for (int k = 0; k < 3; k++)
-            p[k] += dx[k];
-        if (sqrt(dot3(dx, dx)) < 1e-6)
+        const double step = F / dF;
+
+        ang -= step;
+        if (fabs(step) * R < 1e-8) {
+            sincos(ang, &sn, &cs);
+            p = s + R * (cs * e1 + sn * e2);
             return true;
+        }
     }
     return false;
 }
 
-__global__ void tc_geometry_grid_kernel(TcGeo g, TcOrbitSet orbits, double *grid)
+/* v . (p - s) at state vector i: positive before the point is passed */
+__host__ __device__ __forceinline__ double doppler_at(const Orbit &o, int i, V3 p)
 {
-    const int node = blockIdx.x * blockDim.x + threadIdx.x;
+    return dot(row3(o.vel, i), p - row3(o.pos, i));
+}
+
+/* Slant range from p to orbit o at its zero-Doppler time; false when that
+   time is not bracketed inside the orbit or Newton's method stalls. */
+__host__ __device__ bool zero_doppler_range(const Orbit &o, V3 p, double &range)
+{
+    int near = 0;
+    double best = INFINITY;
+
+    for (int i = 0; i < o.nsv; i++) {
+        const V3 d = p - row3(o.pos, i);
+        const double d2 = dot(d, d);
+
+        if (d2 < best) {
+            best = d2;
+            near = i;
+        }
+    }
+    const int lo = doppler_at(o, near, p) >= 0.0 ? near : near - 1, hi = lo + 1;
+
+    if (lo < 0 || hi >= o.nsv)
+        return false;
+    const double flo = doppler_at(o, lo, p), fhi = doppler_at(o, hi, p);
+
+    if (!(flo >= 0.0 && fhi <= 0.0))
+        return false;
+    double t = flo > fhi ? o.t[lo] + flo / (flo - fhi) * (o.t[hi] - o.t[lo]) : o.t[lo];
+
+    for (int it = 0; it < 20; it++) {
+        const State st = orbit_state(o, t);
+        const V3 d = p - st.pos;
+        const double f = dot(st.vel, d), df = dot(st.acc, d) - dot(st.vel, st.vel);
+
+        if (!(df < 0.0))
+            return false;
+        const double step = f / df;
+
+        t -= step;
+        if (fabs(step) < 1e-9) {
+            if (t < o.t[0] || t > o.t[o.nsv - 1])
+                return false;
+            const V3 e = p - orbit_state(o, t).pos;
+
+            range = sqrt(dot(e, e));
+            return true;
+        }
+    }
+    return false;
+}
+
+/* One warp per grid node: ground points on lanes (one height level each),
+   then the (level, date) ranges over the lanes, then the phases. */
+__global__ void __launch_bounds__(32 * GRID_WARPS)
+tc_geometry_grid_kernel(TcGeo g, TcOrbitSet orbits, double *grid)
+{
+    __shared__ double s_range[GRID_WARPS][3][TC_MAX_DATES];
+    __shared__ V3 s_point[GRID_WARPS][3];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int node = blockIdx.x * GRID_WARPS + warp;
 
     if (node >= g.grid_rows * g.grid_cols)
-        return;
+        return; /* the whole warp */
     const int gr = node / g.grid_cols, gc = node - gr * g.grid_cols, n = g.ndates;
-    const double line = g.line0 + (double)gr * GEO_STEP;
-    const double t = g.first_line_time + line * g.azimuth_time_interval;
-    const double sample = g.sample0 + (double)gc * GEO_STEP;
-    const double range = 0.5 * SPEED_OF_LIGHT * (g.slant_range_time + sample / g.range_sampling_rate);
-    const DevOrbit ref = dev_orbit(orbits, g.ref);
-    double p[3] = {0.0, 0.0, 0.0};
+    const int items = g.nheights * n;
+    const double tt =
+        g.first_line_time + (g.line0 + (double)gr * TC_GEO_STEP) * g.azimuth_time_interval;
+    const double R = 0.5 * SPEED_OF_LIGHT *
+                     (g.slant_range_time + (g.sample0 + (double)gc * TC_GEO_STEP) /
+                                               g.range_sampling_rate);
+    bool ok = true;
 
-    for (int hl = 0; hl < g.nheights; hl++) {
-        double *ph = grid + ((size_t)node * g.nheights + hl) * n;
-        double r_ref = 0.0;
+    if (lane < g.nheights) {
+        const State st = orbit_state(orbit_of(orbits, g.ref), tt);
 
-        if (!geolocate(ref, t, range, g.heights[hl], hl > 0, p)) {
+        ok = ground_point(st, R, g.heights[lane], s_point[warp][lane]);
+    }
+    if (!__all_sync(FULL, ok)) {
+        if (lane == 0)
             atomicOr(&g_geo_fault, 1);
-            return;
-        }
-        for (int k = 0; k < n; k++) {
-            const DevOrbit o = dev_orbit(orbits, k);
-            double tk, s[3], v[3], d[3];
+        return;
+    }
+    __syncwarp();
+    for (int q = lane; q < items; q += 32) {
+        const int hl = q / n, k = q - hl * n;
 
-            if (!zero_doppler(o, p, tk)) {
-                atomicOr(&g_geo_fault, 2);
-                return;
-            }
-            orbit_state(o, tk, s, v);
-            for (int c = 0; c < 3; c++)
-                d[c] = p[c] - s[c];
-            ph[k] = sqrt(dot3(d, d));
-            if (k == g.ref)
-                r_ref = ph[k];
-        }
-        for (int k = 0; k < n; k++)
-            ph[k] = 4.0 * M_PI / g.wavelength * (ph[k] - r_ref);
+        ok &= zero_doppler_range(orbit_of(orbits, k), s_point[warp][hl], s_range[warp][hl][k]);
+    }
+    if (!__all_sync(FULL, ok)) {
+        if (lane == 0)
+            atomicOr(&g_geo_fault, 2);
+        return;
+    }
+    __syncwarp();
+    const double scale = 4.0 * M_PI / g.wavelength;
+
+    for (int q = lane; q < items; q += 32) {
+        const int hl = q / n, k = q - hl * n;
+
+        grid[(size_t)node * items + q] = scale * (s_range[warp][hl][k] - s_range[warp][hl][g.ref]);
+    }
+}
+
+/* Coefficient form (TcGridCell): one thread per node and date. With the
+   levels h0 < h1 < h2 and their phases P0, P1, P2, the Newton form about
+   h1 gives phase(h) = P1 + u (d12 - (h2 - h1) d012) + u^2 d012, u = h - h1,
+   d12 and d012 the first and second divided differences. */
+__global__ void tc_geometry_coef_kernel(TcGeo g, const double *__restrict__ grid,
+                                        double *__restrict__ coef)
+{
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = g.ndates;
+
+    if (q >= (long long)g.grid_rows * g.grid_cols * n)
+        return;
+    const long long node = q / n;
+    const int k = (int)(q - node * n);
+    double *out = coef + 3 * q;
+
+    if (g.nheights == 3) {
+        const double *P = grid + node * 3 * n + k;
+        const double *h = g.heights;
+        const double d01 = (P[n] - P[0]) / (h[1] - h[0]);
+        const double d12 = (P[2 * n] - P[n]) / (h[2] - h[1]);
+        const double d012 = (d12 - d01) / (h[2] - h[0]);
+
+        out[0] = P[n];
+        out[1] = d12 - (h[2] - h[1]) * d012;
+        out[2] = d012;
+    }
+    else {
+        out[0] = grid[node * n + k];
+        out[1] = 0.0;
+        out[2] = 0.0;
     }
 }
 
@@ -252,29 +364,6 @@ __device__ __forceinline__ void bitonic(float (&a)[NP])
             }
 }
 
-/* Interpolated phase of date k at region cell (row, col) and height h. */
-__device__ __forceinline__ double grid_phase(const TcGeo &g, const double *grid, int gr, int gc,
-                                             double fr, double fc, const double (&wh)[3], int k)
-{
-    const int n = g.ndates;
-    const size_t stride = (size_t)g.nheights * n;
-    double ph = 0.0;
-
-#pragma unroll
-    for (int hl = 0; hl < 3; hl++) {
-        if (hl >= g.nheights)
-            break;
-        const double *p00 = grid + (((size_t)gr * g.grid_cols + gc) * g.nheights + hl) * n;
-        const double *p01 = p00 + stride;
-        const double *p10 = p00 + (size_t)g.grid_cols * stride;
-        const double *p11 = p10 + stride;
-
-        ph += wh[hl] * ((1.0 - fr) * ((1.0 - fc) * p00[k] + fc * p01[k]) +
-                        fr * ((1.0 - fc) * p10[k] + fc * p11[k]));
-    }
-    return ph;
-}
-
 /* One thread per strip cell; the outputs are pixel-major ([pixel][date]),
    so each warp stages its 32 pixels' amplitudes, then their samples, in
    shared memory (row stride n | 1, conflict-free for the 4-byte
@@ -283,7 +372,8 @@ template <int NP>
 __global__ void __launch_bounds__(256, NP <= 32 ? 3 : 1)
 tc_prep_raw_kernel(int n, const float *__restrict__ re, const float *__restrict__ im,
                    const double *__restrict__ elev, int row0, int region_rows, int padded_rows,
-                   int cols, int halo, int use_geo, TcGeo g, const double *__restrict__ grid,
+                   int cols, int halo, long long cell0, long long cell1, int use_geo, TcGeo g,
+                   const double *__restrict__ grid,
                    const double *__restrict__ dh, const float *__restrict__ psi,
                    float2 *__restrict__ slc, float *__restrict__ amp,
                    unsigned char *__restrict__ valid)
@@ -291,8 +381,8 @@ tc_prep_raw_kernel(int n, const float *__restrict__ re, const float *__restrict_
     extern __shared__ float2 prep_stage[];
     const int W = cols + 2 * halo, ld = n | 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const long long total = (long long)padded_rows * W;
-    const long long pix = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = cell1;
+    const long long pix = cell0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long wpix = pix - lane;
     const int wcount = (int)min(32LL, total - wpix);
     float2 *wb = prep_stage + warp * 32 * ld;
@@ -344,22 +434,12 @@ tc_prep_raw_kernel(int n, const float *__restrict__ re, const float *__restrict_
             wb[lane * ld + k] = make_float2(re[k * plane + at], im[k * plane + at]);
     }
     else {
-        const int gr = row / GEO_STEP, gc = c / GEO_STEP;
-        const double fr = (double)(row - gr * GEO_STEP) / GEO_STEP;
-        const double fc = (double)(c - gc * GEO_STEP) / GEO_STEP;
         /* the adjoint's variables: a height error and a phase screen */
         const double h = (elev ? elev[at] : g.h0) + (dh ? dh[at] : 0.0);
-        double wh[3] = {1.0, 0.0, 0.0};
+        const TcGridCell cell = use_geo ? tc_grid_cell(g, grid, row, c, h) : TcGridCell{};
 
-        if (use_geo && g.nheights == 3) {
-            const double *x = g.heights;
-
-            wh[0] = (h - x[1]) * (h - x[2]) / ((x[0] - x[1]) * (x[0] - x[2]));
-            wh[1] = (h - x[0]) * (h - x[2]) / ((x[1] - x[0]) * (x[1] - x[2]));
-            wh[2] = (h - x[0]) * (h - x[1]) / ((x[2] - x[0]) * (x[2] - x[1]));
-        }
         for (int k = 0; k < n; k++) {
-            const double ph = (use_geo ? grid_phase(g, grid, gr, gc, fr, fc, wh, k) : 0.0) +
+            const double ph = (use_geo ? cell.phase(k, nullptr) : 0.0) +
                               (psi ? (double)psi[k * plane + at] : 0.0);
             double sn, cs;
 
@@ -383,9 +463,10 @@ tc_prep_raw_kernel(int n, const float *__restrict__ re, const float *__restrict_
 template <int NP>
 cudaError_t launch_prep_raw(unsigned blocks, int n, const float *re, const float *im,
                             const double *elev, int row0, int region_rows, int padded_rows,
-                            int cols, int halo, int use, const TcGeo &g, const double *grid,
-                            const double *dh, const float *psi, float2 *s, float *amp,
-                            unsigned char *valid, cudaStream_t st)
+                            int cols, int halo, long long cell0, long long cell1, int use,
+                            const TcGeo &g, const double *grid, const double *dh,
+                            const float *psi, float2 *s, float *amp, unsigned char *valid,
+                            cudaStream_t st)
 {
     const int bytes = 8 * 32 * (n | 1) * (int)sizeof(float2);
     cudaError_t e = cudaFuncSetAttribute(tc_prep_raw_kernel<NP>,
@@ -394,8 +475,8 @@ cudaError_t launch_prep_raw(unsigned blocks, int n, const float *re, const float
     if (e != cudaSuccess)
         return e;
     tc_prep_raw_kernel<NP><<<blocks, 256, bytes, st>>>(n, re, im, elev, row0, region_rows,
-                                                      padded_rows, cols, halo, use, g, grid, dh,
-                                                      psi, s, amp, valid);
+                                                      padded_rows, cols, halo, cell0, cell1, use,
+                                                      g, grid, dh, psi, s, amp, valid);
     return cudaGetLastError();
 }
 
@@ -415,8 +496,8 @@ int tc_geometry_shape(const struct tc_geometry &in, TcGeo &g)
         return tc_error(TC_ERR_ARG, "geometry: height range %g .. %g", in.hmin, in.hmax);
     g.ndates = in.ndates;
     g.ref = in.ref;
-    g.grid_rows = (in.rows - 1) / GEO_STEP + 2;
-    g.grid_cols = (in.cols - 1) / GEO_STEP + 2;
+    g.grid_rows = (in.rows - 1) / TC_GEO_STEP + 2;
+    g.grid_cols = (in.cols - 1) / TC_GEO_STEP + 2;
     if (in.hmax - in.hmin < 1.0) {
         g.nheights = 1;
         g.heights[0] = 0.5 * (in.hmin + in.hmax);
@@ -499,7 +580,8 @@ int tc_geometry_grid(const TcGeo &g, const struct tc_orbit *orbits, double *grid
         os.t = d_t;
         os.pos = d_pos;
         os.vel = d_vel;
-        tc_geometry_grid_kernel<<<(unsigned)((nodes + 127) / 128), 128, 0, st>>>(g, os, d_grid);
+        tc_geometry_grid_kernel<<<(unsigned)((nodes + GRID_WARPS - 1) / GRID_WARPS),
+                                  32 * GRID_WARPS, 0, st>>>(g, os, d_grid);
         e = cudaGetLastError();
     }
     GEO_CK(cudaMemcpyAsync(grid_host, d_grid, grid_bytes, cudaMemcpyDeviceToHost, st));
@@ -524,28 +606,40 @@ int tc_geometry_grid(const TcGeo &g, const struct tc_orbit *orbits, double *grid
     return rc;
 }
 
+cudaError_t tc_launch_geometry_coef(const TcGeo &g, const double *grid, double *coef,
+                                    cudaStream_t st)
+{
+    const long long items = (long long)g.grid_rows * g.grid_cols * g.ndates;
+
+    tc_geometry_coef_kernel<<<(unsigned)((items + 255) / 256), 256, 0, st>>>(g, grid, coef);
+    return cudaGetLastError();
+}
+
 cudaError_t tc_launch_prep_raw(int n, const float *re, const float *im, const double *elev,
                                int row0, int region_rows, int padded_rows, int cols, int halo,
-                               const TcGeo *g, const double *grid, const double *dh,
-                               const float *psi, float *slc, float *amp, unsigned char *valid,
-                               cudaStream_t st)
+                               int prow0, int prow1, const TcGeo *g, const double *grid,
+                               const double *dh, const float *psi, float *slc, float *amp,
+                               unsigned char *valid, cudaStream_t st)
 {
-    const long long cells = (long long)padded_rows * (cols + 2 * halo);
-    const unsigned blocks = (unsigned)((cells + 255) / 256);
+    const long long W = cols + 2 * halo;
+    const long long cell0 = (long long)prow0 * W, cell1 = (long long)prow1 * W;
+    const unsigned blocks = (unsigned)((cell1 - cell0 + 255) / 256);
     const TcGeo none = {};
     const TcGeo &gg = g ? *g : none;
     const int use = g != nullptr;
     float2 *s = (float2 *)slc;
 
+    if (cell1 <= cell0)
+        return cudaSuccess;
     if (n <= 8)
         return launch_prep_raw<8>(blocks, n, re, im, elev, row0, region_rows, padded_rows, cols,
-                                  halo, use, gg, grid, dh, psi, s, amp, valid, st);
+                                  halo, cell0, cell1, use, gg, grid, dh, psi, s, amp, valid, st);
     if (n <= 16)
         return launch_prep_raw<16>(blocks, n, re, im, elev, row0, region_rows, padded_rows, cols,
-                                   halo, use, gg, grid, dh, psi, s, amp, valid, st);
+                                   halo, cell0, cell1, use, gg, grid, dh, psi, s, amp, valid, st);
     if (n <= 32)
         return launch_prep_raw<32>(blocks, n, re, im, elev, row0, region_rows, padded_rows, cols,
-                                   halo, use, gg, grid, dh, psi, s, amp, valid, st);
+                                   halo, cell0, cell1, use, gg, grid, dh, psi, s, amp, valid, st);
     return launch_prep_raw<64>(blocks, n, re, im, elev, row0, region_rows, padded_rows, cols,
-                               halo, use, gg, grid, dh, psi, s, amp, valid, st);
+                               halo, cell0, cell1, use, gg, grid, dh, psi, s, amp, valid, st);
 }

@@ -1,7 +1,9 @@
 /* Phase linking and temporal coherence of every output pixel, from its
- * masked covariance (the packed upper triangle produced by a Gram kernel).
+ * masked covariance (the packed upper triangle produced by a Gram kernel),
+ * for stacks of 33 to 64 dates, and the exact tier of EMI (any number of
+ * dates up to 64; see tc_link_exact_kernel below).
  *
- * One warp per pixel. Stages (tcoh.cl:603-744):
+ * EVD, one warp per pixel. Stages (tcoh.cl:603-744):
  *
  *   coherence matrix T_ij = C_ij / sqrt(C_ii C_jj), optional magnitude bias
  *   correction, in float with round-to-nearest intrinsics in the
@@ -9,17 +11,8 @@
  *   pair coherences |T_ij| (tcoh.cl:515-527, 639);
  *   connectivity of the non-zero T_ij under the bias correction, as a
  *   bit-parallel breadth-first search (tcoh.cl:494-513, 644-647);
- *   EVD: eigenvector of the largest eigenvalue of T, in float (as
- *   tcoh.cl:649-656); EMI: eigenvector of the smallest eigenvalue of
- *   M = |T|^-1 o T (tcoh.cl:657-694), all in double: |T| is inverted by
- *   the symmetric sweep (Gauss-Jordan without pivoting, which takes the
- *   indefinite |T| of noisy stacks) when its pivots stay above 1e-5 in
- *   magnitude and the inverse stays moderate, else by its Jacobi
- *   eigen-pseudo-inverse with the absolute eigenvalue floor 1e-9 of
- *   tests/reference.py:151-156; the two differ only near singularity,
- *   since the pseudo-inverse of a matrix whose eigenvalues all exceed 1e-9
- *   in magnitude is its inverse;
- *   the eigenvector is one Householder reduction to a real tridiagonal
+ *   the eigenvector of the largest eigenvalue of T, in float (as
+ *   tcoh.cl:649-656): one Householder reduction to a real tridiagonal
  *   (LAPACK zhetd2 form), a 33-way multisection on Sturm counts for the
  *   wanted eigenvalue, inverse iteration on the tridiagonal and the
  *   back-transformation (the method of tcoh.cl:201-444);
@@ -27,14 +20,9 @@
  *   when it is negligible) and the Pepe-Lanari goodness of fit
  *   (tcoh.cl:696-744).
  *
- * This file holds the path for 33 to 64 dates, where the matrices stay in
- * shared memory, two rows per lane. With EMI, |T| and its inverse occupy
- * the first half of the working matrix's region (the Jacobi fallback's
- * eigenvectors the second half) until M is formed over them, so that a
- * warp needs T plus one complex double matrix: two warps per SM at 60
- * dates. Up to 32 dates the
- * faster register path of kernels_link_half.cu runs instead (same stages,
- * same numerics, two pixels per warp).
+ * The matrices stay in shared memory, two rows per lane. Up to 32 dates
+ * the faster register path of kernels_link_half.cu runs instead (same
+ * stages, same numerics, two pixels per warp).
  */
 #include "tcoh_internal.h"
 
@@ -80,6 +68,14 @@ __device__ __forceinline__ float wmax(float v)
 #pragma unroll
     for (int o = 16; o; o >>= 1)
         v = fmaxf(v, __shfl_xor_sync(FULL, v, o));
+    return v;
+}
+
+__device__ __forceinline__ double wmaxd(double v)
+{
+#pragma unroll
+    for (int o = 16; o; o >>= 1)
+        v = fmax(v, __shfl_xor_sync(FULL, v, o));
     return v;
 }
 
@@ -150,7 +146,6 @@ __device__ __forceinline__ Ws workspace(double *base, const LinkLayout &L)
 /* ------------------------------------------------------------------ */
 
 __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
-__device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
 
 /* Number of eigenvalues of the double tridiagonal (d, e) below x. Only the
    signs matter: 1/q comes from the float reciprocal and one Newton step
@@ -592,63 +587,6 @@ __device__ unsigned heig_smem(int n, int ld, typename Cx<R>::T *A, int index, co
     return status;
 }
 
-/* In-place inverse of the symmetric W (double, full storage, shared
-   memory) by the symmetric sweep (Gauss-Jordan elimination without
-   pivoting in the form that keeps the matrix symmetric; Goodnight, The
-   American Statistician 33, 1979): sweeping pivot k maps
-       a_ij -> a_ij - a_ik a_kj / a_kk,  a_ik, a_kj -> a_ik / a_kk,
-       a_kk -> -1 / a_kk,
-   and sweeping every pivot leaves -W^-1. It takes indefinite matrices. row
-   is n doubles of scratch (the pivot row before the step). False when a
-   pivot's magnitude is not above 1e-5, or when the inverse is not finite or
-   so large (n max|inv| >= 1e8) that an eigenvalue may lie below the
-   pseudo-inverse floor 1e-9; W is then undefined. */
-__device__ bool sweep_inverse_smem(int n, int ld, double *W, double *row, int lane)
-{
-    for (int k = 0; k < n; k++) {
-        const double d = W[k * ld + k];
-
-        if (!(fabs(d) > 1.0e-5))
-            return false;
-        const double id = 1.0 / d;
-
-        for (int j = lane; j < n; j += 32)
-            row[j] = W[k * ld + j];
-        __syncwarp();
-        for (int r = lane; r < n; r += 32) {
-            double *wr = W + r * ld;
-
-            if (r == k)
-                for (int j = 0; j < n; j++)
-                    wr[j] = j == k ? -id : row[j] * id;
-            else {
-                const double f = wr[k] * id;
-
-                for (int j = 0; j < n; j++)
-                    wr[j] = j == k ? f : fma(-f, row[j], wr[j]);
-            }
-        }
-        __syncwarp();
-    }
-    double mx = 0.0;
-    bool bad = false;
-
-    for (int r = lane; r < n; r += 32)
-        for (int j = 0; j < n; j++) {
-            const double v = -W[r * ld + j];
-
-            W[r * ld + j] = v;
-            bad |= !(fabs(v) <= 1.0e300);
-            mx = fmax(mx, fabs(v));
-        }
-#pragma unroll
-    for (int o = 16; o; o >>= 1)
-        mx = fmax(mx, __shfl_xor_sync(FULL, mx, o));
-    bad = __any_sync(FULL, bad);
-    __syncwarp();
-    return !bad && n * mx < 1.0e8;
-}
-
 /* Pseudo-inverse of the symmetric W (double, full storage) in place, from
    its cyclic Jacobi eigendecomposition; eigenvalues |l| < 1e-9 are dropped
    (tests/reference.py:151-156). V is workspace (n x ld). Returns status
@@ -988,75 +926,18 @@ tc_link_smem_kernel(TcStrip s, TcChunk c, TcLinkConst k, LinkLayout L,
             __syncwarp();
             continue;
         }
-        float gamma;
+        /* EVD (the EMI path of this many dates is tc_link_exact_kernel) */
+        float2 *A = (float2 *)w.A;
 
-        if (!k.emi) {
-            float2 *A = (float2 *)w.A;
+        for (int r = lane; r < n; r += 32)
+            for (int j = 0; j < n; j++)
+                A[r * ld + j] = w.T[r * ld + j];
+        __syncwarp();
+        float2 z[2];
 
-            for (int r = lane; r < n; r += 32)
-                for (int j = 0; j < n; j++)
-                    A[r * ld + j] = w.T[r * ld + j];
-            __syncwarp();
-            float2 z[2];
+        st |= heig_smem<float>(n, ld, A, n - 1, w, lane, z);
+        const float gamma = phasors_and_gamma<float>(n, ld, w, z, upper_tab, lane);
 
-            st |= heig_smem<float>(n, ld, A, n - 1, w, lane, z);
-            gamma = phasors_and_gamma<float>(n, ld, w, z, upper_tab, lane);
-        }
-        else {
-            /* |T| and its inverse in w.G, the first half of the working
-               matrix's region; the second half holds the Jacobi fallback's
-               eigenvectors */
-            double2 *A = (double2 *)w.A;
-            double *V = w.G + n * ld;
-
-            for (int r = lane; r < n; r += 32)
-                for (int j = 0; j < n; j++) {
-                    const float2 t = w.T[r * ld + j];
-
-                    w.G[r * ld + j] = hypot((double)t.x, (double)t.y);
-                }
-            __syncwarp();
-            if (!sweep_inverse_smem(n, ld, w.G, (double *)w.vw, lane)) {
-                __syncwarp();
-                for (int r = lane; r < n; r += 32)
-                    for (int j = 0; j < n; j++) {
-                        const float2 t = w.T[r * ld + j];
-
-                        w.G[r * ld + j] = hypot((double)t.x, (double)t.y);
-                    }
-                __syncwarp();
-                st |= TC_STATUS_EMI_PINV | jacobi_pinv(n, ld, w.G, V, w.lam, lane);
-            }
-            /* M = |T|^-1 o T over the same region, 32 entries at a time from
-               the last one down: complex entry q covers |T|^-1 entries 2q and
-               2q + 1, which are above the block being read (or in it, read
-               before the barrier) and so already consumed */
-            const int total = n * ld;
-
-            for (int base = (total - 1) & ~31; base >= 0; base -= 32) {
-                const int q = base + lane;
-                double2 v = make_double2(0.0, 0.0);
-
-                if (q < total) {
-                    const int r = q / ld, j = q - r * ld;
-
-                    if (j < n) {
-                        const float2 t = w.T[r * ld + j];
-                        const double gg = w.G[q];
-
-                        v = make_double2(gg * (double)t.x, gg * (double)t.y);
-                    }
-                }
-                __syncwarp();
-                if (q < total)
-                    A[q] = v;
-                __syncwarp();
-            }
-            double2 z[2];
-
-            st |= heig_smem<double>(n, ld, A, 0, w, lane, z);
-            gamma = phasors_and_gamma<double>(n, ld, w, z, upper_tab, lane);
-        }
         if (lane == 0)
             coh[out] = gamma;
         if (phases)
@@ -1068,6 +949,909 @@ tc_link_smem_kernel(TcStrip s, TcChunk c, TcLinkConst k, LinkLayout L,
         if (status && lane == 0)
             status[out] = (unsigned char)st;
         __syncwarp();
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* The exact tier: EMI from double-precision coherence sums.           */
+/* ------------------------------------------------------------------ */
+
+/* EMI divides by |T|, whose condition number reaches 1e5 - 1e6 on noisy or
+   highly coherent stacks: the float rounding of the coherence sums and of
+   their normalisation (a few 1e-7 relative) then moves gamma by up to 1e-3,
+   however exactly the rest is computed. This tier recomputes a pixel from
+   its samples with everything in double: the masked sums
+   C = sum over SHPs q of s_q s_q^H (tcoh.cl:567-602, as tests/reference.py
+   sums them), T and its bias correction (tcoh.cl:610-636), |T|^-1 (the
+   symmetric sweep, or the Jacobi pseudo-inverse with the absolute floor
+   1e-9 of tests/reference.py:151-156 when a pivot falls below 1e-5 or the
+   inverse is huge), M = |T|^-1 o T, its Householder reduction to a real
+   tridiagonal, the smallest eigenvalue by multisection on Sturm counts,
+   inverse iteration and the back-transformation; then the phasors and
+   gamma (tcoh.cl:696-744). It runs every pixel of the 33-64-date EMI path,
+   and the pixels that the 32-date kernel flags as ill-conditioned.
+
+   One CTA of four warps per pixel, every matrix in packed upper-triangle
+   storage (index tc_pidx) in shared memory, so that three pixels fit an
+   SM at 60 dates: the sums and T (then M, in place) in complex double,
+   |T| and its inverse in double (then, once M is formed, a float copy of
+   T for gamma in the same place). The sums
+   accumulate in registers, each thread a few 2 x 4 blocks of the
+   triangle, over the SHP samples staged 16 candidates at a time. */
+
+constexpr int EX_THREADS = 128;
+constexpr int EX_CTAS = 3;        /* CTAs per SM */
+constexpr int EX_KC = 16;         /* candidates per staging block */
+constexpr int EX_BC = 4;          /* columns per register block (2 rows x 4) */
+constexpr int EX_NB = 3;          /* register blocks per thread, n <= 64 */
+
+struct ExLayout {
+    int n, npu, nblk, ld;
+    int off_T, off_G, off_tab, off_blk, off_stage, off_cand, off_vec, off_adj;
+    int bytes;
+};
+
+struct ExWs {
+    double2 *T;       /* [npu] sums, then T, then M */
+    double *G;        /* [npu] |T|, then its inverse */
+    float2 *Tf;       /* [npu] T in float, over G once M is formed */
+    unsigned short *tab, *blk, *cand;
+    float2 *stage;    /* [EX_KC][n] */
+    double *d, *e, *e2, *y, *lu, *rrow, *nrm, *red;
+    double2 *v, *w, *tau, *z;
+    float2 *zs;
+    unsigned long long *adj;
+    int *ints;        /* [0] candidates, [1] flags */
+};
+
+__host__ __device__ inline ExLayout ex_layout(int n, int area)
+{
+    ExLayout L;
+    int off = 0;
+    auto take = [&](int bytes) {
+        const int o = off;
+
+        off += (bytes + 15) & ~15;
+        return o;
+    };
+    const int rp = (n + 1) / 2, cg = (n + EX_BC - 1) / EX_BC;
+
+    L.n = n;
+    L.npu = tc_npu(n);
+    L.ld = n | 1;
+    L.nblk = 0;
+    for (int ip = 0; ip < rp; ip++)
+        L.nblk += cg - (2 * ip) / EX_BC;
+    L.off_T = take(16 * L.npu);
+    L.off_G = take(8 * L.npu);
+    L.off_tab = take(2 * L.npu);
+    L.off_blk = take(2 * L.nblk);
+    L.off_stage = take(8 * EX_KC * n);
+    L.off_cand = take(2 * area);
+    L.off_vec = take(8 * (8 * 64 + 8 + 4 * 64) + 16 * 5 * 64 + 8 * 64 + 16);
+    L.off_adj = take(8 * 64);
+    L.bytes = off;
+    return L;
+}
+
+__device__ __forceinline__ ExWs ex_ws(unsigned char *base, const ExLayout &L)
+{
+    ExWs w;
+    double *v = (double *)(base + L.off_vec);
+
+    w.T = (double2 *)(base + L.off_T);
+    w.G = (double *)(base + L.off_G);
+    w.Tf = (float2 *)(base + L.off_G);
+    w.tab = (unsigned short *)(base + L.off_tab);
+    w.blk = (unsigned short *)(base + L.off_blk);
+    w.stage = (float2 *)(base + L.off_stage);
+    w.cand = (unsigned short *)(base + L.off_cand);
+    w.d = v;
+    w.e = v + 64;
+    w.e2 = v + 128;
+    w.y = v + 192;
+    w.rrow = v + 256;
+    w.nrm = v + 320;
+    w.red = v + 384;        /* 8 */
+    w.lu = v + 392;         /* 4 x 64 */
+    double2 *c = (double2 *)(v + 392 + 256);
+
+    w.v = c;
+    w.w = c + 64;
+    w.tau = c + 128;
+    w.z = c + 192;
+    w.zs = (float2 *)(c + 320);
+    w.ints = (int *)(w.zs + 64);
+    w.adj = (unsigned long long *)(base + L.off_adj);
+    return w;
+}
+
+/* Block sums over the CTA (every thread gets them); red holds 8 doubles. */
+__device__ __forceinline__ double2 ex_sum2(double a, double b, double *red)
+{
+    a = wsum<double>(a);
+    b = wsum<double>(b);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) {
+        red[threadIdx.x >> 5] = a;
+        red[4 + (threadIdx.x >> 5)] = b;
+    }
+    __syncthreads();
+    return make_double2(red[0] + red[1] + red[2] + red[3], red[4] + red[5] + red[6] + red[7]);
+}
+
+/* Packed (i, j) of the upper triangle for any order of i, j. */
+__device__ __forceinline__ int ex_sym(int n, int i, int j)
+{
+    return i <= j ? tc_pidx(n, i, j) : tc_pidx(n, j, i);
+}
+
+/* M_ij (Hermitian) from packed upper storage. */
+__device__ __forceinline__ double2 ex_m(const double2 *P, int n, int i, int j)
+{
+    if (i <= j)
+        return P[tc_pidx(n, i, j)];
+    const double2 m = P[tc_pidx(n, j, i)];
+
+    return make_double2(m.x, -m.y);
+}
+
+/* The pixel's SHP candidates (window indices) into w.cand; their number. */
+__device__ int ex_candidates(const TcStrip &s, const TcChunk &c, const uint32_t *mask, int p,
+                             const ExWs &w)
+{
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        uint32_t bits = lane < s.mask_words ? mask[(long long)lane * c.npix + p] : 0u;
+
+        if (lane == s.mask_words - 1 && (s.area & 31))
+            bits &= (1u << (s.area & 31)) - 1u; /* candidates only */
+        const int cnt = __popc(bits);
+        int off = cnt;
+
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(FULL, off, o);
+
+            if (lane >= o)
+                off += v;
+        }
+        if (lane == 31)
+            w.ints[0] = off;
+        off -= cnt;
+        while (bits) {
+            const int b = __ffs(bits) - 1;
+
+            bits &= bits - 1;
+            w.cand[off++] = (unsigned short)(lane * 32 + b);
+        }
+    }
+    __syncthreads();
+    return w.ints[0];
+}
+
+/* C = sum of s_q s_q^H over the candidates, in double, into w.T (packed). */
+__device__ void ex_gram(const TcStrip &s, const float2 *slc, int py0, int px0, int ncand,
+                        const ExWs &w, const ExLayout &L)
+{
+    const int n = s.n, t = threadIdx.x;
+    double2 acc[EX_NB][2][EX_BC];
+    int bi[EX_NB], bj[EX_NB];
+
+#pragma unroll
+    for (int b = 0; b < EX_NB; b++) {
+        const int id = t + b * EX_THREADS;
+
+        bi[b] = bj[b] = -1;
+        if (id < L.nblk) {
+            bi[b] = 2 * (w.blk[id] >> 8);
+            bj[b] = EX_BC * (w.blk[id] & 255);
+        }
+#pragma unroll
+        for (int r = 0; r < 2; r++)
+#pragma unroll
+            for (int q = 0; q < EX_BC; q++)
+                acc[b][r][q] = make_double2(0.0, 0.0);
+    }
+    for (int c0 = 0; c0 < ncand; c0 += EX_KC) {
+        const int kc = min(EX_KC, ncand - c0);
+
+        for (int e = t; e < kc * n; e += EX_THREADS) {
+            const int q = e / n, d = e - q * n;
+            const int u = w.cand[c0 + q], dy = u / s.wr, dx = u - dy * s.wr;
+            float2 v = slc[((long long)(py0 + dy) * s.W + px0 + dx) * n + d];
+
+            if (!isfinite(v.x) || !isfinite(v.y))
+                v = make_float2(0.f, 0.f);
+            w.stage[e] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int b = 0; b < EX_NB; b++) {
+            if (bi[b] < 0)
+                continue;
+            for (int q = 0; q < kc; q++) {
+                const float2 *row = w.stage + q * n;
+                double2 a[2], cj[EX_BC];
+
+#pragma unroll
+                for (int r = 0; r < 2; r++) {
+                    const float2 f = bi[b] + r < n ? row[bi[b] + r] : make_float2(0.f, 0.f);
+
+                    a[r] = make_double2(f.x, f.y);
+                }
+#pragma unroll
+                for (int jj = 0; jj < EX_BC; jj++) {
+                    const float2 f = bj[b] + jj < n ? row[bj[b] + jj] : make_float2(0.f, 0.f);
+
+                    cj[jj] = make_double2(f.x, f.y);
+                }
+#pragma unroll
+                for (int r = 0; r < 2; r++)
+#pragma unroll
+                    for (int jj = 0; jj < EX_BC; jj++) {
+                        /* a conj(b) */
+                        acc[b][r][jj].x = fma(a[r].x, cj[jj].x, fma(a[r].y, cj[jj].y, acc[b][r][jj].x));
+                        acc[b][r][jj].y = fma(a[r].y, cj[jj].x, fma(-a[r].x, cj[jj].y, acc[b][r][jj].y));
+                    }
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int b = 0; b < EX_NB; b++) {
+        if (bi[b] < 0)
+            continue;
+#pragma unroll
+        for (int r = 0; r < 2; r++)
+#pragma unroll
+            for (int jj = 0; jj < EX_BC; jj++) {
+                const int i = bi[b] + r, j = bj[b] + jj;
+
+                if (i < n && j < n && i <= j)
+                    w.T[tc_pidx(n, i, j)] = acc[b][r][jj];
+            }
+    }
+    __syncthreads();
+}
+
+/* T from the sums (tcoh.cl:611-636 in double, as tests/reference.py:124-142)
+   and |T|. */
+__device__ void ex_coherence(int n, int npu, const TcLinkConst &k, int looks, const ExWs &w)
+{
+    const int t = threadIdx.x;
+
+    for (int i = t; i < n; i += EX_THREADS)
+        w.nrm[i] = sqrt(w.T[tc_pidx(n, i, i)].x);
+    __syncthreads();
+    const double fl = (double)looks;
+
+    for (int q = t; q < npu; q += EX_THREADS) {
+        const int i = w.tab[q] >> 8, j = w.tab[q] & 255;
+        double2 v = make_double2(1.0, 0.0);
+
+        if (i != j) {
+            const double dd = w.nrm[i] * w.nrm[j];
+            const double2 cs = w.T[q];
+
+            v = make_double2(0.0, 0.0);
+            if (dd > 0.0) {
+                v = make_double2(cs.x / dd, cs.y / dd);
+                if (k.bias && looks > 1) {
+                    const double m2 = v.x * v.x + v.y * v.y;
+                    const double m2c = (fl * m2 - 1.0) / (fl - 1.0);
+                    const double f = (m2 > 0.0 && m2c > 0.0) ? sqrt(m2c / m2) : 0.0;
+
+                    v.x *= f;
+                    v.y *= f;
+                }
+            }
+        }
+        w.T[q] = v;
+        w.G[q] = hypot(v.x, v.y);
+    }
+    __syncthreads();
+}
+
+/* Whether the non-zero coherences link all dates (tcoh.cl:494-513). */
+__device__ bool ex_linked(int n, const ExWs &w)
+{
+    const int t = threadIdx.x;
+
+    for (int i = t; i < n; i += EX_THREADS) {
+        unsigned long long a = 0ull;
+
+        for (int j = 0; j < n; j++)
+            if (j != i && w.G[ex_sym(n, i, j)] != 0.0)
+                a |= 1ull << j;
+        w.adj[i] = a;
+    }
+    __syncthreads();
+    if (t < 32) {
+        const unsigned long long all = n == 64 ? ~0ull : (1ull << n) - 1ull;
+        unsigned long long reached = 1ull, frontier = 1ull;
+
+        for (int it = 0; it < n; it++) {
+            unsigned long long mine = 0ull;
+
+            if ((frontier >> t) & 1ull)
+                mine |= w.adj[t];
+            if (t + 32 < n && ((frontier >> (t + 32)) & 1ull))
+                mine |= w.adj[t + 32];
+            const unsigned lo = __reduce_or_sync(FULL, (unsigned)mine);
+            const unsigned hi = __reduce_or_sync(FULL, (unsigned)(mine >> 32));
+            const unsigned long long nw = (((unsigned long long)hi << 32) | lo) & ~reached;
+
+            if (!nw)
+                break;
+            reached |= nw;
+            frontier = nw;
+        }
+        if (t == 0)
+            w.ints[1] = reached == all;
+    }
+    __syncthreads();
+    return w.ints[1] != 0;
+}
+
+/* |T|^-1 in place of |T| (packed), by the symmetric sweep; false when a
+   pivot's magnitude is not above 1e-5 or n max|inv| >= 1e8 (an eigenvalue
+   may then lie below the pseudo-inverse floor 1e-9). */
+__device__ bool ex_sweep(int n, int npu, const ExWs &w)
+{
+    const int t = threadIdx.x;
+    bool ok = true;
+
+    for (int kp = 0; kp < n; kp++) {
+        const double d = w.G[tc_pidx(n, kp, kp)];
+
+        if (!(fabs(d) > 1.0e-5)) {
+            ok = false;
+            break;
+        }
+        const double id = 1.0 / d;
+
+        for (int j = t; j < n; j += EX_THREADS)
+            w.rrow[j] = w.G[ex_sym(n, kp, j)] * id;
+        __syncthreads();
+        for (int q = t; q < npu; q += EX_THREADS) {
+            const int i = w.tab[q] >> 8, j = w.tab[q] & 255;
+
+            if (i == kp && j == kp)
+                w.G[q] = -id;
+            else if (i == kp)
+                w.G[q] = w.rrow[j];
+            else if (j == kp)
+                w.G[q] = w.rrow[i];
+            else
+                w.G[q] = fma(-w.rrow[i] * d, w.rrow[j], w.G[q]);
+        }
+        __syncthreads();
+    }
+    if (!ok) {
+        __syncthreads();
+        return false;
+    }
+    double mx = 0.0;
+
+    for (int q = t; q < npu; q += EX_THREADS) {
+        const double v = -w.G[q];
+
+        w.G[q] = v;
+        mx = fmax(mx, fabs(v)) + (v == v ? 0.0 : INFINITY);
+    }
+    mx = wmaxd(mx);
+    __syncthreads();
+    if ((t & 31) == 0)
+        w.red[t >> 5] = mx;
+    __syncthreads();
+    mx = fmax(fmax(w.red[0], w.red[1]), fmax(w.red[2], w.red[3]));
+    __syncthreads();
+    return mx <= 1.0e300 && n * mx < 1.0e8;
+}
+
+/* Householder reduction of the packed Hermitian M (w.T) to the real
+   tridiagonal (w.d, w.e), zhetd2 form; reflector k's vector is left in
+   packed row k (entries k + 2 ..; its entry k + 1 is 1) and its scalar in
+   w.tau[k]. */
+__device__ void ex_householder(int n, int npu, const ExWs &w)
+{
+    const int t = threadIdx.x;
+
+    for (int k = 0; k < n - 1; k++) {
+        /* column k below the diagonal: x_r = conj(M_k,r) */
+        double xn2 = 0.0;
+
+        if (t < n - k - 2) {
+            const double2 a = w.T[tc_pidx(n, k, k + 2 + t)];
+
+            xn2 = a.x * a.x + a.y * a.y;
+        }
+        xn2 = ex_sum2(xn2, 0.0, w.red).x;
+        const double2 am = w.T[tc_pidx(n, k, k + 1)];
+        const double ax = am.x, ay = -am.y; /* alpha = x_k+1 */
+        double beta, tr = 0.0, ti = 0.0, sr = 0.0, si = 0.0;
+
+        if (xn2 == 0.0 && ay == 0.0)
+            beta = ax;
+        else {
+            beta = -copysign(sqrt(ax * ax + ay * ay + xn2), ax);
+            tr = (beta - ax) / beta;
+            ti = -ay / beta;
+            const double dr = ax - beta, di = ay, den = dr * dr + di * di;
+
+            sr = dr / den;
+            si = -di / den;
+        }
+        const bool reflect = tr != 0.0 || ti != 0.0;
+
+        if (t < n) {
+            double2 v = make_double2(0.0, 0.0);
+
+            if (t == k + 1)
+                v = make_double2(1.0, 0.0);
+            else if (t > k + 1 && reflect) {
+                const double2 a = w.T[tc_pidx(n, k, t)];
+                const double xr = a.x, xi = -a.y;
+
+                v = make_double2(xr * sr - xi * si, xr * si + xi * sr);
+                w.T[tc_pidx(n, k, t)] = v;
+            }
+            w.v[t] = v;
+        }
+        if (t == 0) {
+            w.d[k] = w.T[tc_pidx(n, k, k)].x;
+            w.e[k] = beta;
+            w.tau[k] = make_double2(tr, ti);
+        }
+        __syncthreads();
+        if (!reflect)
+            continue;
+        /* p = M22 v over rows k+1 .. n-1, two threads per row */
+        const int i = k + 1 + (t >> 1), h = t & 1;
+        double sx = 0.0, sy = 0.0;
+
+        if (i < n)
+            for (int j = k + 1 + h; j < n; j += 2) {
+                const double2 m = ex_m(w.T, n, i, j), v = w.v[j];
+
+                sx = fma(m.x, v.x, fma(-m.y, v.y, sx));
+                sy = fma(m.x, v.y, fma(m.y, v.x, sy));
+            }
+        sx += __shfl_xor_sync(FULL, sx, 1);
+        sy += __shfl_xor_sync(FULL, sy, 1);
+        const double2 wl = make_double2(tr * sx - ti * sy, tr * sy + ti * sx);
+        double pr = 0.0, pi = 0.0;
+
+        if (i < n && h == 0) {
+            const double2 v = w.v[i];
+
+            pr = wl.x * v.x + wl.y * v.y;
+            pi = wl.x * v.y - wl.y * v.x;
+        }
+        const double2 pp = ex_sum2(pr, pi, w.red);
+        const double hr = -0.5 * (tr * pp.x - ti * pp.y), hi = -0.5 * (tr * pp.y + ti * pp.x);
+
+        if (i < n && h == 0) {
+            const double2 v = w.v[i];
+
+            w.w[i] = make_double2(wl.x + hr * v.x - hi * v.y, wl.y + hr * v.y + hi * v.x);
+        }
+        __syncthreads();
+        /* M22 -= v w^H + w v^H over the trailing triangle (contiguous) */
+        for (int q = tc_pidx(n, k + 1, k + 1) + t; q < npu; q += EX_THREADS) {
+            const int r = w.tab[q] >> 8, j = w.tab[q] & 255;
+            const double2 vr = w.v[r], wr = w.w[r], vj = w.v[j], wj = w.w[j];
+            double2 a = w.T[q];
+
+            a.x -= vr.x * wj.x + vr.y * wj.y + wr.x * vj.x + wr.y * vj.y;
+            a.y -= vr.y * wj.x - vr.x * wj.y + wr.y * vj.x - wr.x * vj.y;
+            w.T[q] = a;
+        }
+        __syncthreads();
+    }
+    if (t == 0)
+        w.d[n - 1] = w.T[tc_pidx(n, n - 1, n - 1)].x;
+    __syncthreads();
+}
+
+/* Smallest eigenvalue of (w.d, w.e) by 128-way multisection on double
+   Sturm counts, then its eigenvector by inverse iteration (thread 0), then
+   z = Q y by the reflectors (warp 0): into w.z. Returns status bits. */
+__device__ unsigned ex_eigvec(int n, const ExWs &w)
+{
+    const int t = threadIdx.x;
+    unsigned status = 0;
+    double lo = INFINITY, hi = -INFINITY;
+
+    if (t < n) {
+        const double rad = (t > 0 ? fabs(w.e[t - 1]) : 0.0) + (t < n - 1 ? fabs(w.e[t]) : 0.0);
+
+        lo = w.d[t] - rad;
+        hi = w.d[t] + rad;
+        if (t < n - 1)
+            w.e2[t] = w.e[t] * w.e[t];
+    }
+    {
+        double a = lo, b = hi;
+
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            a = fmin(a, __shfl_xor_sync(FULL, a, o));
+            b = fmax(b, __shfl_xor_sync(FULL, b, o));
+        }
+        __syncthreads();
+        if ((t & 31) == 0) {
+            w.red[t >> 5] = a;
+            w.red[4 + (t >> 5)] = b;
+        }
+        __syncthreads();
+        lo = fmin(fmin(w.red[0], w.red[1]), fmin(w.red[2], w.red[3]));
+        hi = fmax(fmax(w.red[4], w.red[5]), fmax(w.red[6], w.red[7]));
+        __syncthreads();
+    }
+    const double norm = fmax(fabs(lo), fabs(hi));
+
+    lo -= 1.0e-12 * norm + 1e-300;
+    hi += 1.0e-12 * norm + 1e-300;
+    const double pivmin = 1e-290 + 1e-28 * norm;
+    int round = 0;
+
+    for (; round < 12; round++) {
+        if (hi - lo <= 2.0e-15 * norm)
+            break;
+        const double xq = lo + (hi - lo) * ((double)(t + 1) / (double)(EX_THREADS + 1));
+        const bool gt = sturmd(w.d, w.e2, n, xq, pivmin) > 0;
+        const unsigned bal = __ballot_sync(FULL, gt);
+
+        if ((t & 31) == 0)
+            w.ints[2 + (t >> 5)] = bal ? (t & ~31) + __ffs(bal) - 1 : EX_THREADS;
+        __syncthreads();
+        const int f = min(min(w.ints[2], w.ints[3]), min(w.ints[4], w.ints[5]));
+        double nlo, nhi;
+
+        if (f == EX_THREADS) {
+            nlo = lo + (hi - lo) * ((double)EX_THREADS / (double)(EX_THREADS + 1));
+            nhi = hi;
+        }
+        else {
+            nhi = lo + (hi - lo) * ((double)(f + 1) / (double)(EX_THREADS + 1));
+            nlo = f == 0 ? lo : lo + (hi - lo) * ((double)f / (double)(EX_THREADS + 1));
+        }
+        __syncthreads();
+        if (!(nlo > lo || nhi < hi))
+            break;
+        lo = fmax(nlo, lo);
+        hi = fmin(nhi, hi);
+    }
+    if (round == 12)
+        status |= TC_STATUS_ITER_CAP;
+    const double lambda = 0.5 * (lo + hi);
+
+    /* Inverse iteration: LU of T - lambda I with partial pivoting, three
+       solves from a vector of ones (the method of tcoh.cl:342-410). */
+    if (t == 0) {
+        const double tiny = 1.0e-13 * (norm > 1e-300 ? norm : 1e-300);
+        double *lu = w.lu, *y = w.y;
+        unsigned long long piv = 0ull;
+        double dd = w.d[0] - lambda, s1 = n > 1 ? w.e[0] : 0.0;
+
+        for (int kk = 0; kk < n - 1; kk++) {
+            const double sub = w.e[kk], nd = w.d[kk + 1] - lambda;
+            const double ns = kk + 1 < n - 1 ? w.e[kk + 1] : 0.0;
+
+            if (fabs(dd) >= fabs(sub)) {
+                if (fabs(dd) < tiny)
+                    dd = dd < 0.0 ? -tiny : tiny;
+                const double rd = 1.0 / dd, l = sub * rd;
+
+                lu[4 * kk] = rd;
+                lu[4 * kk + 1] = s1;
+                lu[4 * kk + 2] = 0.0;
+                lu[4 * kk + 3] = l;
+                dd = nd - l * s1;
+                s1 = ns;
+            }
+            else {
+                const double rs = 1.0 / sub, l = dd * rs;
+
+                piv |= 1ull << kk;
+                lu[4 * kk] = rs;
+                lu[4 * kk + 1] = nd;
+                lu[4 * kk + 2] = ns;
+                lu[4 * kk + 3] = l;
+                dd = s1 - l * nd;
+                s1 = -l * ns;
+            }
+        }
+        if (fabs(dd) < tiny)
+            dd = dd < 0.0 ? -tiny : tiny;
+        lu[4 * (n - 1)] = 1.0 / dd;
+        lu[4 * (n - 1) + 1] = 0.0;
+        lu[4 * (n - 1) + 2] = 0.0;
+        for (int kk = 0; kk < n; kk++)
+            y[kk] = 1.0;
+        for (int it = 0; it < 3; it++) {
+            double nrm = 0.0;
+
+            for (int kk = 0; kk < n - 1; kk++) {
+                if ((piv >> kk) & 1ull) {
+                    const double tmp = y[kk];
+
+                    y[kk] = y[kk + 1];
+                    y[kk + 1] = tmp;
+                }
+                y[kk + 1] -= lu[4 * kk + 3] * y[kk];
+            }
+            for (int kk = n - 1; kk >= 0; kk--) {
+                double v = y[kk];
+
+                if (kk + 1 < n)
+                    v -= lu[4 * kk + 1] * y[kk + 1];
+                if (kk + 2 < n)
+                    v -= lu[4 * kk + 2] * y[kk + 2];
+                y[kk] = v * lu[4 * kk];
+                nrm = fmax(nrm, fabs(y[kk]));
+            }
+            const double inv = 1.0 / nrm;
+
+            for (int kk = 0; kk < n; kk++)
+                y[kk] *= inv;
+        }
+    }
+    __syncthreads();
+    /* z = H_0 ... H_n-2 y (warp 0, rows lane and lane + 32) */
+    if (t < 32) {
+        double2 z[2];
+
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int r = t + 32 * q;
+
+            z[q] = make_double2(r < n ? w.y[r] : 0.0, 0.0);
+        }
+        for (int kk = n - 2; kk >= 0; kk--) {
+            const double2 ta = w.tau[kk];
+
+            if (ta.x == 0.0 && ta.y == 0.0)
+                continue;
+            double sr = 0.0, si = 0.0;
+            double2 vq[2];
+
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const int r = t + 32 * q;
+
+                vq[q] = make_double2(0.0, 0.0);
+                if (r == kk + 1)
+                    vq[q] = make_double2(1.0, 0.0);
+                else if (r > kk + 1 && r < n)
+                    vq[q] = w.T[tc_pidx(n, kk, r)];
+                sr += vq[q].x * z[q].x + vq[q].y * z[q].y;
+                si += vq[q].x * z[q].y - vq[q].y * z[q].x;
+            }
+            sr = wsum<double>(sr);
+            si = wsum<double>(si);
+            const double hr = ta.x * sr - ta.y * si, hi2 = ta.x * si + ta.y * sr;
+
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                z[q].x -= vq[q].x * hr - vq[q].y * hi2;
+                z[q].y -= vq[q].x * hi2 + vq[q].y * hr;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int r = t + 32 * q;
+
+            if (r < n)
+                w.z[r] = z[q];
+        }
+    }
+    __syncthreads();
+    return status;
+}
+
+/* Unit phasors relative to the median date (tcoh.cl:700-724) into w.zs
+   (warp 0), then gamma over the pairs (tcoh.cl:728-744), every thread. */
+__device__ float ex_gamma(int n, int npu, const ExWs &w)
+{
+    const int t = threadIdx.x;
+
+    if (t < 32) {
+        double m[2];
+
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int r = t + 32 * q;
+
+            m[q] = r < n ? hypot(w.z[r].x, w.z[r].y) : 0.0;
+        }
+        double mx = fmax(m[0], m[1]);
+
+        mx = wmaxd(mx);
+        int ref = n / 2;
+
+        if (hypot(w.z[ref].x, w.z[ref].y) <= 1.0e-3 * mx) {
+            int last = -1;
+
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const int r = t + 32 * q;
+
+                if (r < n && m[q] == mx)
+                    last = max(last, r);
+            }
+#pragma unroll
+            for (int o = 16; o; o >>= 1)
+                last = max(last, __shfl_xor_sync(FULL, last, o));
+            ref = last;
+        }
+        const double2 zr = w.z[ref];
+        const double refm = hypot(zr.x, zr.y);
+        const double refr = zr.x / refm, refi = -zr.y / refm, floor_ = 1.0e-3 * mx;
+
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int r = t + 32 * q;
+
+            if (r < n) {
+                const double2 z = w.z[r];
+                const double re = z.x * refr - z.y * refi, im = z.x * refi + z.y * refr;
+                const double mm = hypot(re, im);
+
+                w.zs[r] = mm > floor_ ? make_float2((float)(re / mm), (float)(im / mm))
+                                      : make_float2(1.f, 0.f);
+            }
+        }
+    }
+    __syncthreads();
+    float sr = 0.f, si = 0.f;
+
+    for (int q = t; q < npu; q += EX_THREADS) {
+        const int i = w.tab[q] >> 8, j = w.tab[q] & 255;
+
+        if (i == j)
+            continue;
+        const float2 tv = w.Tf[q];
+        const float m2 = tv.x * tv.x + tv.y * tv.y;
+        float ur = 1.f, ui = 0.f;
+
+        if (m2 > 0.f) {
+            const float r = rsqrtf(m2);
+
+            ur = tv.x * r;
+            ui = tv.y * r;
+        }
+        const float2 zi = w.zs[i], zj = w.zs[j];
+        const float wr = zi.x * zj.x + zi.y * zj.y, wi = zi.x * zj.y - zi.y * zj.x;
+
+        sr += ur * wr - ui * wi;
+        si += ur * wi + ui * wr;
+    }
+    const double2 ssum = ex_sum2(sr, si, w.red);
+
+    return (float)(hypot(ssum.x, ssum.y) / (0.5 * n * (n - 1)));
+}
+
+/* list: null for every pixel of the chunk, else list[0] pixels list[1 ..]. */
+__global__ void __launch_bounds__(EX_THREADS, EX_CTAS)
+tc_link_exact_kernel(TcStrip s, TcChunk c, TcLinkConst k, ExLayout L,
+                     const float2 *__restrict__ slc, const uint32_t *__restrict__ mask,
+                     const int *__restrict__ count, const int *__restrict__ list,
+                     const unsigned short *__restrict__ upper_tab,
+                     const unsigned short *__restrict__ pair_tab, double *__restrict__ scratch,
+                     float *__restrict__ coh, float *__restrict__ pairs,
+                     float *__restrict__ phases, unsigned char *__restrict__ status)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const ExWs w = ex_ws(smem, L);
+    const int n = s.n, npu = L.npu, t = threadIdx.x, ld = L.ld;
+    const long long plane = (long long)s.rows * s.cols;
+    double *W = scratch + (size_t)blockIdx.x * (2 * n * ld + 64);
+
+    for (int q = t; q < npu; q += EX_THREADS)
+        w.tab[q] = upper_tab[q];
+    if (t == 0) {
+        const int rp = (n + 1) / 2, cg = (n + EX_BC - 1) / EX_BC;
+        int b = 0;
+
+        for (int ip = 0; ip < rp; ip++)
+            for (int jg = (2 * ip) / EX_BC; jg < cg; jg++)
+                w.blk[b++] = (unsigned short)(ip << 8 | jg);
+    }
+    __syncthreads();
+    const int total = list ? list[0] : c.npix;
+
+    for (int it = blockIdx.x; it < total; it += gridDim.x) {
+        const int p = list ? list[1 + it] : it;
+        int y, x;
+
+        tc_pixel_yx(c, p, y, x);
+        if (y >= c.row0 + c.nrows || y >= s.rows || x >= s.cols)
+            continue;
+        const long long out = (long long)y * s.cols + x;
+        const int looks = count[out];
+
+        if (looks < k.min_looks) {
+            if (t == 0)
+                coh[out] = NAN;
+            for (int q = t; q < k.npairs; q += EX_THREADS)
+                pairs[q * plane + out] = NAN;
+            if (phases)
+                for (int r = t; r < n; r += EX_THREADS)
+                    phases[out * n + r] = NAN;
+            if (status && t == 0)
+                status[out] = 0;
+            continue;
+        }
+        const int ncand = ex_candidates(s, c, mask, p, w);
+
+        ex_gram(s, slc, y, x, ncand, w, L);
+        ex_coherence(n, npu, k, looks, w);
+        for (int q = t; q < k.npairs; q += EX_THREADS) {
+            const int i = pair_tab[q] >> 8, j = pair_tab[q] & 255;
+
+            pairs[q * plane + out] = (float)w.G[tc_pidx(n, i, j)];
+        }
+        if (k.bias && !ex_linked(n, w)) {
+            if (t == 0)
+                coh[out] = NAN;
+            if (phases)
+                for (int r = t; r < n; r += EX_THREADS)
+                    phases[out * n + r] = NAN;
+            if (status && t == 0)
+                status[out] = TC_STATUS_UNLINKED;
+            __syncthreads();
+            continue;
+        }
+        unsigned st = TC_STATUS_FP64;
+
+        if (!ex_sweep(n, npu, w)) {
+            /* the pseudo-inverse, on warp 0, in full storage in global
+               scratch: |T| again from T */
+            st |= TC_STATUS_EMI_PINV;
+            if (t < 32) {
+                double *V = W + n * ld, *lam = W + 2 * n * ld;
+
+                for (int r = t; r < n; r += 32)
+                    for (int j = 0; j < n; j++) {
+                        const double2 v = ex_m(w.T, n, r, j);
+
+                        W[r * ld + j] = r == j ? 1.0 : hypot(v.x, v.y);
+                    }
+                __syncwarp();
+                st |= jacobi_pinv(n, ld, W, V, lam, t);
+                for (int r = t; r < n; r += 32)
+                    for (int j = r; j < n; j++)
+                        w.G[tc_pidx(n, r, j)] = W[r * ld + j];
+            }
+            __syncthreads();
+        }
+        /* M = |T|^-1 o T in place of T; T in float in place of |T|^-1 */
+        for (int q = t; q < npu; q += EX_THREADS) {
+            const double g = w.G[q];
+            const double2 v = w.T[q];
+
+            w.T[q] = make_double2(g * v.x, g * v.y);
+            w.Tf[q] = make_float2((float)v.x, (float)v.y);
+        }
+        __syncthreads();
+        ex_householder(n, npu, w);
+        st |= ex_eigvec(n, w);
+        const float gamma = ex_gamma(n, npu, w);
+
+        if (t == 0)
+            coh[out] = gamma;
+        if (phases)
+            for (int r = t; r < n; r += EX_THREADS) {
+                const float2 u = w.zs[r];
+
+                phases[out * n + r] = atan2f(u.y, u.x);
+            }
+        if (status && t == 0)
+            status[out] = (unsigned char)st;
+        __syncthreads();
     }
 }
 
@@ -1096,21 +1880,74 @@ LinkLayout layout_for(int n, int emi, bool regs)
 
 } // namespace
 
+static size_t exact_scratch_bytes(int n, int sms)
+{
+    /* per CTA: |T| and the Jacobi eigenvectors in full storage, and the
+       eigenvalues, for the pseudo-inverse tier */
+    return (size_t)sms * EX_CTAS * (2 * n * (n | 1) + 64) * sizeof(double);
+}
+
+static cudaError_t launch_exact(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
+                                const float *slc, const uint32_t *mask, const int *count,
+                                const int *list, const unsigned short *upper_tab,
+                                const unsigned short *pair_tab, double *scratch, float *coh,
+                                float *pairs, float *phases, unsigned char *status, int sms,
+                                cudaStream_t st)
+{
+    const ExLayout L = ex_layout(s.n, s.area);
+    const int ctas = sms * EX_CTAS;
+    const int blocks = list ? ctas : (c.npix < ctas ? c.npix : ctas);
+    cudaError_t e = cudaFuncSetAttribute(tc_link_exact_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, L.bytes);
+
+    if (e != cudaSuccess)
+        return e;
+    tc_link_exact_kernel<<<blocks, EX_THREADS, L.bytes, st>>>(
+        s, c, k, L, (const float2 *)slc, mask, count, list, upper_tab, pair_tab, scratch, coh,
+        pairs, phases, status);
+    return cudaGetLastError();
+}
+
+bool tc_link_needs_gram(int n, int emi)
+{
+    return n <= 32 || !emi;
+}
+
 size_t tc_link_scratch_bytes(int n, int sms)
 {
-    return tc_link_half_scratch_bytes(n, sms);
+    /* the 32-date kernel and the exact tier run one after the other */
+    const size_t a = tc_link_half_scratch_bytes(n, sms), b = exact_scratch_bytes(n, sms);
+
+    return a > b ? a : b;
 }
 
 cudaError_t tc_launch_link(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
-                           const float2 *gram, const int *count,
+                           const float2 *gram, const float *slc, const uint32_t *mask,
+                           const int *count, int *exact_list,
                            const unsigned short *upper_tab, const unsigned short *pair_tab,
                            double *scratch, float *coh, float *pairs, float *phases,
                            unsigned char *status, int sms, cudaStream_t st)
 {
-    if (s.n <= 32)
-        return tc_launch_link_half(s, c, k, gram, count, upper_tab, pair_tab, scratch, coh,
-                                   pairs, phases, status, sms, st);
-    const LinkLayout L = layout_for(s.n, k.emi, false);
+    cudaError_t e;
+
+    if (k.emi && !exact_list)
+        return cudaErrorInvalidValue;
+    if (s.n <= 32) {
+        if (k.emi && (e = cudaMemsetAsync(exact_list, 0, sizeof(int), st)) != cudaSuccess)
+            return e;
+        if ((e = tc_launch_link_half(s, c, k, gram, count, upper_tab, pair_tab, scratch, coh,
+                                     pairs, phases, status, k.emi ? exact_list : nullptr, sms,
+                                     st)) != cudaSuccess)
+            return e;
+        if (!k.emi)
+            return cudaSuccess;
+        return launch_exact(s, c, k, slc, mask, count, exact_list, upper_tab, pair_tab, scratch,
+                            coh, pairs, phases, status, sms, st);
+    }
+    if (k.emi)
+        return launch_exact(s, c, k, slc, mask, count, nullptr, upper_tab, pair_tab, scratch, coh,
+                            pairs, phases, status, sms, st);
+    const LinkLayout L = layout_for(s.n, 0, false);
     const size_t per_warp = (size_t)L.per_warp * sizeof(double);
     int wpb = (int)((227 * 1024) / per_warp);
 
@@ -1121,9 +1958,9 @@ cudaError_t tc_launch_link(const TcStrip &s, const TcChunk &c, const TcLinkConst
     const size_t smem = per_warp * wpb;
     const int want = (c.npix + wpb - 1) / wpb;
     const int blocks = want < sms ? want : sms;
-    cudaError_t e = cudaFuncSetAttribute(tc_link_smem_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 
+    e = cudaFuncSetAttribute(tc_link_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
     if (e == cudaSuccess)
         tc_link_smem_kernel<<<blocks, wpb * 32, smem, st>>>(
             s, c, k, L, gram, count, upper_tab, pair_tab, scratch, coh, pairs, phases, status);

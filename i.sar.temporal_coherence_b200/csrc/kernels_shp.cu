@@ -157,17 +157,28 @@ tc_shp_kernel(TcStrip s, TcChunk c, TcShpConst k, const float *__restrict__ amp,
                         /* Merge walk, centre first on ties: 2N - 1 steps.
                            Both series end in an INFINITY sentinel, so a
                            side that ran out is never taken without bound
-                           checks; after step j, ib = j - ia. */
+                           checks. The heads of both series stay in
+                           registers and each step loads one value, the
+                           next one of the side it took (one shared load
+                           per step instead of two). */
                         const float *bl = b_s + lane;
-                        int ia = 0;
+                        int ia = 0, ib = 0;
+                        float av = a_s[0], bv = bl[0];
 
                         if (TEST == 0) {
                             int d = 0;
 
 #pragma unroll 4
                             for (int j = 1; j < 2 * n; j++) {
-                                ia += a_s[ia] <= bl[(j - 1 - ia) * 32];
-                                d = max(d, abs(2 * ia - j));
+                                const bool ta = av <= bv;
+
+                                ia += ta;
+                                ib += !ta;
+                                const float v = *(ta ? a_s + ia : bl + ib * 32);
+
+                                av = ta ? v : av;
+                                bv = ta ? bv : v;
+                                d = max(d, abs(ia - ib));
                             }
                             ok = d <= k.ks_max;
                         }
@@ -177,7 +188,14 @@ tc_shp_kernel(TcStrip s, TcChunk c, TcShpConst k, const float *__restrict__ amp,
 
 #pragma unroll 4
                             for (int j = 1; j < 2 * n; j++, tj += n + 1) {
-                                ia += a_s[ia] <= bl[(j - 1 - ia) * 32];
+                                const bool ta = av <= bv;
+
+                                ia += ta;
+                                ib += !ta;
+                                const float v = *(ta ? a_s + ia : bl + ib * 32);
+
+                                av = ta ? v : av;
+                                bv = ta ? bv : v;
                                 acc = __fadd_rn(acc, tj[ia]);
                             }
                             ok = __fdiv_rn(__fsub_rn(__fmul_rn(k.ad_norm, acc), 1.0f),

@@ -90,6 +90,8 @@ static size_t substrip_bytes(const struct settings *s, int padded_cols, int cols
     b += up256(sizeof(float2) * (size_t)tc_npu(s->ndates) * npix);
     if (s->npairs)
         b += up256(sizeof(float) * (size_t)s->npairs * mr * cols);
+    if (s->emi)
+        b += up256(sizeof(int) * (npix + 1)); /* the exact tier's pixel list */
     return b;
 }
 
@@ -210,7 +212,13 @@ TC_API int tc_run_device_static(const struct settings *s, int padded_cols, const
         float2 *gram = (float2 *)q;
 
         q += up256(sizeof(float2) * (size_t)tc_npu(n) * c.npix);
-        float *spairs = s->npairs ? (float *)q : nullptr;
+        float *spairs = nullptr;
+
+        if (s->npairs) {
+            spairs = (float *)q;
+            q += up256(sizeof(float) * (size_t)s->npairs * m * cols);
+        }
+        int *elist = s->emi ? (int *)q : nullptr;
 
         const float *s_slc = slc + (size_t)r0 * W * n * 2;
         const float *s_amp = amp + (size_t)r0 * W * n;
@@ -223,8 +231,10 @@ TC_API int tc_run_device_static(const struct settings *s, int padded_cols, const
              (e = tc_launch_logstats(ss, s_amp, s_valid, logstat, st)) != cudaSuccess) ||
             (e = tc_launch_shp(ss, c, shp, s_amp, s_valid, logstat, mask, s_count, sms, st)) !=
                 cudaSuccess ||
-            (e = tc_launch_gram_fp32(ss, c, block, soa, mask, gram, st)) != cudaSuccess ||
-            (e = tc_launch_link(ss, c, lk, gram, s_count, upper, ptab, lscr, s_coh, spairs,
+            (tc_link_needs_gram(n, s->emi) &&
+             (e = tc_launch_gram_fp32(ss, c, block, soa, mask, gram, st)) != cudaSuccess) ||
+            (e = tc_launch_link(ss, c, lk, gram, s_slc, mask, s_count, elist, upper, ptab, lscr,
+                                s_coh, spairs,
                                 phases ? phases + (size_t)r0 * cols * n : nullptr,
                                 status ? status + (size_t)r0 * cols : nullptr, sms, st)) !=
                 cudaSuccess)

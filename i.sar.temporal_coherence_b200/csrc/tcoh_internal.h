@@ -88,14 +88,77 @@ struct TcOrbitSet {
     const double *t, *pos, *vel;
 };
 
+/* The phase grid on the device, in coefficient form: for every node and
+   date, phase(h) = c0 + u (c1 + u c2) with u = h - (the middle height level)
+   is the quadratic through the node's phases at the three height levels
+   (c1 = c2 = 0 with one level), double [grid_rows][grid_cols][ndates][3].
+   Interpolation between nodes is bilinear in line and sample, every 16 of
+   each; with linear interpolation commuting with the polynomial, this is
+   the reference's bilinear-then-quadratic interpolation (geometry.c:256-291)
+   evaluated in another order. */
+#define TC_GEO_STEP 16
+
+struct TcGridCell {
+    const double *q00, *q01, *q10, *q11;
+    double w00, w01, w10, w11, u;
+    bool quad;
+
+    /* phase of date k, and its height derivative when dh is not null */
+    __device__ __forceinline__ double phase(int k, double *dh) const
+    {
+        const double *a = q00 + 3 * k, *b = q01 + 3 * k, *c = q10 + 3 * k, *d = q11 + 3 * k;
+        const double c0 = w00 * a[0] + w01 * b[0] + w10 * c[0] + w11 * d[0];
+
+        if (!quad) {
+            if (dh)
+                *dh = 0.0;
+            return c0;
+        }
+        const double c1 = w00 * a[1] + w01 * b[1] + w10 * c[1] + w11 * d[1];
+        const double c2 = w00 * a[2] + w01 * b[2] + w10 * c[2] + w11 * d[2];
+
+        if (dh)
+            *dh = c1 + 2.0 * u * c2;
+        return c0 + u * (c1 + u * c2);
+    }
+};
+
+/* Region cell (row, col) at height h (the grid covers it: row, col >= 0). */
+__host__ __device__ inline TcGridCell tc_grid_cell(const TcGeo &g, const double *coef, int row,
+                                                   int col, double h)
+{
+    TcGridCell c;
+    const int gr = row / TC_GEO_STEP, gc = col / TC_GEO_STEP, n = g.ndates;
+    const double fr = (double)(row - gr * TC_GEO_STEP) / TC_GEO_STEP;
+    const double fc = (double)(col - gc * TC_GEO_STEP) / TC_GEO_STEP;
+    const size_t node = (size_t)3 * n;
+
+    c.q00 = coef + ((size_t)gr * g.grid_cols + gc) * node;
+    c.q01 = c.q00 + node;
+    c.q10 = c.q00 + (size_t)g.grid_cols * node;
+    c.q11 = c.q10 + node;
+    c.w00 = (1.0 - fr) * (1.0 - fc);
+    c.w01 = (1.0 - fr) * fc;
+    c.w10 = fr * (1.0 - fc);
+    c.w11 = fr * fc;
+    c.quad = g.nheights == 3;
+    c.u = c.quad ? h - g.heights[1] : 0.0;
+    return c;
+}
+
 int tc_geometry_shape(const struct tc_geometry &in, TcGeo &g);
 int tc_geometry_grid(const TcGeo &g, const struct tc_orbit *orbits, double *grid_host,
                      cudaStream_t st);
+/* The coefficient form of a phase grid (device, as tc_geometry_grid writes
+   it: double [grid_rows][grid_cols][nheights][ndates]) into coef. */
+cudaError_t tc_launch_geometry_coef(const TcGeo &g, const double *grid, double *coef,
+                                    cudaStream_t st);
+/* Strip preparation from raw planes for padded rows prow0 .. prow1 - 1. */
 cudaError_t tc_launch_prep_raw(int n, const float *re, const float *im, const double *elev,
                                int row0, int region_rows, int padded_rows, int cols, int halo,
-                               const TcGeo *g, const double *grid, const double *dh,
-                               const float *psi, float *slc, float *amp, unsigned char *valid,
-                               cudaStream_t st);
+                               int prow0, int prow1, const TcGeo *g, const double *grid,
+                               const double *dh, const float *psi, float *slc, float *amp,
+                               unsigned char *valid, cudaStream_t st);
 /* Adjoint (adjoint.cu): dL/dtheta += the chunk's contribution (dtheta
    [n][padded_rows][cols], zeroed by the caller); dL/ddh from dL/dtheta. */
 cudaError_t tc_launch_adjoint_scatter(const TcStrip &s, const TcChunk &c, int halo,
@@ -140,17 +203,26 @@ cudaError_t tc_launch_adjoint_scatter_tensor(const TcStrip &s, const TcChunk &c,
                                              const float2 *gbar, const uint32_t *mask,
                                              const float *slc, float *dtheta, cudaStream_t st);
 int tc_gram_block_for(int n);
+/* The link stage: phase linking and gamma of every pixel of a chunk from its
+   coherence sums (gram), or, for EMI, from the samples (slc, AoS) and SHP
+   masks in double precision where float sums are not accurate enough:
+   every pixel above 32 dates (the Gram stage is then skipped, see
+   tc_link_needs_gram), the ill-conditioned ones up to 32 dates. exact_list
+   holds 1 + npix ints of device memory (EMI; null otherwise). */
 cudaError_t tc_launch_link(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
-                           const float2 *gram, const int *count,
+                           const float2 *gram, const float *slc, const uint32_t *mask,
+                           const int *count, int *exact_list,
                            const unsigned short *upper_tab, const unsigned short *pair_tab,
                            double *scratch, float *coh, float *pairs, float *phases,
                            unsigned char *status, int sms, cudaStream_t st);
+bool tc_link_needs_gram(int n, int emi);
 size_t tc_link_scratch_bytes(int n, int sms);
 cudaError_t tc_launch_link_half(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
                                 const float2 *gram, const int *count,
                                 const unsigned short *upper_tab, const unsigned short *pair_tab,
                                 double *scratch, float *coh, float *pairs, float *phases,
-                                unsigned char *status, int sms, cudaStream_t st);
+                                unsigned char *status, int *exact_list, int sms,
+                                cudaStream_t st);
 size_t tc_link_half_scratch_bytes(int n, int sms);
 /* The link stage with the adjoint (n <= 32): gamma into coh, and into gbar
    (layout of gram) the gradient of gamma with respect to each pixel's

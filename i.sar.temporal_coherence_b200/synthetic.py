@@ -15,6 +15,9 @@ the SHP tests are exercised.
 
 ``generate`` works in numpy (small stacks) or in torch on a GPU (large
 ones); both are deterministic for a given seed, but they draw differently.
+The torch form draws every band of rows from a generator of its own, so
+that a range of rows of a scene too large for the device (``row_range``)
+is the same whether it is generated alone or with the whole scene.
 """
 
 import numpy as np
@@ -43,9 +46,10 @@ def coherence_model(n, spacing, g0, ginf, tau):
 
 
 def generate(n, rows, cols, nregions=8, g0_max=0.95, spacing=12.0, seed=0, null_frac=0.005,
-             device=None, scale=300.0):
+             device=None, scale=300.0, row_range=None):
     """Stack (n, rows, cols) complex64 (NaN = NULL), as numpy, or as a torch
-    tensor on `device` when given."""
+    tensor on `device` when given; with row_range = (a, b) (torch only),
+    rows a .. b - 1 of that scene, (n, b - a, cols)."""
     rng = np.random.default_rng(seed)
     sy, sx = _regions(rng, nregions, rows, cols)
     par = region_params(rng, nregions, g0_max)
@@ -59,10 +63,12 @@ def generate(n, rows, cols, nregions=8, g0_max=0.95, spacing=12.0, seed=0, null_
     null_date = rng.integers(0, n, nnull)
     null_zero = rng.random(nnull) < 0.5
     if device is None:
+        if row_range is not None:
+            raise ValueError("row_range needs the torch form (device)")
         return _generate_numpy(rng, n, rows, cols, sy, sx, par, chol, fy, fx, null_pix,
                                null_date, null_zero, scale)
     return _generate_torch(seed, n, rows, cols, sy, sx, par, chol, fy, fx, null_pix,
-                           null_date, null_zero, scale, device)
+                           null_date, null_zero, scale, device, row_range)
 
 
 def _ramp(n, rows, cols, fy, fx, y, x):
@@ -86,20 +92,23 @@ def _generate_numpy(rng, n, rows, cols, sy, sx, par, chol, fy, fx, null_pix, nul
 
 
 def _generate_torch(seed, n, rows, cols, sy, sx, par, chol, fy, fx, null_pix, null_date,
-                    null_zero, scale, device):
+                    null_zero, scale, device, row_range=None):
     import torch
 
+    a, b = (0, rows) if row_range is None else (int(row_range[0]), int(row_range[1]))
+    if not 0 <= a <= b <= rows:
+        raise ValueError("row range %r of %d rows" % ((a, b), rows))
     g = torch.Generator(device=device)
-    g.manual_seed(int(seed))
-    out = torch.empty((n, rows, cols), dtype=torch.complex64, device=device)
+    out = torch.empty((n, b - a, cols), dtype=torch.complex64, device=device)
     sy_t = torch.tensor(sy, device=device, dtype=torch.float32)
     sx_t = torch.tensor(sx, device=device, dtype=torch.float32)
     chol_t = torch.tensor(chol, device=device, dtype=torch.complex64)
     sigma = torch.tensor(par["sigma"], device=device, dtype=torch.float32)
     k = torch.arange(n, device=device, dtype=torch.float64)[:, None]
     band = max(1, (1 << 21) // max(cols, 1))
-    for r0 in range(0, rows, band):
+    for r0 in range(a // band * band, b, band):
         r1 = min(rows, r0 + band)
+        g.manual_seed(int(seed) * 1000003 + r0 // band)
         yy, xx = torch.meshgrid(torch.arange(r0, r1, device=device, dtype=torch.float32),
                                 torch.arange(cols, device=device, dtype=torch.float32),
                                 indexing="ij")
@@ -118,9 +127,14 @@ def _generate_torch(seed, n, rows, cols, sy, sx, par, chol, fy, fx, null_pix, nu
                                                 fx * xx.double()[None, :] / cols)
         s = lz * torch.polar(torch.ones_like(ramp), ramp).to(torch.complex64)
         s = torch.complex(torch.round(s.real * scale), torch.round(s.imag * scale))
-        out[:, r0:r1] = s.reshape(n, r1 - r0, cols)
-    flat = out.view(n, -1)
-    vals = torch.tensor(np.where(null_zero, 0.0, np.nan), device=device, dtype=torch.float32)
-    flat[torch.tensor(null_date, device=device), torch.tensor(null_pix, device=device)] = \
-        torch.complex(vals, vals)
+        s = s.reshape(n, r1 - r0, cols)
+        lo, hi = max(a, r0), min(b, r1)
+        out[:, lo - a:hi - a] = s[:, lo - r0:hi - r0]
+    keep = (null_pix >= a * cols) & (null_pix < b * cols)
+    if keep.any():
+        flat = out.view(n, -1)
+        vals = torch.tensor(np.where(null_zero[keep], 0.0, np.nan), device=device,
+                            dtype=torch.float32)
+        flat[torch.tensor(null_date[keep], device=device),
+             torch.tensor(null_pix[keep] - a * cols, device=device)] = torch.complex(vals, vals)
     return out

@@ -105,6 +105,12 @@ struct tc_options {
                                   inverted by its eigen-pseudo-inverse */
 #define TC_STATUS_UNLINKED   2 /* bias correction unlinked the dates */
 #define TC_STATUS_ITER_CAP   4 /* an iterative solver reached its cap */
+#define TC_STATUS_FP64       8 /* EMI: recomputed from double-precision
+                                  coherence sums (every pixel above 32
+                                  dates; up to 32 dates, the pixels whose
+                                  float result the conditioning of |T| and
+                                  of M's eigengap may have moved by more
+                                  than ~1e-5) */
 
 /* Message of the last failed tc_* call of this thread. */
 const char *tc_last_error(void);
@@ -248,6 +254,11 @@ int tc_close(struct ocl *o);
 /* Measured FP32 FMA throughput of device `device` in TFLOP/s (two flops per
    FMA), the roofline denominator of the kernels on the CUDA cores. */
 int tc_fp32_peak(int device, double *tflops);
+
+/* The same in double precision: the denominator of the kernels that
+   compute in FP64 (the EMI exact tier, the geometry grid, the raw strip
+   preparation). */
+int tc_fp64_peak(int device, double *tflops);
 
 /* tc_run_device for callers that must not allocate device memory: no
    context, no cudaMalloc, on the current device and `stream` (NULL: CUDA's

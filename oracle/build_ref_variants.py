@@ -12,7 +12,8 @@ constant trip counts. The generic oracle/_ref/libtcoh_ref*.so turn those
 constants into run-time globals; the libraries built here are the faithful
 form: the same tcoh.cl, compiled from the reference checkout where it lies
 (never copied), with the same -D constants, one library per configuration
-of the CPU baseline (the bench's workloads on crops of 512 output columns).
+of the CPU baseline (the bench's workloads on crops of 512 output columns,
+1024 at 60 dates).
 oracle.run_reference picks the library of a strip's configuration when it
 exists, else the generic one.
 
@@ -38,8 +39,8 @@ VARIANTS = [
     (30, (21, 7), 512, "ad", 0.05, "emi", True, 20, 0, False),    # the metric's: AD/EMI/-b
     (30, (21, 7), 512, "ad", 0.05, "evd", True, 20, 0, False),
     (30, (21, 7), 512, "tlog", 0.05, "evd", False, 20, 435, True),  # all pair planes
-    (60, (21, 7), 512, "ks", 0.05, "evd", False, 20, 0, False),   # N=60 KS, EVD and EMI
-    (60, (21, 7), 512, "ks", 0.05, "emi", False, 20, 0, False),
+    (60, (21, 7), 1024, "ks", 0.05, "evd", False, 20, 0, False),  # N=60 KS, EVD and EMI
+    (60, (21, 7), 1024, "ks", 0.05, "emi", False, 20, 0, False),  # (1024-column crops)
 ]
 
 

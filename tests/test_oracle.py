@@ -111,21 +111,22 @@ def test_specialised_reference_build_is_the_generic_one(n, test, estimator, bias
 
     kw = dict(window=(21, 7), shp_test=test, alpha=0.05, min_shp=10 if n == 10 else 20,
               estimator=estimator, bias=bias)
-    if oracle.ref_build(n, (21, 7), 518, npairs=0, pairs_all=False,
+    cols = 1024 if n == 60 else 512
+    if oracle.ref_build(n, (21, 7), cols + 6, npairs=0, pairs_all=False,
                         **{k: v for k, v in kw.items() if k != "window"}) != "specialised":
         pytest.skip("the specialised build of this configuration is absent")
-    stack = syn.generate(n, 3, 512, seed=n, g0_max=0.99, spacing=6.0 if n == 60 else 12.0)
+    stack = syn.generate(n, 3, cols, seed=n, g0_max=0.99, spacing=6.0 if n == 60 else 12.0)
     slc, amp, valid = tcoh_b200.read_strip(stack.real, stack.imag, -10, 23, 3)
-    spec = oracle.run_reference(slc, amp, valid, 3, 512, **kw)
+    spec = oracle.run_reference(slc, amp, valid, 3, cols, **kw)
     gen = oracle._ref_lib(False)  # the generic build, called directly
     k = oracle.kernel_constants(n, test, 0.05)
-    coh = np.empty((3, 512), np.float32)
-    count = np.empty((3, 512), np.int32)
-    pairs = np.empty((1, 3, 512), np.float32)
+    coh = np.empty((3, cols), np.float32)
+    count = np.empty((3, cols), np.int32)
+    pairs = np.empty((1, 3, cols), np.float32)
     assert gen.ref_run(n, 21, 7, oracle.TESTS[test], int(estimator == "emi"), int(bias),
                        max(kw["min_shp"], n), k.ks_max, k.ad_norm, k.ad_sigma, k.ad_crit,
                        k.tlog_crit, 0, oracle._ptr(slc), oracle._ptr(amp), oracle._ptr(valid),
-                       23, 518, 3, 512, oracle._ptr(coh), oracle._ptr(count),
+                       23, cols + 6, 3, cols, oracle._ptr(coh), oracle._ptr(count),
                        oracle._ptr(pairs), 0) == 0
     assert np.array_equal(spec["count"], count)
     assert np.array_equal(spec["coh"], coh, equal_nan=True)
