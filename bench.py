@@ -312,6 +312,16 @@ def crop_accuracy(crop, coh_gpu, count_gpu, size, n, kw, flips_size=64):
     o64 = oracle.run_oracle(*fc, fs, fs, shp_fp32=False, **kw)
     out["shp_count_flips_float_vs_fp64"] = {
         "pixels": fs * fs, "flips": int((o["count"][:fs, :fs] != o64["count"]).sum())}
+    # the pixels beyond the tolerance, for the record
+    bad = np.argwhere(m & (np.abs(np.nan_to_num(g - o["coh"])) > 1e-4))
+    out["over_1e-4_pixels"] = [
+        {"row": int(y), "col": int(x), "err": float(abs(g[y, x] - o["coh"][y, x])),
+         "gpu": float(g[y, x]), "oracle": float(o["coh"][y, x]), "status": int(r["status"][y, x]),
+         "looks": int(count_gpu[y, x])} for y, x in bad[:12]]
+    if os.environ.get("TCOH_BENCH_DUMP") and len(bad):
+        np.savez_compressed(os.environ["TCOH_BENCH_DUMP"], slc=crop[0], amp=crop[1],
+                            valid=crop[2], coh_gpu=g, coh_oracle=o["coh"], status=r["status"],
+                            bad=bad, kw=json.dumps(kw))
     return out
 
 

@@ -641,7 +641,7 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
     CK(ensure(o->mask, sizeof(uint32_t) * s.mask_words * max_npix));
     CK(ensure(o->gram, sizeof(float2) * tc_npu(o->n) * max_npix));
     CK(ensure(o->link_scratch, tc_link_scratch_bytes(o->n, o->sms)));
-    if (o->emi)
+    if (o->emi || o->bias)
         CK(ensure(o->exact_list, sizeof(int) * (max_npix + 1)));
     if (o->opt.gram == TC_GRAM_FP32)
         CK(ensure(o->soa, sizeof(float2) * s.planes * s.npad));

@@ -685,12 +685,15 @@ struct PixelCtx {
     long long out, plane;
 };
 
-/* T from the packed Gram sums (tcoh.cl:611-636). */
+/* T from the packed Gram sums (tcoh.cl:611-636); boundary: whether an
+   entry's bias decision lies within TC_BIAS_BAND of its threshold. */
 __device__ void load_coherence(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
                                int p, int looks, const float2 *__restrict__ gram,
                                const unsigned short *__restrict__ upper_tab, const Ws &w,
-                               int ld, int lane)
+                               int ld, int lane, bool &boundary)
 {
+    bool near = false;
+
     const int n = s.n, npu = tc_npu(n);
 
     for (int r = lane; r < n; r += 32)
@@ -714,8 +717,10 @@ __device__ void load_coherence(const TcStrip &s, const TcChunk &c, const TcLinkC
             im = __fdiv_rn(g.y, dd);
             if (k.bias && looks > 1) {
                 const float m2 = __fadd_rn(__fmul_rn(re, re), __fmul_rn(im, im));
-                const float m2c =
-                    __fdiv_rn(__fsub_rn(__fmul_rn(fl, m2), 1.0f), __fsub_rn(fl, 1.0f));
+                const float lm1 = __fsub_rn(__fmul_rn(fl, m2), 1.0f);
+                const float m2c = __fdiv_rn(lm1, __fsub_rn(fl, 1.0f));
+
+                near |= fabsf(lm1) < TC_BIAS_BAND * fl * m2;
                 const float f = (m2 > 0.f && m2c > 0.f) ? __fsqrt_rn(__fdiv_rn(m2c, m2)) : 0.f;
 
                 re = __fmul_rn(re, f);
@@ -725,6 +730,7 @@ __device__ void load_coherence(const TcStrip &s, const TcChunk &c, const TcLinkC
         w.T[i * ld + j] = make_float2(re, im);
         w.T[j * ld + i] = make_float2(re, -im);
     }
+    boundary = __any_sync(FULL, near);
     __syncwarp();
 }
 
@@ -875,7 +881,8 @@ tc_link_smem_kernel(TcStrip s, TcChunk c, TcLinkConst k, LinkLayout L,
                     const unsigned short *__restrict__ upper_tab,
                     const unsigned short *__restrict__ pair_tab, double *__restrict__ scratch,
                     float *__restrict__ coh, float *__restrict__ pairs,
-                    float *__restrict__ phases, unsigned char *__restrict__ status)
+                    float *__restrict__ phases, unsigned char *__restrict__ status,
+                    int *__restrict__ exact_list)
 {
     extern __shared__ double smd[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -906,7 +913,11 @@ tc_link_smem_kernel(TcStrip s, TcChunk c, TcLinkConst k, LinkLayout L,
                 status[out] = 0;
             continue;
         }
-        load_coherence(s, c, k, p, looks, gram, upper_tab, w, ld, lane);
+        bool boundary = false;
+
+        load_coherence(s, c, k, p, looks, gram, upper_tab, w, ld, lane, boundary);
+        if (exact_list && boundary && lane == 0)
+            exact_list[1 + atomicAdd(exact_list, 1)] = p;
         for (int q = lane; q < k.npairs; q += 32) {
             const int i = pair_tab[q] >> 8, j = pair_tab[q] & 255;
             const float2 t = w.T[i * ld + j];
@@ -953,31 +964,35 @@ tc_link_smem_kernel(TcStrip s, TcChunk c, TcLinkConst k, LinkLayout L,
 }
 
 /* ------------------------------------------------------------------ */
-/* The exact tier: EMI from double-precision coherence sums.           */
+/* The exact tier: a pixel from double-precision coherence sums.       */
 /* ------------------------------------------------------------------ */
 
 /* EMI divides by |T|, whose condition number reaches 1e5 - 1e6 on noisy or
    highly coherent stacks: the float rounding of the coherence sums and of
    their normalisation (a few 1e-7 relative) then moves gamma by up to 1e-3,
-   however exactly the rest is computed. This tier recomputes a pixel from
-   its samples with everything in double: the masked sums
+   however exactly the rest is computed. And the bias correction zeroes an
+   entry at L m2 <= 1, a jump of gamma by up to 2 / (n (n - 1)) that float
+   sums may place on the other side of the threshold. This tier recomputes
+   a pixel from its samples with everything in double: the masked sums
    C = sum over SHPs q of s_q s_q^H (tcoh.cl:567-602, as tests/reference.py
-   sums them), T and its bias correction (tcoh.cl:610-636), |T|^-1 (the
-   symmetric sweep, or the Jacobi pseudo-inverse with the absolute floor
-   1e-9 of tests/reference.py:151-156 when a pivot falls below 1e-5 or the
-   inverse is huge), M = |T|^-1 o T, its Householder reduction to a real
-   tridiagonal, the smallest eigenvalue by multisection on Sturm counts,
-   inverse iteration and the back-transformation; then the phasors and
-   gamma (tcoh.cl:696-744). It runs every pixel of the 33-64-date EMI path,
-   and the pixels that the 32-date kernel flags as ill-conditioned.
+   sums them), T and its bias correction (tcoh.cl:610-636); for EMI |T|^-1
+   (ex_inverse: the symmetric sweep, through |T|^2, or the Jacobi
+   pseudo-inverse with the absolute floor 1e-9 of
+   tests/reference.py:151-156) and M = |T|^-1 o T, for EVD T itself; the
+   Householder reduction to a real tridiagonal, the wanted eigenvalue by
+   multisection on Sturm counts, inverse iteration and the
+   back-transformation; then the phasors and gamma (tcoh.cl:696-744). It
+   runs every pixel of the 33-64-date EMI path, and the pixels that the
+   float kernels flag: ill-conditioned EMI pixels up to 32 dates, and with
+   the bias correction any pixel with an entry at its threshold.
 
    One CTA of four warps per pixel, every matrix in packed upper-triangle
    storage (index tc_pidx) in shared memory, so that three pixels fit an
    SM at 60 dates: the sums and T (then M, in place) in complex double,
-   |T| and its inverse in double (then, once M is formed, a float copy of
-   T for gamma in the same place). The sums
-   accumulate in registers, each thread a few 2 x 4 blocks of the
-   triangle, over the SHP samples staged 16 candidates at a time. */
+   |T| and its inverse in double (then a float copy of T for gamma in the
+   same place). The sums accumulate in registers, each thread a few 2 x 4
+   blocks of the triangle, over the SHP samples staged 16 candidates at a
+   time. */
 
 constexpr int EX_THREADS = 128;
 constexpr int EX_CTAS = 3;        /* CTAs per SM */
@@ -1294,51 +1309,61 @@ __device__ bool ex_linked(int n, const ExWs &w)
     return w.ints[1] != 0;
 }
 
-/* |T|^-1 in place of |T| (packed), by the symmetric sweep; false when a
-   pivot's magnitude is not above 1e-5 or n max|inv| >= 1e8 (an eigenvalue
-   may then lie below the pseudo-inverse floor 1e-9). */
-__device__ bool ex_sweep(int n, int npu, const ExWs &w)
+/* A^-1 in place of the packed symmetric A by the symmetric sweep
+   (Gauss-Jordan elimination without pivoting in the form that keeps the
+   matrix symmetric; Goodnight, The American Statistician 33, 1979):
+   sweeping pivot k maps a_ij -> a_ij - a_ik a_kj / a_kk,
+   a_ik, a_kj -> a_ik / a_kk, a_kk -> -1 / a_kk, and all pivots leave
+   -A^-1, negated back at the end. It takes indefinite matrices. False when
+   a pivot's magnitude is not above floor_ (A is then undefined). */
+__device__ bool ex_sweep(int n, int npu, const ExWs &w, double *A, double floor_)
 {
     const int t = threadIdx.x;
-    bool ok = true;
 
     for (int kp = 0; kp < n; kp++) {
-        const double d = w.G[tc_pidx(n, kp, kp)];
+        const double d = A[tc_pidx(n, kp, kp)];
 
-        if (!(fabs(d) > 1.0e-5)) {
-            ok = false;
-            break;
+        if (!(fabs(d) > floor_)) {
+            __syncthreads();
+            return false;
         }
         const double id = 1.0 / d;
 
         for (int j = t; j < n; j += EX_THREADS)
-            w.rrow[j] = w.G[ex_sym(n, kp, j)] * id;
+            w.rrow[j] = A[ex_sym(n, kp, j)] * id;
         __syncthreads();
         for (int q = t; q < npu; q += EX_THREADS) {
             const int i = w.tab[q] >> 8, j = w.tab[q] & 255;
 
             if (i == kp && j == kp)
-                w.G[q] = -id;
+                A[q] = -id;
             else if (i == kp)
-                w.G[q] = w.rrow[j];
+                A[q] = w.rrow[j];
             else if (j == kp)
-                w.G[q] = w.rrow[i];
+                A[q] = w.rrow[i];
             else
-                w.G[q] = fma(-w.rrow[i] * d, w.rrow[j], w.G[q]);
+                A[q] = fma(-w.rrow[i] * d, w.rrow[j], A[q]);
         }
         __syncthreads();
     }
-    if (!ok) {
-        __syncthreads();
-        return false;
-    }
+    for (int q = t; q < npu; q += EX_THREADS)
+        A[q] = -A[q];
+    __syncthreads();
+    return true;
+}
+
+/* Whether the packed inverse is finite and moderate: n max|inv_ij| < 1e8,
+   which keeps every eigenvalue of |T| above the pseudo-inverse floor 1e-9
+   of tests/reference.py:151-156, where the pseudo-inverse is the inverse. */
+__device__ bool ex_moderate(int n, int npu, const ExWs &w, const double *A)
+{
+    const int t = threadIdx.x;
     double mx = 0.0;
 
     for (int q = t; q < npu; q += EX_THREADS) {
-        const double v = -w.G[q];
+        const double v = A[q];
 
-        w.G[q] = v;
-        mx = fmax(mx, fabs(v)) + (v == v ? 0.0 : INFINITY);
+        mx = v == v ? fmax(mx, fabs(v)) : INFINITY;
     }
     mx = wmaxd(mx);
     __syncthreads();
@@ -1348,6 +1373,74 @@ __device__ bool ex_sweep(int n, int npu, const ExWs &w)
     mx = fmax(fmax(w.red[0], w.red[1]), fmax(w.red[2], w.red[3]));
     __syncthreads();
     return mx <= 1.0e300 && n * mx < 1.0e8;
+}
+
+/* Packed symmetric C = A B (A, B packed symmetric, commuting: C symmetric). */
+__device__ void ex_symmul(int n, int npu, const ExWs &w, const double *A, const double *B,
+                          double *C)
+{
+    for (int q = threadIdx.x; q < npu; q += EX_THREADS) {
+        const int i = w.tab[q] >> 8, j = w.tab[q] & 255;
+        double acc = 0.0;
+
+        for (int kk = 0; kk < n; kk++)
+            acc = fma(A[ex_sym(n, i, kk)], B[ex_sym(n, kk, j)], acc);
+        C[q] = acc;
+    }
+    __syncthreads();
+}
+
+/* |T|^-1 into w.G (which holds |T|), in tiers as the 32-date kernel does:
+   the sweep with pivots above 1e-5; else (|T|^2)^-1 |T| (|T|^2 is positive
+   semi-definite, its sweep takes any non-zero pivot) in the CTA's global
+   scratch W; else, or when the inverse is not moderate, the Jacobi
+   eigen-pseudo-inverse with the absolute floor 1e-9
+   (tests/reference.py:151-156) on warp 0. Returns status bits. */
+__device__ unsigned ex_inverse(int n, int npu, int ld, const ExWs &w, double *W)
+{
+    const int t = threadIdx.x;
+
+    if (ex_sweep(n, npu, w, w.G, 1.0e-5) && ex_moderate(n, npu, w, w.G))
+        return 0;
+    double *G2 = W, *P = W + n * ld;
+
+    for (int q = t; q < npu; q += EX_THREADS) {
+        const double2 v = w.T[q];
+        const int i = w.tab[q] >> 8, j = w.tab[q] & 255;
+
+        w.G[q] = i == j ? 1.0 : hypot(v.x, v.y);
+    }
+    __syncthreads();
+    ex_symmul(n, npu, w, w.G, w.G, G2);
+    if (ex_sweep(n, npu, w, G2, 1.0e-300)) {
+        ex_symmul(n, npu, w, G2, w.G, P);
+        for (int q = t; q < npu; q += EX_THREADS)
+            w.G[q] = P[q];
+        __syncthreads();
+        if (ex_moderate(n, npu, w, w.G))
+            return TC_STATUS_EMI_PINV;
+    }
+    unsigned st = TC_STATUS_EMI_PINV;
+
+    if (t < 32) {
+        double *V = W + n * ld, *lam = W + 2 * n * ld;
+
+        for (int r = t; r < n; r += 32)
+            for (int j = 0; j < n; j++) {
+                const double2 v = ex_m(w.T, n, r, j);
+
+                W[r * ld + j] = r == j ? 1.0 : hypot(v.x, v.y);
+            }
+        __syncwarp();
+        st |= jacobi_pinv(n, ld, W, V, lam, t);
+        for (int r = t; r < n; r += 32)
+            for (int j = r; j < n; j++)
+                w.G[tc_pidx(n, r, j)] = W[r * ld + j];
+    }
+    if (t == 0)
+        w.ints[1] = (int)st;
+    __syncthreads();
+    return (unsigned)w.ints[1];
 }
 
 /* Householder reduction of the packed Hermitian M (w.T) to the real
@@ -1455,10 +1548,11 @@ __device__ void ex_householder(int n, int npu, const ExWs &w)
     __syncthreads();
 }
 
-/* Smallest eigenvalue of (w.d, w.e) by 128-way multisection on double
-   Sturm counts, then its eigenvector by inverse iteration (thread 0), then
+/* Eigenvalue of rank `index` of (w.d, w.e) (0: the smallest, for EMI;
+   n - 1: the largest, for EVD) by 128-way multisection on double Sturm
+   counts, then its eigenvector by inverse iteration (thread 0), then
    z = Q y by the reflectors (warp 0): into w.z. Returns status bits. */
-__device__ unsigned ex_eigvec(int n, const ExWs &w)
+__device__ unsigned ex_eigvec(int n, int index, const ExWs &w)
 {
     const int t = threadIdx.x;
     unsigned status = 0;
@@ -1501,7 +1595,7 @@ __device__ unsigned ex_eigvec(int n, const ExWs &w)
         if (hi - lo <= 2.0e-15 * norm)
             break;
         const double xq = lo + (hi - lo) * ((double)(t + 1) / (double)(EX_THREADS + 1));
-        const bool gt = sturmd(w.d, w.e2, n, xq, pivmin) > 0;
+        const bool gt = sturmd(w.d, w.e2, n, xq, pivmin) > index;
         const unsigned bal = __ballot_sync(FULL, gt);
 
         if ((t & 31) == 0)
@@ -1807,38 +1901,27 @@ tc_link_exact_kernel(TcStrip s, TcChunk c, TcLinkConst k, ExLayout L,
         }
         unsigned st = TC_STATUS_FP64;
 
-        if (!ex_sweep(n, npu, w)) {
-            /* the pseudo-inverse, on warp 0, in full storage in global
-               scratch: |T| again from T */
-            st |= TC_STATUS_EMI_PINV;
-            if (t < 32) {
-                double *V = W + n * ld, *lam = W + 2 * n * ld;
+        if (k.emi) {
+            st |= ex_inverse(n, npu, ld, w, W);
+            /* M = |T|^-1 o T in place of T; T in float in place of |T|^-1 */
+            for (int q = t; q < npu; q += EX_THREADS) {
+                const double g = w.G[q];
+                const double2 v = w.T[q];
 
-                for (int r = t; r < n; r += 32)
-                    for (int j = 0; j < n; j++) {
-                        const double2 v = ex_m(w.T, n, r, j);
-
-                        W[r * ld + j] = r == j ? 1.0 : hypot(v.x, v.y);
-                    }
-                __syncwarp();
-                st |= jacobi_pinv(n, ld, W, V, lam, t);
-                for (int r = t; r < n; r += 32)
-                    for (int j = r; j < n; j++)
-                        w.G[tc_pidx(n, r, j)] = W[r * ld + j];
+                w.T[q] = make_double2(g * v.x, g * v.y);
+                w.Tf[q] = make_float2((float)v.x, (float)v.y);
             }
-            __syncthreads();
         }
-        /* M = |T|^-1 o T in place of T; T in float in place of |T|^-1 */
-        for (int q = t; q < npu; q += EX_THREADS) {
-            const double g = w.G[q];
-            const double2 v = w.T[q];
+        else
+            /* EVD: T itself; T in float in place of |T| */
+            for (int q = t; q < npu; q += EX_THREADS) {
+                const double2 v = w.T[q];
 
-            w.T[q] = make_double2(g * v.x, g * v.y);
-            w.Tf[q] = make_float2((float)v.x, (float)v.y);
-        }
+                w.Tf[q] = make_float2((float)v.x, (float)v.y);
+            }
         __syncthreads();
         ex_householder(n, npu, w);
-        st |= ex_eigvec(n, w);
+        st |= ex_eigvec(n, k.emi ? 0 : n - 1, w);
         const float gamma = ex_gamma(n, npu, w);
 
         if (t == 0)
@@ -1930,23 +2013,26 @@ cudaError_t tc_launch_link(const TcStrip &s, const TcChunk &c, const TcLinkConst
 {
     cudaError_t e;
 
-    if (k.emi && !exact_list)
+    /* the float kernels hand pixels to the exact tier with EMI and with
+       the bias correction */
+    int *list = k.emi || k.bias ? exact_list : nullptr;
+
+    if ((k.emi || k.bias) && !exact_list)
         return cudaErrorInvalidValue;
-    if (s.n <= 32) {
-        if (k.emi && (e = cudaMemsetAsync(exact_list, 0, sizeof(int), st)) != cudaSuccess)
-            return e;
-        if ((e = tc_launch_link_half(s, c, k, gram, count, upper_tab, pair_tab, scratch, coh,
-                                     pairs, phases, status, k.emi ? exact_list : nullptr, sms,
-                                     st)) != cudaSuccess)
-            return e;
-        if (!k.emi)
-            return cudaSuccess;
-        return launch_exact(s, c, k, slc, mask, count, exact_list, upper_tab, pair_tab, scratch,
-                            coh, pairs, phases, status, sms, st);
-    }
-    if (k.emi)
+    if (s.n > 32 && k.emi)
         return launch_exact(s, c, k, slc, mask, count, nullptr, upper_tab, pair_tab, scratch, coh,
                             pairs, phases, status, sms, st);
+    if (list && (e = cudaMemsetAsync(list, 0, sizeof(int), st)) != cudaSuccess)
+        return e;
+    if (s.n <= 32) {
+        if ((e = tc_launch_link_half(s, c, k, gram, count, upper_tab, pair_tab, scratch, coh,
+                                     pairs, phases, status, list, sms, st)) != cudaSuccess)
+            return e;
+        if (!list)
+            return cudaSuccess;
+        return launch_exact(s, c, k, slc, mask, count, list, upper_tab, pair_tab, scratch, coh,
+                            pairs, phases, status, sms, st);
+    }
     const LinkLayout L = layout_for(s.n, 0, false);
     const size_t per_warp = (size_t)L.per_warp * sizeof(double);
     int wpb = (int)((227 * 1024) / per_warp);
@@ -1963,8 +2049,12 @@ cudaError_t tc_launch_link(const TcStrip &s, const TcChunk &c, const TcLinkConst
                              (int)smem);
     if (e == cudaSuccess)
         tc_link_smem_kernel<<<blocks, wpb * 32, smem, st>>>(
-            s, c, k, L, gram, count, upper_tab, pair_tab, scratch, coh, pairs, phases, status);
-    if (e != cudaSuccess)
+            s, c, k, L, gram, count, upper_tab, pair_tab, scratch, coh, pairs, phases, status,
+            list);
+    if (e == cudaSuccess)
+        e = cudaGetLastError();
+    if (e != cudaSuccess || !list)
         return e;
-    return cudaGetLastError();
+    return launch_exact(s, c, k, slc, mask, count, list, upper_tab, pair_tab, scratch, coh, pairs,
+                        phases, status, sms, st);
 }

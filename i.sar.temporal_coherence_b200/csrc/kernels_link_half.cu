@@ -1097,7 +1097,7 @@ template <int B>
 __device__ __forceinline__ void load_T_batch(const float2 (&gv)[B], int t0, int n, int npu, bool active,
                                              int looks, const TcLinkConst &k,
                                              const unsigned short *upper_tab, const HWs &w,
-                                             int ld, const Grp &g)
+                                             int ld, const Grp &g, bool &boundary)
 {
     const float fl = (float)looks;
     const bool debias = k.bias && looks > 1;
@@ -1128,7 +1128,10 @@ __device__ __forceinline__ void load_T_batch(const float2 (&gv)[B], int t0, int 
                 if (debias) {
                     /* f^2 = m2c / m2, m2c = (L m2 - 1) / (L - 1) */
                     const float m2 = re * re + im * im;
-                    const float m2c = fmaf(fl, m2, -1.0f) * ilm1;
+                    const float lm1 = fmaf(fl, m2, -1.0f);
+                    const float m2c = lm1 * ilm1;
+
+                    boundary |= fabsf(lm1) < TC_BIAS_BAND * fl * m2;
                     const float f2 = m2 > 0.f && m2c > 0.f ? m2c * __fdividef(1.0f, m2) : 0.f;
                     const float f = f2 > 0.f ? f2 * rsqrtf(f2) : 0.f;
 
@@ -1149,7 +1152,8 @@ __device__ __forceinline__ void load_T_batch(const float2 (&gv)[B], int t0, int 
    is the CTA's shared-memory copy of the packed-entry table. */
 __device__ void load_T(const TcStrip &s, const TcChunk &c, const TcLinkConst &k, int p, bool active,
                        int looks, const float2 *__restrict__ gram,
-                       const unsigned short *upper_tab, const HWs &w, int ld, const Grp &g)
+                       const unsigned short *upper_tab, const HWs &w, int ld, const Grp &g,
+                       bool &boundary)
 {
     const int n = s.n, npu = tc_npu(n);
     const int i0 = g.gl, i1 = g.gl + 16;
@@ -1168,15 +1172,16 @@ __device__ void load_T(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
     if (i1 < n)
         w.nrm[i1] = d1 > 0.f ? __frcp_rn(__fsqrt_rn(d1)) : 0.f;
     gsync(g);
-    load_T_batch<17>(ga, 0, n, npu, active, looks, k, upper_tab, w, ld, g);
+    load_T_batch<17>(ga, 0, n, npu, active, looks, k, upper_tab, w, ld, g, boundary);
 #pragma unroll
     for (int t = 0; t < 16; t++) {
         const int q = g.gl + 16 * (17 + t);
 
         gb[t] = (active && q < npu) ? gram[tc_gram_at(npu, p, q)] : make_float2(0.f, 0.f);
     }
-    load_T_batch<16>(gb, 17, n, npu, active, looks, k, upper_tab, w, ld, g);
+    load_T_batch<16>(gb, 17, n, npu, active, looks, k, upper_tab, w, ld, g, boundary);
     gsync(g);
+    boundary = __any_sync(g.mask, boundary);
 }
 
 /* Whether the non-zero coherences link all dates (n <= 32). */
@@ -1699,8 +1704,17 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
         bool run = __any_sync(FULL, active);
 
         /* stage 1: coherence matrix, pair coherences, connectivity */
+        bool sent = false; /* the pixel is on the exact tier's list */
+
         if (run) {
-            load_T(s, c, k, p, active, looks, gram, s_upper, w, ld, g);
+            bool boundary = false;
+
+            load_T(s, c, k, p, active, looks, gram, s_upper, w, ld, g, boundary);
+            if (exact_list && active && boundary) {
+                sent = true;
+                if (g.gl == 0)
+                    exact_list[1 + atomicAdd(exact_list, 1)] = p;
+            }
             if (active)
                 for (int t = g.gl; t < k.npairs; t += 16) {
                     const int i = pair_tab[t] >> 8, j = pair_tab[t] & 255;
@@ -1802,7 +1816,7 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
                    30 and 60 dates against the FP64 oracle: with the bound
                    3e4, no unflagged pixel was off by more than 1.1e-5, the
                    worst pixels sitting at 1.4e5 and above. */
-                if (exact_list && active) {
+                if (exact_list && active && !sent) {
                     const double delta = inv_max * (double)norm / 3.0e4;
                     bool flag = !(delta < (double)norm);
 
@@ -1942,7 +1956,7 @@ cudaError_t tc_launch_link_half(const TcStrip &s, const TcChunk &c, const TcLink
         return launch_half<true, false>(s, c, k, gram, count, upper_tab, pair_tab, scratch, coh,
                                         pairs, phases, status, nullptr, exact_list, sms, st);
     return launch_half<false, false>(s, c, k, gram, count, upper_tab, pair_tab, scratch, coh,
-                                     pairs, phases, status, nullptr, nullptr, sms, st);
+                                     pairs, phases, status, nullptr, exact_list, sms, st);
 }
 
 cudaError_t tc_launch_link_adjoint(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,

@@ -90,7 +90,7 @@ static size_t substrip_bytes(const struct settings *s, int padded_cols, int cols
     b += up256(sizeof(float2) * (size_t)tc_npu(s->ndates) * npix);
     if (s->npairs)
         b += up256(sizeof(float) * (size_t)s->npairs * mr * cols);
-    if (s->emi)
+    if (s->emi || s->bias)
         b += up256(sizeof(int) * (npix + 1)); /* the exact tier's pixel list */
     return b;
 }
@@ -218,7 +218,7 @@ TC_API int tc_run_device_static(const struct settings *s, int padded_cols, const
             spairs = (float *)q;
             q += up256(sizeof(float) * (size_t)s->npairs * m * cols);
         }
-        int *elist = s->emi ? (int *)q : nullptr;
+        int *elist = s->emi || s->bias ? (int *)q : nullptr;
 
         const float *s_slc = slc + (size_t)r0 * W * n * 2;
         const float *s_amp = amp + (size_t)r0 * W * n;

@@ -52,6 +52,13 @@ struct TcLinkConst {
 
 __host__ __device__ inline int tc_npu(int n) { return n * (n + 1) / 2; }
 
+/* The bias correction zeroes an entry when L m2 <= 1 (tcoh.cl:626-632), a
+   jump of gamma by up to 2 / (n (n - 1)). Where the float rounding of the
+   sums could decide it otherwise than double sums, |L m2 - 1| within this
+   fraction of L m2 (the float error there is about 2e-6 of it), the float
+   kernels send the pixel to the exact tier, which decides in double. */
+#define TC_BIAS_BAND 3.0e-5f
+
 /* The coherence sums of a chunk are float2 [npix][npu], pixel-major: the
    lanes that load one pixel's matrix read contiguous bytes. */
 __host__ __device__ inline long long tc_gram_at(int npu, long long p, int q)

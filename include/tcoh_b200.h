@@ -105,12 +105,14 @@ struct tc_options {
                                   inverted by its eigen-pseudo-inverse */
 #define TC_STATUS_UNLINKED   2 /* bias correction unlinked the dates */
 #define TC_STATUS_ITER_CAP   4 /* an iterative solver reached its cap */
-#define TC_STATUS_FP64       8 /* EMI: recomputed from double-precision
-                                  coherence sums (every pixel above 32
-                                  dates; up to 32 dates, the pixels whose
+#define TC_STATUS_FP64       8 /* recomputed from double-precision
+                                  coherence sums: EMI, every pixel above 32
+                                  dates, and up to 32 dates the pixels whose
                                   float result the conditioning of |T| and
                                   of M's eigengap may have moved by more
-                                  than ~1e-5) */
+                                  than ~1e-5; with the bias correction, the
+                                  pixels with an entry at the threshold of
+                                  the correction */
 
 /* Message of the last failed tc_* call of this thread. */
 const char *tc_last_error(void);

@@ -30,11 +30,12 @@ CASES = [
     dict(n=10, rows=35, cols=70, seed=3, shp_test="tlog", estimator="evd", bias=False,
          window=(9, 5), pairs=False, pairs_all=False),
     # Several sub-strips: the coherence sums of the whole strip alone take
-    # 8 B x 465 entries x (7 x 63 tiles of 128 pixels) = 210 MB, more than
-    # three times the 64 MiB array, so the strip is cut into at least four
-    # sub-strips, the last one of 100 mod 16 = 4 rows; the pair planes go
-    # through the strided copy into the caller's [npairs][rows][cols].
-    dict(n=30, rows=100, cols=500, seed=4, shp_test="ks", estimator="emi", bias=True,
+    # 8 B x 465 entries x (7 x 38 tiles of 128 pixels) = 127 MB, twice the
+    # 64 MiB array (which also holds 36 MB of EMI scratch), so the strip is
+    # cut into at least three sub-strips, the last one of 100 mod 16 = 4
+    # rows; the pair planes go through the strided copy into the caller's
+    # [npairs][rows][cols].
+    dict(n=30, rows=100, cols=300, seed=4, shp_test="ks", estimator="emi", bias=True,
          window=(21, 7), pairs=True, pairs_all=False),
 ]
 
