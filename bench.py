@@ -307,6 +307,14 @@ def crop_accuracy(crop, coh_gpu, count_gpu, size, n, kw, flips_size=64):
     out["phases_rad"] = {"max_abs": float(np.abs(d).max()) if d.size else None,
                          "rms": float(np.sqrt(np.mean(d ** 2))) if d.size else None,
                          "p999": float(np.quantile(np.abs(d), 0.999)) if d.size else None}
+    if d.size:
+        dd = np.zeros(o["phases"].shape)
+        dd[ph] = np.abs(d)
+        worst = np.argsort(dd.ravel())[::-1][:5]
+        out["phases_rad"]["worst"] = [
+            {"row": int(i // (size * n)), "col": int(i // n % size), "date": int(i % n),
+             "err": float(dd.ravel()[i]), "status": int(r["status"].ravel()[i // n]),
+             "coh": float(g.ravel()[i // n])} for i in worst]
     fs = min(flips_size, size)
     fc = cpu_crop(*crop, size, size, 0, fs, fs, ha, hr)
     o64 = oracle.run_oracle(*fc, fs, fs, shp_fp32=False, **kw)

@@ -1393,7 +1393,8 @@ __device__ void ex_symmul(int n, int npu, const ExWs &w, const double *A, const 
 /* |T|^-1 into w.G (which holds |T|), in tiers as the 32-date kernel does:
    the sweep with pivots above 1e-5; else (|T|^2)^-1 |T| (|T|^2 is positive
    semi-definite, its sweep takes any non-zero pivot) in the CTA's global
-   scratch W; else, or when the inverse is not moderate, the Jacobi
+   scratch W, when it inverts |T| to 1e-6; else, or when the inverse is not
+   moderate, the Jacobi
    eigen-pseudo-inverse with the absolute floor 1e-9
    (tests/reference.py:151-156) on warp 0. Returns status bits. */
 __device__ unsigned ex_inverse(int n, int npu, int ld, const ExWs &w, double *W)
@@ -1414,11 +1415,32 @@ __device__ unsigned ex_inverse(int n, int npu, int ld, const ExWs &w, double *W)
     ex_symmul(n, npu, w, w.G, w.G, G2);
     if (ex_sweep(n, npu, w, G2, 1.0e-300)) {
         ex_symmul(n, npu, w, G2, w.G, P);
-        for (int q = t; q < npu; q += EX_THREADS)
-            w.G[q] = P[q];
+        /* accepted when |T| P = I to 1e-6: for a singular |T| the rounding
+           of |T|^2 leaves P moderate but wrong along the null space */
+        double res = 0.0;
+
+        for (int q = t; q < npu; q += EX_THREADS) {
+            const int i = w.tab[q] >> 8, j = w.tab[q] & 255;
+            double acc = 0.0;
+
+            for (int kk = 0; kk < n; kk++)
+                acc = fma(w.G[ex_sym(n, i, kk)], P[ex_sym(n, kk, j)], acc);
+            res = fmax(res, fabs(acc - (i == j ? 1.0 : 0.0)));
+            res = res == res ? res : INFINITY;
+        }
+        res = wmaxd(res);
+        if ((t & 31) == 0)
+            w.red[t >> 5] = res;
         __syncthreads();
-        if (ex_moderate(n, npu, w, w.G))
-            return TC_STATUS_EMI_PINV;
+        res = fmax(fmax(w.red[0], w.red[1]), fmax(w.red[2], w.red[3]));
+        __syncthreads();
+        if (res < 1.0e-6) {
+            for (int q = t; q < npu; q += EX_THREADS)
+                w.G[q] = P[q];
+            __syncthreads();
+            if (ex_moderate(n, npu, w, w.G))
+                return TC_STATUS_EMI_PINV;
+        }
     }
     unsigned st = TC_STATUS_EMI_PINV;
 

@@ -73,7 +73,7 @@ template <int TEST>
 __global__ void __launch_bounds__(256)
 tc_shp_kernel(TcStrip s, TcChunk c, TcShpConst k, const float *__restrict__ amp,
               const unsigned char *__restrict__ valid, const float2 *__restrict__ logstat,
-              uint32_t *__restrict__ mask, int *__restrict__ count)
+              uint32_t *__restrict__ mask, int *__restrict__ count, int vec)
 {
     extern __shared__ float sm[];
     const int n = s.n;
@@ -151,8 +151,29 @@ tc_shp_kernel(TcStrip s, TcChunk c, TcShpConst k, const float *__restrict__ amp,
                     else {
                         const float *b = amp + q * n;
 
-                        for (int j = 0; j < n; j++)
-                            b_s[j * 32 + lane] = b[j];
+                        /* the lanes read different pixels: vector loads
+                           (vec = 4 or 2 when the series start on 16- or
+                           8-byte boundaries, checked on the host) cut the
+                           number of scattered requests */
+                        if (vec == 4)
+                            for (int j = 0; j < n; j += 4) {
+                                const float4 v = *(const float4 *)(b + j);
+
+                                b_s[j * 32 + lane] = v.x;
+                                b_s[(j + 1) * 32 + lane] = v.y;
+                                b_s[(j + 2) * 32 + lane] = v.z;
+                                b_s[(j + 3) * 32 + lane] = v.w;
+                            }
+                        else if (vec == 2)
+                            for (int j = 0; j < n; j += 2) {
+                                const float2 v = *(const float2 *)(b + j);
+
+                                b_s[j * 32 + lane] = v.x;
+                                b_s[(j + 1) * 32 + lane] = v.y;
+                            }
+                        else
+                            for (int j = 0; j < n; j++)
+                                b_s[j * 32 + lane] = b[j];
                         b_s[n * 32 + lane] = INFINITY;
                         /* Merge walk, centre first on ties: 2N - 1 steps.
                            Both series end in an INFINITY sentinel, so a
@@ -250,6 +271,8 @@ cudaError_t tc_launch_shp(const TcStrip &s, const TcChunk &c, const TcShpConst &
     const size_t smem = sizeof(float) * (tab + wpb * ((s.n + 1) + (s.n + 1) * 32));
     const int want = (c.npix + wpb - 1) / wpb;
     const int blocks = want < sms * 8 ? want : sms * 8;
+    const uintptr_t base = (uintptr_t)amp;
+    const int vec = (s.n % 4 == 0 && base % 16 == 0) ? 4 : (s.n % 2 == 0 && base % 8 == 0) ? 2 : 1;
     cudaError_t e;
 
     switch (k.test) {
@@ -258,21 +281,21 @@ cudaError_t tc_launch_shp(const TcStrip &s, const TcChunk &c, const TcShpConst &
                                  (int)smem);
         if (e == cudaSuccess)
             tc_shp_kernel<0><<<blocks, threads, smem, st>>>(s, c, k, amp, valid, logstat, mask,
-                                                            count);
+                                                            count, vec);
         break;
     case 1:
         e = cudaFuncSetAttribute(tc_shp_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem);
         if (e == cudaSuccess)
             tc_shp_kernel<1><<<blocks, threads, smem, st>>>(s, c, k, amp, valid, logstat, mask,
-                                                            count);
+                                                            count, vec);
         break;
     default:
         e = cudaFuncSetAttribute(tc_shp_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem);
         if (e == cudaSuccess)
             tc_shp_kernel<2><<<blocks, threads, smem, st>>>(s, c, k, amp, valid, logstat, mask,
-                                                            count);
+                                                            count, vec);
         break;
     }
     if (e != cudaSuccess)
