@@ -1041,7 +1041,9 @@ __host__ __device__ inline ExLayout ex_layout(int n, int area)
     L.off_G = take(8 * L.npu);
     L.off_tab = take(2 * L.npu);
     L.off_blk = take(2 * L.nblk);
-    L.off_stage = take(8 * EX_KC * n);
+    /* the staged samples; once the sums are formed, up to 32 dates, the
+       two packed matrices of the |T|^2 inverse tier */
+    L.off_stage = take(n <= 32 && 16 * L.npu > 8 * EX_KC * n ? 16 * L.npu : 8 * EX_KC * n);
     L.off_cand = take(2 * area);
     L.off_vec = take(8 * (8 * 64 + 8 + 4 * 64) + 16 * 5 * 64 + 8 * 64 + 16);
     L.off_adj = take(8 * 64);
@@ -1403,7 +1405,10 @@ __device__ unsigned ex_inverse(int n, int npu, int ld, const ExWs &w, double *W)
 
     if (ex_sweep(n, npu, w, w.G, 1.0e-5) && ex_moderate(n, npu, w, w.G))
         return 0;
-    double *G2 = W, *P = W + n * ld;
+    /* |T|^2 and the product in shared memory (the staged samples' region)
+       up to 32 dates, in the CTA's global scratch above */
+    double *G2 = n <= 32 ? (double *)w.stage : W;
+    double *P = n <= 32 ? G2 + npu : W + n * ld;
 
     for (int q = t; q < npu; q += EX_THREADS) {
         const double2 v = w.T[q];
