@@ -976,8 +976,8 @@ tc_link_smem_kernel(TcStrip s, TcChunk c, TcLinkConst k, LinkLayout L,
    a pixel from its samples with everything in double: the masked sums
    C = sum over SHPs q of s_q s_q^H (tcoh.cl:567-602, as tests/reference.py
    sums them), T and its bias correction (tcoh.cl:610-636); for EMI |T|^-1
-   (ex_inverse: the symmetric sweep, through |T|^2, or the Jacobi
-   pseudo-inverse with the absolute floor 1e-9 of
+   (ex_inverse: the symmetric sweep, Gauss-Jordan with partial pivoting,
+   or the Jacobi pseudo-inverse with the absolute floor 1e-9 of
    tests/reference.py:151-156) and M = |T|^-1 o T, for EVD T itself; the
    Householder reduction to a real tridiagonal, the wanted eigenvalue by
    multisection on Sturm counts, inverse iteration and the
@@ -1042,8 +1042,8 @@ __host__ __device__ inline ExLayout ex_layout(int n, int area)
     L.off_tab = take(2 * L.npu);
     L.off_blk = take(2 * L.nblk);
     /* the staged samples; once the sums are formed, up to 32 dates, the
-       two packed matrices of the |T|^2 inverse tier */
-    L.off_stage = take(n <= 32 && 16 * L.npu > 8 * EX_KC * n ? 16 * L.npu : 8 * EX_KC * n);
+       full |T| of the Gauss-Jordan inverse tier */
+    L.off_stage = take(n <= 32 && 8 * n * n > 8 * EX_KC * n ? 8 * n * n : 8 * EX_KC * n);
     L.off_cand = take(2 * area);
     L.off_vec = take(8 * (8 * 64 + 8 + 4 * 64) + 16 * 5 * 64 + 8 * 64 + 16);
     L.off_adj = take(8 * 64);
@@ -1377,76 +1377,128 @@ __device__ bool ex_moderate(int n, int npu, const ExWs &w, const double *A)
     return mx <= 1.0e300 && n * mx < 1.0e8;
 }
 
-/* Packed symmetric C = A B (A, B packed symmetric, commuting: C symmetric). */
-__device__ void ex_symmul(int n, int npu, const ExWs &w, const double *A, const double *B,
-                          double *C)
+/* A^-1 in place of the full n x n A (row-major) by Gauss-Jordan
+   elimination with partial pivoting (the row of the largest magnitude in
+   the pivot column; the column permutation is undone at the end). It takes
+   indefinite and ill-conditioned matrices; false when a pivot falls below
+   1e-14 of the largest entry (numerically singular). */
+__device__ bool ex_gauss_jordan(int n, const ExWs &w, double *A)
 {
-    for (int q = threadIdx.x; q < npu; q += EX_THREADS) {
-        const int i = w.tab[q] >> 8, j = w.tab[q] & 255;
-        double acc = 0.0;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    int *perm = (int *)w.adj;
+    double amax = 0.0;
 
-        for (int kk = 0; kk < n; kk++)
-            acc = fma(A[ex_sym(n, i, kk)], B[ex_sym(n, kk, j)], acc);
-        C[q] = acc;
-    }
+    for (int e = t; e < n * n; e += EX_THREADS)
+        amax = fmax(amax, fabs(A[e]));
+    amax = wmaxd(amax);
+    if (lane == 0)
+        w.red[warp] = amax;
     __syncthreads();
+    amax = fmax(fmax(w.red[0], w.red[1]), fmax(w.red[2], w.red[3]));
+    __syncthreads();
+    for (int k = 0; k < n; k++) {
+        /* pivot row: the largest |A[i][k]|, i >= k */
+        double v = t >= k && t < n ? fabs(A[t * n + k]) : -1.0;
+        int idx = t;
+
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const double ov = __shfl_xor_sync(FULL, v, o);
+            const int oi = __shfl_xor_sync(FULL, idx, o);
+
+            if (ov > v || (ov == v && oi < idx)) {
+                v = ov;
+                idx = oi;
+            }
+        }
+        if (lane == 0) {
+            w.red[warp] = v;
+            w.ints[2 + warp] = idx;
+        }
+        __syncthreads();
+        int p = w.ints[2];
+        double best = w.red[0];
+
+        for (int q = 1; q < EX_THREADS / 32; q++)
+            if (w.red[q] > best) {
+                best = w.red[q];
+                p = w.ints[2 + q];
+            }
+        __syncthreads();
+        if (!(best > 1.0e-14 * amax))
+            return false;
+        if (t == 0)
+            perm[k] = p;
+        /* swap rows p and k, then scale row k (its pivot becomes 1 / piv) */
+        const double piv = A[p * n + k];
+
+        __syncthreads();
+        for (int j = t; j < n; j += EX_THREADS) {
+            const double rk = A[k * n + j], rp = A[p * n + j];
+
+            A[p * n + j] = rk;
+            A[k * n + j] = (j == k ? 1.0 : rp) / piv;
+        }
+        __syncthreads();
+        for (int i = t; i < n; i += EX_THREADS)
+            w.rrow[i] = i == k ? 0.0 : A[i * n + k];
+        __syncthreads();
+        for (int e = t; e < n * n; e += EX_THREADS) {
+            const int i = e / n, j = e - i * n;
+
+            if (i != k)
+                A[e] = (j == k ? 0.0 : A[e]) - A[k * n + j] * w.rrow[i];
+        }
+        __syncthreads();
+    }
+    /* undo the row swaps on the columns of the inverse, last swap first */
+    for (int k = n - 1; k >= 0; k--) {
+        const int p = perm[k];
+
+        if (p != k)
+            for (int i = t; i < n; i += EX_THREADS) {
+                const double x = A[i * n + k];
+
+                A[i * n + k] = A[i * n + p];
+                A[i * n + p] = x;
+            }
+        __syncthreads();
+    }
+    return true;
 }
 
-/* |T|^-1 into w.G (which holds |T|), in tiers as the 32-date kernel does:
-   the sweep with pivots above 1e-5; else (|T|^2)^-1 |T| (|T|^2 is positive
-   semi-definite, its sweep takes any non-zero pivot) in the CTA's global
-   scratch W, when it inverts |T| to 1e-6; else, or when the inverse is not
-   moderate, the Jacobi
-   eigen-pseudo-inverse with the absolute floor 1e-9
-   (tests/reference.py:151-156) on warp 0. Returns status bits. */
+/* |T|^-1 into w.G (which holds |T|), in tiers: the symmetric sweep with
+   pivots above 1e-5; else Gauss-Jordan elimination with partial pivoting
+   on the full |T| (in shared memory, the staged samples' region, up to 32
+   dates; in the CTA's global scratch W above); else, or when the inverse is
+   not moderate, the Jacobi eigen-pseudo-inverse with the absolute floor
+   1e-9 (tests/reference.py:151-156) on warp 0. Returns status bits. */
 __device__ unsigned ex_inverse(int n, int npu, int ld, const ExWs &w, double *W)
 {
     const int t = threadIdx.x;
 
     if (ex_sweep(n, npu, w, w.G, 1.0e-5) && ex_moderate(n, npu, w, w.G))
         return 0;
-    /* |T|^2 and the product in shared memory (the staged samples' region)
-       up to 32 dates, in the CTA's global scratch above */
-    double *G2 = n <= 32 ? (double *)w.stage : W;
-    double *P = n <= 32 ? G2 + npu : W + n * ld;
+    double *A = n <= 32 ? (double *)w.stage : W;
 
-    for (int q = t; q < npu; q += EX_THREADS) {
-        const double2 v = w.T[q];
-        const int i = w.tab[q] >> 8, j = w.tab[q] & 255;
+    for (int e = t; e < n * n; e += EX_THREADS) {
+        const int i = e / n, j = e - i * n;
+        const double2 v = ex_m(w.T, n, i, j);
 
-        w.G[q] = i == j ? 1.0 : hypot(v.x, v.y);
+        A[e] = i == j ? 1.0 : hypot(v.x, v.y);
     }
     __syncthreads();
-    ex_symmul(n, npu, w, w.G, w.G, G2);
-    if (ex_sweep(n, npu, w, G2, 1.0e-300)) {
-        ex_symmul(n, npu, w, G2, w.G, P);
-        /* accepted when |T| P = I to 1e-6: for a singular |T| the rounding
-           of |T|^2 leaves P moderate but wrong along the null space */
-        double res = 0.0;
-
+    if (ex_gauss_jordan(n, w, A)) {
         for (int q = t; q < npu; q += EX_THREADS) {
             const int i = w.tab[q] >> 8, j = w.tab[q] & 255;
-            double acc = 0.0;
 
-            for (int kk = 0; kk < n; kk++)
-                acc = fma(w.G[ex_sym(n, i, kk)], P[ex_sym(n, kk, j)], acc);
-            res = fmax(res, fabs(acc - (i == j ? 1.0 : 0.0)));
-            res = res == res ? res : INFINITY;
+            w.G[q] = 0.5 * (A[i * n + j] + A[j * n + i]);
         }
-        res = wmaxd(res);
-        if ((t & 31) == 0)
-            w.red[t >> 5] = res;
         __syncthreads();
-        res = fmax(fmax(w.red[0], w.red[1]), fmax(w.red[2], w.red[3]));
-        __syncthreads();
-        if (res < 1.0e-6) {
-            for (int q = t; q < npu; q += EX_THREADS)
-                w.G[q] = P[q];
-            __syncthreads();
-            if (ex_moderate(n, npu, w, w.G))
-                return TC_STATUS_EMI_PINV;
-        }
+        if (ex_moderate(n, npu, w, w.G))
+            return TC_STATUS_EMI_PINV;
     }
+    __syncthreads();
     unsigned st = TC_STATUS_EMI_PINV;
 
     if (t < 32) {
