@@ -56,11 +56,13 @@ def metric_name(w):
         return METRIC
     return "Mpixel/s temporal coherence at N=%d, %dx%d window, <=1e-4 vs FP64" % (
         w["n"], w["window"][0], w["window"][1])
-# DRAM bytes (read + write) per pixel of one phase-linking launch, from an
-# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of one
-# 65,536-pixel chunk at N=30, AD / EMI / bias correction: 232.2 MB read (the
-# packed Gram, 465 x 8 B per pixel, read at most once) + 7.3 MB written.
-LINK_DRAM_BYTES_PER_PIXEL = 239.4e6 / 65536
+# DRAM bytes (read + write) per pixel of one phase-linking launch: a
+# constant, from the ncu capture of profiles/
+# tc_link_half_kernel_emi_bias_n30_256x4096.md (dram__bytes_read.sum +
+# dram__bytes_write.sum of one 65,536-pixel chunk at N=30, AD / EMI / bias
+# correction: 237.7 MB read, the packed Gram, 465 x 8 B per pixel, read at
+# most once, + 9.6 MB written), not a measurement of the run that reports it.
+LINK_DRAM_BYTES_PER_PIXEL = 247.3e6 / 65536
 
 
 def parse():
@@ -310,6 +312,11 @@ def crop_accuracy(crop, coh_gpu, count_gpu, size, n, kw, flips_size=64):
     if d.size:
         dd = np.zeros(o["phases"].shape)
         dd[ph] = np.abs(d)
+        # the phases of coherent pixels (gamma >= 0.2; on incoherent ones the
+        # eigenproblem is nearly degenerate and the phases ill-determined)
+        coherent = np.nan_to_num(o["coh"]) >= 0.2
+        out["phases_rad"]["max_abs_coherence_ge_0.2"] = float(dd[coherent].max()) \
+            if coherent.any() else None
         worst = np.argsort(dd.ravel())[::-1][:5]
         out["phases_rad"]["worst"] = [
             {"row": int(i // (size * n)), "col": int(i // n % size), "date": int(i % n),
@@ -888,8 +895,9 @@ def main():
         px_launch = npix / d["launches"]
         roofline["traffic"] = LINK_DRAM_BYTES_PER_PIXEL * px_launch
         roofline["algorithmic_bytes_per_launch"] = (8.0 * w["n"] * (w["n"] + 1) / 2 + 4) * px_launch
-        roofline["traffic_source"] = ("ncu dram bytes of one 65,536-pixel launch, scaled by "
-                                      "the pixels per launch")
+        roofline["traffic_source"] = ("constant: ncu dram bytes of one 65,536-pixel launch "
+                                      "(profiles/tc_link_half_kernel_emi_bias_n30_256x4096.md), "
+                                      "scaled by the pixels per launch")
     line = {"metric": metric_name(w), "value": value, "unit": "Mpixel/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",

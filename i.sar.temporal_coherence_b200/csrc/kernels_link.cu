@@ -1579,17 +1579,31 @@ __device__ void ex_householder(int n, int npu, const ExWs &w)
         __syncthreads();
         if (!reflect)
             continue;
-        /* p = M22 v over rows k+1 .. n-1, two threads per row */
+        /* p = M22 v over rows k+1 .. n-1, two threads per row (columns of
+           one parity each): M_ij = conj(P(j, i)) for j < i, at
+           rb(j) + i - j with rb(j) = j (2n - j + 1) / 2, then P(i, j) for
+           j >= i, contiguous */
         const int i = k + 1 + (t >> 1), h = t & 1;
         double sx = 0.0, sy = 0.0;
 
-        if (i < n)
-            for (int j = k + 1 + h; j < n; j += 2) {
-                const double2 m = ex_m(w.T, n, i, j), v = w.v[j];
+        if (i < n) {
+            int j = k + 1 + h;
+            int idx = j * (2 * n - j + 1) / 2 + (i - j);
+
+            for (; j < i; j += 2) {
+                const double2 m = w.T[idx], v = w.v[j];
+
+                sx = fma(m.x, v.x, fma(m.y, v.y, sx));
+                sy = fma(m.x, v.y, fma(-m.y, v.x, sy));
+                idx += 2 * (n - j) - 3;
+            }
+            for (idx = i * (2 * n - i + 1) / 2 + (j - i); j < n; j += 2, idx += 2) {
+                const double2 m = w.T[idx], v = w.v[j];
 
                 sx = fma(m.x, v.x, fma(-m.y, v.y, sx));
                 sy = fma(m.x, v.y, fma(m.y, v.x, sy));
             }
+        }
         sx += __shfl_xor_sync(FULL, sx, 1);
         sy += __shfl_xor_sync(FULL, sy, 1);
         const double2 wl = make_double2(tr * sx - ti * sy, tr * sy + ti * sx);
@@ -1667,6 +1681,36 @@ __device__ unsigned ex_eigvec(int n, int index, const ExWs &w)
 
     lo -= 1.0e-12 * norm + 1e-300;
     hi += 1.0e-12 * norm + 1e-300;
+    /* float Sturm counts first (on float copies in the LU's region), down to
+       a few float ulps of the spectrum's scale; then, the interval widened
+       by the float counts' possible error, double counts */
+    float *df = (float *)w.lu, *e2f = df + 64;
+
+    for (int r = t; r < n; r += EX_THREADS) {
+        df[r] = (float)w.d[r];
+        if (r < n - 1)
+            e2f[r] = (float)w.e2[r];
+    }
+    __syncthreads();
+    for (int fr = 0; fr < 4 && hi - lo > 1.0e-6 * norm; fr++) {
+        const double xq = lo + (hi - lo) * ((double)(t + 1) / (double)(EX_THREADS + 1));
+        const bool gt = sturmf(df, e2f, n, (float)xq, 1.0e-30f + 1.0e-14f * (float)norm) > index;
+        const unsigned bal = __ballot_sync(FULL, gt);
+
+        if ((t & 31) == 0)
+            w.ints[2 + (t >> 5)] = bal ? (t & ~31) + __ffs(bal) - 1 : EX_THREADS;
+        __syncthreads();
+        const int f = min(min(w.ints[2], w.ints[3]), min(w.ints[4], w.ints[5]));
+        const double nlo = f == 0 ? lo : lo + (hi - lo) * ((double)f / (double)(EX_THREADS + 1));
+        const double nhi =
+            f == EX_THREADS ? hi : lo + (hi - lo) * ((double)(f + 1) / (double)(EX_THREADS + 1));
+
+        __syncthreads();
+        lo = nlo;
+        hi = nhi;
+    }
+    lo -= 4.0e-7 * norm;
+    hi += 4.0e-7 * norm;
     const double pivmin = 1e-290 + 1e-28 * norm;
     int round = 0;
 
