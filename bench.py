@@ -297,6 +297,10 @@ def crop_accuracy(crop, coh_gpu, count_gpu, size, n, kw, flips_size=64):
         "crop_run_equals_timed_run": bool(np.array_equal(r["coh"], coh_gpu, equal_nan=True)),
         "fp64_tier_fraction": float(((r["status"][m] & tcoh_b200.STATUS_FP64) != 0).mean())
         if m.any() else None,
+        "emi_pivoted_fraction": float(((r["status"][m] & tcoh_b200.STATUS_EMI_PIVOTED) != 0)
+                                      .mean()) if m.any() else None,
+        "emi_pinv_fraction": float(((r["status"][m] & tcoh_b200.STATUS_EMI_PINV) != 0).mean())
+        if m.any() else None,
         "oracle_seconds": t_oracle,
     }
     pm = ~np.isnan(o["pairs"]) & ~np.isnan(r["pairs"])

@@ -1173,14 +1173,17 @@ __device__ void ex_gram(const TcStrip &s, const float2 *slc, int py0, int px0, i
     for (int c0 = 0; c0 < ncand; c0 += EX_KC) {
         const int kc = min(EX_KC, ncand - c0);
 
-        for (int e = t; e < kc * n; e += EX_THREADS) {
-            const int q = e / n, d = e - q * n;
+        for (int q = t >> 5; q < kc; q += EX_THREADS / 32) {
             const int u = w.cand[c0 + q], dy = u / s.wr, dx = u - dy * s.wr;
-            float2 v = slc[((long long)(py0 + dy) * s.W + px0 + dx) * n + d];
+            const float2 *src = slc + ((long long)(py0 + dy) * s.W + px0 + dx) * n;
 
-            if (!isfinite(v.x) || !isfinite(v.y))
-                v = make_float2(0.f, 0.f);
-            w.stage[e] = v;
+            for (int d = t & 31; d < n; d += 32) {
+                float2 v = src[d];
+
+                if (!isfinite(v.x) || !isfinite(v.y))
+                    v = make_float2(0.f, 0.f);
+                w.stage[q * n + d] = v;
+            }
         }
         __syncthreads();
 #pragma unroll
@@ -1312,23 +1315,52 @@ __device__ bool ex_linked(int n, const ExWs &w)
 }
 
 /* A^-1 in place of the packed symmetric A by the symmetric sweep
-   (Gauss-Jordan elimination without pivoting in the form that keeps the
-   matrix symmetric; Goodnight, The American Statistician 33, 1979):
-   sweeping pivot k maps a_ij -> a_ij - a_ik a_kj / a_kk,
-   a_ik, a_kj -> a_ik / a_kk, a_kk -> -1 / a_kk, and all pivots leave
-   -A^-1, negated back at the end. It takes indefinite matrices. False when
-   a pivot's magnitude is not above floor_ (A is then undefined). */
+   (Gauss-Jordan elimination in the form that keeps the matrix symmetric;
+   Goodnight, The American Statistician 33, 1979): sweeping pivot k maps
+   a_ij -> a_ij - a_ik a_kj / a_kk, a_ik, a_kj -> a_ik / a_kk,
+   a_kk -> -1 / a_kk, and sweeping every index once, in any order, leaves
+   -A^-1, negated back at the end. The next pivot is the unswept index with
+   the largest diagonal magnitude, which keeps indefinite and
+   ill-conditioned matrices away from small pivots. False when that
+   magnitude is not above floor_ (A is then undefined). */
 __device__ bool ex_sweep(int n, int npu, const ExWs &w, double *A, double floor_)
 {
-    const int t = threadIdx.x;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    unsigned long long swept = 0ull;
 
-    for (int kp = 0; kp < n; kp++) {
-        const double d = A[tc_pidx(n, kp, kp)];
+    for (int step = 0; step < n; step++) {
+        double v = t < n && !((swept >> t) & 1ull) ? fabs(A[tc_pidx(n, t, t)]) : -1.0;
+        int idx = t;
 
-        if (!(fabs(d) > floor_)) {
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const double ov = __shfl_xor_sync(FULL, v, o);
+            const int oi = __shfl_xor_sync(FULL, idx, o);
+
+            if (ov > v || (ov == v && oi < idx)) {
+                v = ov;
+                idx = oi;
+            }
+        }
+        if (lane == 0) {
+            w.red[warp] = v;
+            w.ints[2 + warp] = idx;
+        }
+        __syncthreads();
+        int kp = w.ints[2];
+        double best = w.red[0];
+
+        for (int q = 1; q < EX_THREADS / 32; q++)
+            if (w.red[q] > best) {
+                best = w.red[q];
+                kp = w.ints[2 + q];
+            }
+        if (!(best > floor_)) {
             __syncthreads();
             return false;
         }
+        swept |= 1ull << kp;
+        const double d = A[tc_pidx(n, kp, kp)];
         const double id = 1.0 / d;
 
         for (int j = t; j < n; j += EX_THREADS)
@@ -1443,12 +1475,10 @@ __device__ bool ex_gauss_jordan(int n, const ExWs &w, double *A)
         for (int i = t; i < n; i += EX_THREADS)
             w.rrow[i] = i == k ? 0.0 : A[i * n + k];
         __syncthreads();
-        for (int e = t; e < n * n; e += EX_THREADS) {
-            const int i = e / n, j = e - i * n;
-
+        for (int i = warp; i < n; i += EX_THREADS / 32)
             if (i != k)
-                A[e] = (j == k ? 0.0 : A[e]) - A[k * n + j] * w.rrow[i];
-        }
+                for (int j = lane; j < n; j += 32)
+                    A[i * n + j] = (j == k ? 0.0 : A[i * n + j]) - A[k * n + j] * w.rrow[i];
         __syncthreads();
     }
     /* undo the row swaps on the columns of the inverse, last swap first */
@@ -1468,7 +1498,8 @@ __device__ bool ex_gauss_jordan(int n, const ExWs &w, double *A)
 }
 
 /* |T|^-1 into w.G (which holds |T|), in tiers: the symmetric sweep with
-   pivots above 1e-5; else Gauss-Jordan elimination with partial pivoting
+   pivots (largest diagonal first) above 1e-5; else Gauss-Jordan
+   elimination with partial pivoting
    on the full |T| (in shared memory, the staged samples' region, up to 32
    dates; in the CTA's global scratch W above); else, or when the inverse is
    not moderate, the Jacobi eigen-pseudo-inverse with the absolute floor
@@ -1481,12 +1512,12 @@ __device__ unsigned ex_inverse(int n, int npu, int ld, const ExWs &w, double *W)
         return 0;
     double *A = n <= 32 ? (double *)w.stage : W;
 
-    for (int e = t; e < n * n; e += EX_THREADS) {
-        const int i = e / n, j = e - i * n;
-        const double2 v = ex_m(w.T, n, i, j);
+    for (int i = t >> 5; i < n; i += EX_THREADS / 32)
+        for (int j = t & 31; j < n; j += 32) {
+            const double2 v = ex_m(w.T, n, i, j);
 
-        A[e] = i == j ? 1.0 : hypot(v.x, v.y);
-    }
+            A[i * n + j] = i == j ? 1.0 : hypot(v.x, v.y);
+        }
     __syncthreads();
     if (ex_gauss_jordan(n, w, A)) {
         for (int q = t; q < npu; q += EX_THREADS) {
@@ -1496,7 +1527,7 @@ __device__ unsigned ex_inverse(int n, int npu, int ld, const ExWs &w, double *W)
         }
         __syncthreads();
         if (ex_moderate(n, npu, w, w.G))
-            return TC_STATUS_EMI_PINV;
+            return TC_STATUS_EMI_PIVOTED;
     }
     __syncthreads();
     unsigned st = TC_STATUS_EMI_PINV;

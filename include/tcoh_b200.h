@@ -101,7 +101,7 @@ struct tc_options {
 };
 
 /* Status bits per pixel (tc_run_ex). */
-#define TC_STATUS_EMI_PINV   1 /* EMI: |T| not safely positive definite,
+#define TC_STATUS_EMI_PINV   1 /* EMI: |T| (numerically) singular or nearly,
                                   inverted by its eigen-pseudo-inverse */
 #define TC_STATUS_UNLINKED   2 /* bias correction unlinked the dates */
 #define TC_STATUS_ITER_CAP   4 /* an iterative solver reached its cap */
@@ -113,6 +113,9 @@ struct tc_options {
                                   than ~1e-5; with the bias correction, the
                                   pixels with an entry at the threshold of
                                   the correction */
+#define TC_STATUS_EMI_PIVOTED 16 /* EMI: |T| inverted by elimination with
+                                    pivoting (the symmetric sweep met a
+                                    pivot below 1e-5) */
 
 /* Message of the last failed tc_* call of this thread. */
 const char *tc_last_error(void);
