@@ -1315,52 +1315,23 @@ __device__ bool ex_linked(int n, const ExWs &w)
 }
 
 /* A^-1 in place of the packed symmetric A by the symmetric sweep
-   (Gauss-Jordan elimination in the form that keeps the matrix symmetric;
-   Goodnight, The American Statistician 33, 1979): sweeping pivot k maps
-   a_ij -> a_ij - a_ik a_kj / a_kk, a_ik, a_kj -> a_ik / a_kk,
-   a_kk -> -1 / a_kk, and sweeping every index once, in any order, leaves
-   -A^-1, negated back at the end. The next pivot is the unswept index with
-   the largest diagonal magnitude, which keeps indefinite and
-   ill-conditioned matrices away from small pivots. False when that
-   magnitude is not above floor_ (A is then undefined). */
+   (Gauss-Jordan elimination without pivoting in the form that keeps the
+   matrix symmetric; Goodnight, The American Statistician 33, 1979):
+   sweeping pivot k maps a_ij -> a_ij - a_ik a_kj / a_kk,
+   a_ik, a_kj -> a_ik / a_kk, a_kk -> -1 / a_kk, and all pivots leave
+   -A^-1, negated back at the end. It takes indefinite matrices. False when
+   a pivot's magnitude is not above floor_ (A is then undefined). */
 __device__ bool ex_sweep(int n, int npu, const ExWs &w, double *A, double floor_)
 {
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    unsigned long long swept = 0ull;
+    const int t = threadIdx.x;
 
-    for (int step = 0; step < n; step++) {
-        double v = t < n && !((swept >> t) & 1ull) ? fabs(A[tc_pidx(n, t, t)]) : -1.0;
-        int idx = t;
+    for (int kp = 0; kp < n; kp++) {
+        const double d = A[tc_pidx(n, kp, kp)];
 
-#pragma unroll
-        for (int o = 16; o; o >>= 1) {
-            const double ov = __shfl_xor_sync(FULL, v, o);
-            const int oi = __shfl_xor_sync(FULL, idx, o);
-
-            if (ov > v || (ov == v && oi < idx)) {
-                v = ov;
-                idx = oi;
-            }
-        }
-        if (lane == 0) {
-            w.red[warp] = v;
-            w.ints[2 + warp] = idx;
-        }
-        __syncthreads();
-        int kp = w.ints[2];
-        double best = w.red[0];
-
-        for (int q = 1; q < EX_THREADS / 32; q++)
-            if (w.red[q] > best) {
-                best = w.red[q];
-                kp = w.ints[2 + q];
-            }
-        if (!(best > floor_)) {
+        if (!(fabs(d) > floor_)) {
             __syncthreads();
             return false;
         }
-        swept |= 1ull << kp;
-        const double d = A[tc_pidx(n, kp, kp)];
         const double id = 1.0 / d;
 
         for (int j = t; j < n; j += EX_THREADS)
@@ -1498,8 +1469,7 @@ __device__ bool ex_gauss_jordan(int n, const ExWs &w, double *A)
 }
 
 /* |T|^-1 into w.G (which holds |T|), in tiers: the symmetric sweep with
-   pivots (largest diagonal first) above 1e-5; else Gauss-Jordan
-   elimination with partial pivoting
+   pivots above 1e-5; else Gauss-Jordan elimination with partial pivoting
    on the full |T| (in shared memory, the staged samples' region, up to 32
    dates; in the CTA's global scratch W above); else, or when the inverse is
    not moderate, the Jacobi eigen-pseudo-inverse with the absolute floor

@@ -261,161 +261,6 @@ cudaError_t tc_launch_logstats(const TcStrip &s, const float *amp,
     return cudaGetLastError();
 }
 
-/* KS and AD with the candidates' series staged once per CTA: the CTA's
-   8 warps take 8 horizontally adjacent pixels (one row of a tile), whose
-   windows together cover WA x (8 + WR - 1) padded cells; their sorted
-   amplitudes (and validity) come into shared memory with coalesced loads,
-   once for the 8 pixels, instead of every lane reading its candidate's
-   series from another pixel's cache line. Each warp then copies its
-   lanes' candidates into its transposed column buffer and walks the merges
-   exactly as tc_shp_kernel does (same decisions, bit for bit). */
-template <int TEST>
-__global__ void __launch_bounds__(256)
-tc_shp_union_kernel(TcStrip s, TcChunk c, TcShpConst k, const float *__restrict__ amp,
-                    const unsigned char *__restrict__ valid, uint32_t *__restrict__ mask,
-                    int *__restrict__ count)
-{
-    extern __shared__ float sm[];
-    const int n = s.n;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int UW = TC_TILE_W + s.wr - 1, U = s.wa * UW;
-    const int tab_len = TEST == 1 ? (n + 1) * (2 * n - 1) : 0;
-    float *tab = sm;
-    float *ustage = sm + tab_len;                 /* [U][n] */
-    float *wbuf = ustage + U * n + warp * ((n + 1) + (n + 1) * 32);
-    float *a_s = wbuf;                            /* n + 1 */
-    float *b_s = wbuf + n + 1;                    /* (n + 1) x 32 */
-    unsigned char *uvalid = (unsigned char *)(ustage + U * n + 8 * ((n + 1) + (n + 1) * 32));
-
-    if (TEST == 1) {
-        /* fl((2Nm - jN)^2 / (j (2N - j))), j = 1 .. 2N-1, m = 0 .. N. */
-        for (int i = threadIdx.x; i < tab_len; i += blockDim.x) {
-            const int m = i % (n + 1), j = i / (n + 1) + 1;
-            const float num = (float)(2 * n * m - j * n);
-
-            tab[i] = __fdiv_rn(__fmul_rn(num, num), (float)(j * (2 * n - j)));
-        }
-    }
-    for (int pg = blockIdx.x * 8; pg < c.npix; pg += gridDim.x * 8) {
-        int y, x0;
-
-        tc_pixel_yx(c, pg, y, x0);
-        if (y >= c.row0 + c.nrows || y >= s.rows || x0 >= s.cols)
-            continue; /* the whole group (uniform over the CTA) */
-        __syncthreads(); /* the previous group's readers of ustage are done */
-        /* union rows y .. y + WA - 1 (padded), columns x0 .. x0 + UW - 1:
-           each union row's UW x n amplitudes are contiguous */
-        for (int e = threadIdx.x; e < U * n; e += blockDim.x) {
-            const int u = e / n, j = e - u * n;
-            const int uy = u / UW, col = x0 + (u - uy * UW);
-
-            ustage[e] = col < s.W ? amp[((long long)(y + uy) * s.W + col) * n + j] : 0.f;
-        }
-        for (int u = threadIdx.x; u < U; u += blockDim.x) {
-            const int uy = u / UW, col = x0 + (u - uy * UW);
-
-            uvalid[u] = col < s.W ? valid[(long long)(y + uy) * s.W + col] : 0;
-        }
-        __syncthreads();
-        const int p = pg + warp, x = x0 + warp;
-
-        if (x >= s.cols)
-            continue; /* this warp; the next group's barrier waits for all */
-        const long long out = (long long)y * s.cols + x;
-        const int uc = (s.wa / 2) * UW + warp + s.wr / 2;
-
-        if (!uvalid[uc]) {
-            for (int w = lane; w < s.mask_words; w += 32)
-                mask[(long long)w * c.npix + p] = 0u;
-            if (lane == 0)
-                count[out] = -1;
-            continue;
-        }
-        for (int j = lane; j < n; j += 32)
-            a_s[j] = ustage[uc * n + j];
-        if (lane == 0)
-            a_s[n] = INFINITY;
-        __syncwarp();
-        int looks = 0;
-
-        for (int w = 0; w < s.mask_words; w++) {
-            const int cand = w * 32 + lane;
-            bool ok = false;
-
-            if (cand < s.area) {
-                const int dy = cand / s.wr, dx = cand - dy * s.wr;
-                const int u = dy * UW + warp + dx;
-
-                if (uvalid[u]) {
-                    const float *b = ustage + u * n;
-
-                    for (int j = 0; j < n; j++)
-                        b_s[j * 32 + lane] = b[j];
-                    b_s[n * 32 + lane] = INFINITY;
-                    /* the merge walk of tc_shp_kernel */
-                    const float *bl = b_s + lane;
-                    int ia = 0, ib = 0;
-                    float av = a_s[0], bv = bl[0];
-
-                    if (TEST == 0) {
-                        int d = 0;
-
-#pragma unroll 4
-                        for (int j = 1; j < 2 * n; j++) {
-                            const bool ta = av <= bv;
-
-                            ia += ta;
-                            ib += !ta;
-                            const float v = *(ta ? a_s + ia : bl + ib * 32);
-
-                            av = ta ? v : av;
-                            bv = ta ? bv : v;
-                            d = max(d, abs(ia - ib));
-                        }
-                        ok = d <= k.ks_max;
-                    }
-                    else {
-                        float acc = 0.f;
-                        const float *tj = tab;
-
-#pragma unroll 4
-                        for (int j = 1; j < 2 * n; j++, tj += n + 1) {
-                            const bool ta = av <= bv;
-
-                            ia += ta;
-                            ib += !ta;
-                            const float v = *(ta ? a_s + ia : bl + ib * 32);
-
-                            av = ta ? v : av;
-                            bv = ta ? bv : v;
-                            acc = __fadd_rn(acc, tj[ia]);
-                        }
-                        ok = __fdiv_rn(__fsub_rn(__fmul_rn(k.ad_norm, acc), 1.0f),
-                                       k.ad_sigma) <= k.ad_crit;
-                    }
-                }
-            }
-            const uint32_t bits = __ballot_sync(0xffffffffu, ok);
-
-            if (lane == 0)
-                mask[(long long)w * c.npix + p] = bits;
-            looks += __popc(bits);
-        }
-        if (lane == 0)
-            count[out] = looks;
-        __syncwarp();
-    }
-}
-
-/* Shared memory of tc_shp_union_kernel (bytes). */
-static size_t shp_union_smem(const TcStrip &s, int test)
-{
-    const int n = s.n, U = s.wa * (TC_TILE_W + s.wr - 1);
-    const size_t tab = test == 1 ? (size_t)(n + 1) * (2 * n - 1) : 0;
-
-    return sizeof(float) * (tab + (size_t)U * n + 8 * ((n + 1) + (n + 1) * 32)) + U + 16;
-}
-
 cudaError_t tc_launch_shp(const TcStrip &s, const TcChunk &c, const TcShpConst &k,
                           const float *amp, const unsigned char *valid,
                           const float2 *logstat, uint32_t *mask, int *count, int sms,
@@ -429,32 +274,6 @@ cudaError_t tc_launch_shp(const TcStrip &s, const TcChunk &c, const TcShpConst &
     const uintptr_t base = (uintptr_t)amp;
     const int vec = (s.n % 4 == 0 && base % 16 == 0) ? 4 : (s.n % 2 == 0 && base % 8 == 0) ? 2 : 1;
     cudaError_t e;
-
-    /* KS and AD: candidates staged once per tile row when they fit */
-    const size_t usm = shp_union_smem(s, k.test);
-
-    if (k.test != 2 && usm <= 112 * 1024 && c.npix % 8 == 0) {
-        const int groups = c.npix / 8;
-        const int ublocks = groups < sms * 2 ? groups : sms * 2;
-
-        if (k.test == 0) {
-            e = cudaFuncSetAttribute(tc_shp_union_kernel<0>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)usm);
-            if (e == cudaSuccess)
-                tc_shp_union_kernel<0><<<ublocks, 256, usm, st>>>(s, c, k, amp, valid, mask,
-                                                                  count);
-        }
-        else {
-            e = cudaFuncSetAttribute(tc_shp_union_kernel<1>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)usm);
-            if (e == cudaSuccess)
-                tc_shp_union_kernel<1><<<ublocks, 256, usm, st>>>(s, c, k, amp, valid, mask,
-                                                                  count);
-        }
-        if (e != cudaSuccess)
-            return e;
-        return cudaGetLastError();
-    }
 
     switch (k.test) {
     case 0:
