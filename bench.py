@@ -630,6 +630,10 @@ def scene_workload(args, name):
                       "bound": bound, "peak_tflops": peak, "frac": achieved / peak}
     dom = max(kernels, key=lambda k: kernels[k]["ms_middle_strip"])
     d = kernels[dom]
+    if stages["exact"][1]:
+        # the exact tier on the pixels the float kernels queued for it
+        kernels["exact"] = {"ms_middle_strip": stages["exact"][0], "launches": stages["exact"][1],
+                            "bound": "fp64"}
     roofline = {"kernel": dom, "bound": d["bound"], "achieved": d["achieved_tflops"],
                 "peak": d["peak_tflops"], "unit": "TFLOP/s", "frac": d["frac"],
                 "traffic": None,
@@ -888,6 +892,10 @@ def main():
                          "bound": bound, "peak_tflops": peak, "frac": achieved / peak}
     dom = max(kernels, key=lambda k: kernels[k]["ms_per_step"])
     d = kernels[dom]
+    if stages["exact"][1]:
+        # the exact tier on the pixels the float kernels queued for it
+        kernels["exact"] = {"ms_per_step": stages["exact"][0], "launches": stages["exact"][1],
+                            "bound": "fp64"}
     roofline = {"kernel": dom, "bound": d["bound"], "achieved": d["achieved_tflops"],
                 "peak": d["peak_tflops"], "unit": "TFLOP/s",
                 "frac": d["frac"], "traffic": None,

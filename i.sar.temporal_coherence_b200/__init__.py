@@ -30,7 +30,7 @@ LIBRARY = os.path.join(HERE, "libtcoh_b200.so")
 SHP_TESTS = {"ks": 0, "ad": 1, "tlog": 2}
 GRAM_TENSOR, GRAM_FP32 = 0, 1
 STATUS_EMI_PINV, STATUS_UNLINKED, STATUS_ITER_CAP, STATUS_FP64, STATUS_EMI_PIVOTED = 1, 2, 4, 8, 16
-STAGES = ("prep", "shp", "gram", "link", "copy", "adjoint")
+STAGES = ("prep", "shp", "gram", "link", "copy", "adjoint", "exact")
 
 # Exported symbols of include/tcoh_b200.h.
 EXPORTS = (

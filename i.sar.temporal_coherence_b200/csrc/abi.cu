@@ -216,7 +216,7 @@ static cudaError_t ensure(DevBuf &b, size_t size)
     return e;
 }
 
-enum { ST_PREP, ST_SHP, ST_GRAM, ST_LINK, ST_COPY, ST_ADJOINT, ST_COUNT };
+enum { ST_PREP, ST_SHP, ST_GRAM, ST_LINK, ST_COPY, ST_ADJOINT, ST_EXACT, ST_COUNT };
 
 /* tc_run_ex copies a strip in this many row blocks on a second stream, and
    each chunk waits only for the blocks holding its rows. */
@@ -641,8 +641,31 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
     CK(ensure(o->mask, sizeof(uint32_t) * s.mask_words * max_npix));
     CK(ensure(o->gram, sizeof(float2) * tc_npu(o->n) * max_npix));
     CK(ensure(o->link_scratch, tc_link_scratch_bytes(o->n, o->sms)));
-    if (o->emi || o->bias)
-        CK(ensure(o->exact_list, sizeof(int) * (max_npix + 1)));
+    TcLinkConst lk;
+
+    lk.emi = o->emi;
+    lk.bias = o->bias;
+    lk.min_looks = o->min_looks;
+    lk.npairs = o->npairs;
+    lk.pairs_all = o->pairs_all;
+    /* the exact tier's queue: about 32 MB, at least one chunk, at most 16
+       chunks (a flush is one launch over the queued pixels of its chunks) */
+    TcExactQueue q = {};
+
+    if (!adj && tc_link_queues(o->n, lk)) {
+        const long long entry = 4ll * (1 + s.mask_words);
+        long long cap = (32ll << 20) / entry;
+
+        if (cap > 16 * max_npix)
+            cap = 16 * max_npix;
+        if (cap < max_npix)
+            cap = max_npix;
+        CK(ensure(o->exact_list, tc_exact_queue_bytes(s.mask_words, cap)));
+        q.buf = (int *)o->exact_list.p;
+        q.stride = 1 + s.mask_words;
+        q.capacity = cap;
+        CK(cudaMemsetAsync(q.buf, 0, sizeof(int), st));
+    }
     if (o->opt.gram == TC_GRAM_FP32)
         CK(ensure(o->soa, sizeof(float2) * s.planes * s.npad));
     if (o->test == SHP_TLOG)
@@ -663,13 +686,6 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
         CK(tc_launch_logstats(s, amp, valid, (float2 *)o->logstat.p, st));
         tm.end(t);
     }
-    TcLinkConst lk;
-
-    lk.emi = o->emi;
-    lk.bias = o->bias;
-    lk.min_looks = o->min_looks;
-    lk.npairs = o->npairs;
-    lk.pairs_all = o->pairs_all;
     if (mark_chunks) {
         const size_t nchunks = (size_t)((rows + crows - 1) / crows);
 
@@ -680,6 +696,26 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
             o->chunk_done.push_back(ev);
         }
     }
+    /* chunks whose outputs the queued exact-tier pixels may still change:
+       their completion events follow the flush */
+    int unflushed = 0;
+    auto flush = [&](int upto) -> int {
+        if (q.buf) {
+            const int tf = q.pending > 0 ? tm.begin(ST_EXACT) : -1;
+
+            CK(tc_flush_exact(s, lk, &q, slc, count, (const unsigned short *)o->upper_tab.p,
+                              (const unsigned short *)o->pair_tab.p,
+                              (double *)o->link_scratch.p, coh, pairs, phases, status, o->sms,
+                              st));
+            tm.end(tf);
+        }
+        if (mark_chunks)
+            for (; unflushed < upto; unflushed++)
+                CK(cudaEventRecord(o->chunk_done[unflushed], st));
+        unflushed = upto;
+        return TC_OK;
+    };
+
     for (int row0 = 0, chunk = 0; row0 < rows; row0 += crows, chunk++) {
         TcChunk c;
 
@@ -715,10 +751,16 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
                                          (const uint32_t *)o->mask.p, (float2 *)o->gram.p, st));
             tm.end(t);
         }
+        if (q.buf && q.pending + c.npix > q.capacity) {
+            const int rc = flush(chunk);
+
+            if (rc != TC_OK)
+                return rc;
+        }
         t = tm.begin(ST_LINK);
         if (!adj)
             CK(tc_launch_link(s, c, lk, (const float2 *)o->gram.p, slc,
-                              (const uint32_t *)o->mask.p, count, (int *)o->exact_list.p,
+                              (const uint32_t *)o->mask.p, count, &q,
                               (const unsigned short *)o->upper_tab.p,
                               (const unsigned short *)o->pair_tab.p,
                               (double *)o->link_scratch.p, coh, pairs, phases, status, o->sms,
@@ -740,10 +782,14 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
                                              (const uint32_t *)o->mask.p, slc, adj->dtheta, st));
         }
         tm.end(t);
-        if (mark_chunks)
-            CK(cudaEventRecord(o->chunk_done[row0 / crows], st));
+        if (!q.buf) {
+            const int rc = flush(chunk + 1);
+
+            if (rc != TC_OK)
+                return rc;
+        }
     }
-    return TC_OK;
+    return flush((rows + crows - 1) / crows);
 }
 
 TC_API int tc_run_device(struct ocl *o, const float *slc, const float *amp,

@@ -882,7 +882,7 @@ tc_link_smem_kernel(TcStrip s, TcChunk c, TcLinkConst k, LinkLayout L,
                     const unsigned short *__restrict__ pair_tab, double *__restrict__ scratch,
                     float *__restrict__ coh, float *__restrict__ pairs,
                     float *__restrict__ phases, unsigned char *__restrict__ status,
-                    int *__restrict__ exact_list)
+                    const uint32_t *__restrict__ mask, int *__restrict__ queue, int qstride)
 {
     extern __shared__ double smd[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -916,8 +916,8 @@ tc_link_smem_kernel(TcStrip s, TcChunk c, TcLinkConst k, LinkLayout L,
         bool boundary = false;
 
         load_coherence(s, c, k, p, looks, gram, upper_tab, w, ld, lane, boundary);
-        if (exact_list && boundary && lane == 0)
-            exact_list[1 + atomicAdd(exact_list, 1)] = p;
+        if (queue && boundary && lane == 0)
+            tc_exact_push(queue, qstride, out, mask, c.npix, p);
         for (int q = lane; q < k.npairs; q += 32) {
             const int i = pair_tab[q] >> 8, j = pair_tab[q] & 255;
             const float2 t = w.T[i * ld + j];
@@ -1113,13 +1113,14 @@ __device__ __forceinline__ double2 ex_m(const double2 *P, int n, int i, int j)
     return make_double2(m.x, -m.y);
 }
 
-/* The pixel's SHP candidates (window indices) into w.cand; their number. */
-__device__ int ex_candidates(const TcStrip &s, const TcChunk &c, const uint32_t *mask, int p,
+/* The pixel's SHP candidates (window indices) into w.cand; their number.
+   Mask word i of the pixel is words[i * stride]. */
+__device__ int ex_candidates(const TcStrip &s, const uint32_t *words, long long stride,
                              const ExWs &w)
 {
     if (threadIdx.x < 32) {
         const int lane = threadIdx.x;
-        uint32_t bits = lane < s.mask_words ? mask[(long long)lane * c.npix + p] : 0u;
+        uint32_t bits = lane < s.mask_words ? words[lane * stride] : 0u;
 
         if (lane == s.mask_words - 1 && (s.area & 31))
             bits &= (1u << (s.area & 31)) - 1u; /* candidates only */
@@ -1952,11 +1953,12 @@ __device__ float ex_gamma(int n, int npu, const ExWs &w)
     return (float)(hypot(ssum.x, ssum.y) / (0.5 * n * (n - 1)));
 }
 
-/* list: null for every pixel of the chunk, else list[0] pixels list[1 ..]. */
+/* queue: null for every pixel of the chunk c (with its mask), else the
+   queue's entries (TcExactQueue, any pixels of the strip; c unused). */
 __global__ void __launch_bounds__(EX_THREADS, EX_CTAS)
 tc_link_exact_kernel(TcStrip s, TcChunk c, TcLinkConst k, ExLayout L,
                      const float2 *__restrict__ slc, const uint32_t *__restrict__ mask,
-                     const int *__restrict__ count, const int *__restrict__ list,
+                     const int *__restrict__ count, const int *__restrict__ queue, int qstride,
                      const unsigned short *__restrict__ upper_tab,
                      const unsigned short *__restrict__ pair_tab, double *__restrict__ scratch,
                      float *__restrict__ coh, float *__restrict__ pairs,
@@ -1979,15 +1981,21 @@ tc_link_exact_kernel(TcStrip s, TcChunk c, TcLinkConst k, ExLayout L,
                 w.blk[b++] = (unsigned short)(ip << 8 | jg);
     }
     __syncthreads();
-    const int total = list ? list[0] : c.npix;
+    const int total = queue ? queue[0] : c.npix;
 
     for (int it = blockIdx.x; it < total; it += gridDim.x) {
-        const int p = list ? list[1 + it] : it;
+        const int *entry = queue ? queue + 1 + (long long)it * qstride : nullptr;
         int y, x;
 
-        tc_pixel_yx(c, p, y, x);
-        if (y >= c.row0 + c.nrows || y >= s.rows || x >= s.cols)
-            continue;
+        if (entry) {
+            y = entry[0] / s.cols;
+            x = entry[0] - y * s.cols;
+        }
+        else {
+            tc_pixel_yx(c, it, y, x);
+            if (y >= c.row0 + c.nrows || y >= s.rows || x >= s.cols)
+                continue;
+        }
         const long long out = (long long)y * s.cols + x;
         const int looks = count[out];
 
@@ -2003,7 +2011,9 @@ tc_link_exact_kernel(TcStrip s, TcChunk c, TcLinkConst k, ExLayout L,
                 status[out] = 0;
             continue;
         }
-        const int ncand = ex_candidates(s, c, mask, p, w);
+        const int ncand =
+            entry ? ex_candidates(s, (const uint32_t *)entry + 1, 1, w)
+                  : ex_candidates(s, mask + it, c.npix, w);
 
         ex_gram(s, slc, y, x, ncand, w, L);
         ex_coherence(n, npu, k, looks, w);
@@ -2096,22 +2106,27 @@ static size_t exact_scratch_bytes(int n, int sms)
 
 static cudaError_t launch_exact(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
                                 const float *slc, const uint32_t *mask, const int *count,
-                                const int *list, const unsigned short *upper_tab,
+                                const TcExactQueue *q, const unsigned short *upper_tab,
                                 const unsigned short *pair_tab, double *scratch, float *coh,
                                 float *pairs, float *phases, unsigned char *status, int sms,
                                 cudaStream_t st)
 {
     const ExLayout L = ex_layout(s.n, s.area);
     const int ctas = sms * EX_CTAS;
-    const int blocks = list ? ctas : (c.npix < ctas ? c.npix : ctas);
+    int blocks = ctas;
+
+    if (!q && c.npix < ctas)
+        blocks = c.npix;
+    if (q && q->pending < ctas)
+        blocks = (int)q->pending;
     cudaError_t e = cudaFuncSetAttribute(tc_link_exact_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, L.bytes);
 
     if (e != cudaSuccess)
         return e;
     tc_link_exact_kernel<<<blocks, EX_THREADS, L.bytes, st>>>(
-        s, c, k, L, (const float2 *)slc, mask, count, list, upper_tab, pair_tab, scratch, coh,
-        pairs, phases, status);
+        s, c, k, L, (const float2 *)slc, mask, count, q ? q->buf : nullptr, q ? q->stride : 0,
+        upper_tab, pair_tab, scratch, coh, pairs, phases, status);
     return cudaGetLastError();
 }
 
@@ -2128,57 +2143,82 @@ size_t tc_link_scratch_bytes(int n, int sms)
     return a > b ? a : b;
 }
 
+bool tc_link_queues(int n, const TcLinkConst &k)
+{
+    /* the float kernels hand pixels to the exact tier with EMI and with
+       the bias correction; EMI above 32 dates is all exact */
+    return (k.emi || k.bias) && !(n > 32 && k.emi);
+}
+
+size_t tc_exact_queue_bytes(int mask_words, long long capacity)
+{
+    return sizeof(int) * (1 + (size_t)capacity * (1 + mask_words));
+}
+
+cudaError_t tc_flush_exact(const TcStrip &s, const TcLinkConst &k, TcExactQueue *q,
+                           const float *slc, const int *count, const unsigned short *upper_tab,
+                           const unsigned short *pair_tab, double *scratch, float *coh,
+                           float *pairs, float *phases, unsigned char *status, int sms,
+                           cudaStream_t st)
+{
+    cudaError_t e = cudaSuccess;
+
+    if (q->pending > 0) {
+        TcChunk none = {};
+
+        if ((e = launch_exact(s, none, k, slc, nullptr, count, q, upper_tab, pair_tab, scratch,
+                              coh, pairs, phases, status, sms, st)) == cudaSuccess)
+            e = cudaMemsetAsync(q->buf, 0, sizeof(int), st);
+    }
+    q->pending = 0;
+    return e;
+}
+
 cudaError_t tc_launch_link(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
                            const float2 *gram, const float *slc, const uint32_t *mask,
-                           const int *count, int *exact_list,
+                           const int *count, TcExactQueue *q,
                            const unsigned short *upper_tab, const unsigned short *pair_tab,
                            double *scratch, float *coh, float *pairs, float *phases,
                            unsigned char *status, int sms, cudaStream_t st)
 {
     cudaError_t e;
+    const bool queued = tc_link_queues(s.n, k);
 
-    /* the float kernels hand pixels to the exact tier with EMI and with
-       the bias correction */
-    int *list = k.emi || k.bias ? exact_list : nullptr;
-
-    if ((k.emi || k.bias) && !exact_list)
+    if (queued && (!q || !q->buf || q->stride != 1 + s.mask_words ||
+                   q->pending + c.npix > q->capacity))
         return cudaErrorInvalidValue;
+    int *qb = queued ? q->buf : nullptr;
+    const int qs = queued ? q->stride : 0;
+
     if (s.n > 32 && k.emi)
         return launch_exact(s, c, k, slc, mask, count, nullptr, upper_tab, pair_tab, scratch, coh,
                             pairs, phases, status, sms, st);
-    if (list && (e = cudaMemsetAsync(list, 0, sizeof(int), st)) != cudaSuccess)
-        return e;
-    if (s.n <= 32) {
-        if ((e = tc_launch_link_half(s, c, k, gram, count, upper_tab, pair_tab, scratch, coh,
-                                     pairs, phases, status, list, sms, st)) != cudaSuccess)
-            return e;
-        if (!list)
-            return cudaSuccess;
-        return launch_exact(s, c, k, slc, mask, count, list, upper_tab, pair_tab, scratch, coh,
-                            pairs, phases, status, sms, st);
+    if (s.n <= 32)
+        e = tc_launch_link_half(s, c, k, gram, mask, count, upper_tab, pair_tab, scratch, coh,
+                                pairs, phases, status, qb, qs, sms, st);
+    else {
+        const LinkLayout L = layout_for(s.n, 0, false);
+        const size_t per_warp = (size_t)L.per_warp * sizeof(double);
+        int wpb = (int)((227 * 1024) / per_warp);
+
+        if (wpb > 8)
+            wpb = 8;
+        if (wpb < 1)
+            return cudaErrorInvalidConfiguration;
+        const size_t smem = per_warp * wpb;
+        const int want = (c.npix + wpb - 1) / wpb;
+        const int blocks = want < sms ? want : sms;
+
+        e = cudaFuncSetAttribute(tc_link_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        if (e == cudaSuccess)
+            tc_link_smem_kernel<<<blocks, wpb * 32, smem, st>>>(
+                s, c, k, L, gram, count, upper_tab, pair_tab, scratch, coh, pairs, phases, status,
+                mask, qb, qs);
+        if (e == cudaSuccess)
+            e = cudaGetLastError();
     }
-    const LinkLayout L = layout_for(s.n, 0, false);
-    const size_t per_warp = (size_t)L.per_warp * sizeof(double);
-    int wpb = (int)((227 * 1024) / per_warp);
-
-    if (wpb > 8)
-        wpb = 8;
-    if (wpb < 1)
-        return cudaErrorInvalidConfiguration;
-    const size_t smem = per_warp * wpb;
-    const int want = (c.npix + wpb - 1) / wpb;
-    const int blocks = want < sms ? want : sms;
-
-    e = cudaFuncSetAttribute(tc_link_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
-    if (e == cudaSuccess)
-        tc_link_smem_kernel<<<blocks, wpb * 32, smem, st>>>(
-            s, c, k, L, gram, count, upper_tab, pair_tab, scratch, coh, pairs, phases, status,
-            list);
-    if (e == cudaSuccess)
-        e = cudaGetLastError();
-    if (e != cudaSuccess || !list)
-        return e;
-    return launch_exact(s, c, k, slc, mask, count, list, upper_tab, pair_tab, scratch, coh, pairs,
-                        phases, status, sms, st);
+    if (e == cudaSuccess && queued)
+        q->pending += c.npix;
+    return e;
 }

@@ -1651,7 +1651,8 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
                     const unsigned short *__restrict__ pair_tab, double *__restrict__ scratch,
                     float *__restrict__ coh, float *__restrict__ pairs,
                     float *__restrict__ phases, unsigned char *__restrict__ status,
-                    float2 *__restrict__ gbar, int *__restrict__ exact_list)
+                    float2 *__restrict__ gbar, const uint32_t *__restrict__ mask,
+                    int *__restrict__ queue, int qstride)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1710,10 +1711,10 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
             bool boundary = false;
 
             load_T(s, c, k, p, active, looks, gram, s_upper, w, ld, g, boundary);
-            if (exact_list && active && boundary) {
+            if (queue && active && boundary) {
                 sent = true;
                 if (g.gl == 0)
-                    exact_list[1 + atomicAdd(exact_list, 1)] = p;
+                    tc_exact_push(queue, qstride, out, mask, c.npix, p);
             }
             if (active)
                 for (int t = g.gl; t < k.npairs; t += 16) {
@@ -1816,7 +1817,7 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
                    30 and 60 dates against the FP64 oracle: with the bound
                    3e4, no unflagged pixel was off by more than 1.1e-5, the
                    worst pixels sitting at 1.4e5 and above. */
-                if (exact_list && active && !sent) {
+                if (queue && active && !sent) {
                     const double delta = inv_max * (double)norm / 3.0e4;
                     bool flag = !(delta < (double)norm);
 
@@ -1824,7 +1825,7 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
                         flag = sturm16(w.d, w.e2f, n, lambda + (float)delta,
                                        1.0e-30f + 1.0e-14f * norm) >= 2;
                     if (flag && g.gl == 0)
-                        exact_list[1 + atomicAdd(exact_list, 1)] = p;
+                        tc_exact_push(queue, qstride, out, mask, c.npix, p);
                 }
             }
             __syncthreads();
@@ -1918,7 +1919,8 @@ static cudaError_t launch_half(const TcStrip &s, const TcChunk &c, const TcLinkC
                                const float2 *gram, const int *count,
                                const unsigned short *upper_tab, const unsigned short *pair_tab,
                                double *scratch, float *coh, float *pairs, float *phases,
-                               unsigned char *status, float2 *gbar, int *exact_list, int sms,
+                               unsigned char *status, float2 *gbar, const uint32_t *mask,
+                               int *queue, int qstride, int sms,
                                cudaStream_t st)
 {
     const HalfLayout L = half_layout(s.n, EMI, ADJ);
@@ -1941,22 +1943,24 @@ static cudaError_t launch_half(const TcStrip &s, const TcChunk &c, const TcLinkC
         return e;
     tc_link_half_kernel<EMI, ADJ><<<blocks, wpb * 32, smem, st>>>(
         s, c, k, L, gram, count, upper_tab, pair_tab, scratch, coh, pairs, phases, status, gbar,
-        exact_list);
+        mask, queue, qstride);
     return cudaGetLastError();
 }
 
 cudaError_t tc_launch_link_half(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
-                                const float2 *gram, const int *count,
+                                const float2 *gram, const uint32_t *mask, const int *count,
                                 const unsigned short *upper_tab, const unsigned short *pair_tab,
                                 double *scratch, float *coh, float *pairs, float *phases,
-                                unsigned char *status, int *exact_list, int sms,
+                                unsigned char *status, int *queue, int qstride, int sms,
                                 cudaStream_t st)
 {
     if (k.emi)
         return launch_half<true, false>(s, c, k, gram, count, upper_tab, pair_tab, scratch, coh,
-                                        pairs, phases, status, nullptr, exact_list, sms, st);
+                                        pairs, phases, status, nullptr, mask, queue, qstride,
+                                        sms, st);
     return launch_half<false, false>(s, c, k, gram, count, upper_tab, pair_tab, scratch, coh,
-                                     pairs, phases, status, nullptr, exact_list, sms, st);
+                                     pairs, phases, status, nullptr, mask, queue, qstride, sms,
+                                     st);
 }
 
 cudaError_t tc_launch_link_adjoint(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
@@ -1969,7 +1973,8 @@ cudaError_t tc_launch_link_adjoint(const TcStrip &s, const TcChunk &c, const TcL
         return cudaErrorInvalidValue;
     if (k.emi)
         return launch_half<true, true>(s, c, k, gram, count, upper_tab, pair_tab, scratch, coh,
-                                       pairs, nullptr, nullptr, gbar, nullptr, sms, st);
+                                       pairs, nullptr, nullptr, gbar, nullptr, nullptr, 0, sms,
+                                       st);
     return launch_half<false, true>(s, c, k, gram, count, upper_tab, pair_tab, scratch, coh,
-                                    pairs, nullptr, nullptr, gbar, nullptr, sms, st);
+                                    pairs, nullptr, nullptr, gbar, nullptr, nullptr, 0, sms, st);
 }

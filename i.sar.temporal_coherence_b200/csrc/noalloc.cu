@@ -90,8 +90,8 @@ static size_t substrip_bytes(const struct settings *s, int padded_cols, int cols
     b += up256(sizeof(float2) * (size_t)tc_npu(s->ndates) * npix);
     if (s->npairs)
         b += up256(sizeof(float) * (size_t)s->npairs * mr * cols);
-    if (s->emi || s->bias)
-        b += up256(sizeof(int) * (npix + 1)); /* the exact tier's pixel list */
+    if (s->emi || s->bias) /* the exact tier's queue, one sub-strip's pixels */
+        b += up256(tc_exact_queue_bytes((int)words, (long long)npix));
     return b;
 }
 
@@ -218,7 +218,15 @@ TC_API int tc_run_device_static(const struct settings *s, int padded_cols, const
             spairs = (float *)q;
             q += up256(sizeof(float) * (size_t)s->npairs * m * cols);
         }
-        int *elist = s->emi || s->bias ? (int *)q : nullptr;
+        TcExactQueue eq = {};
+
+        if (tc_link_queues(n, lk)) {
+            eq.buf = (int *)q;
+            eq.stride = 1 + ss.mask_words;
+            eq.capacity = c.npix;
+            if ((e = cudaMemsetAsync(eq.buf, 0, sizeof(int), st)) != cudaSuccess)
+                return tc_error(TC_ERR_CUDA, "exact-tier queue: %s", cudaGetErrorString(e));
+        }
 
         const float *s_slc = slc + (size_t)r0 * W * n * 2;
         const float *s_amp = amp + (size_t)r0 * W * n;
@@ -233,11 +241,16 @@ TC_API int tc_run_device_static(const struct settings *s, int padded_cols, const
                 cudaSuccess ||
             (tc_link_needs_gram(n, s->emi) &&
              (e = tc_launch_gram_fp32(ss, c, block, soa, mask, gram, st)) != cudaSuccess) ||
-            (e = tc_launch_link(ss, c, lk, gram, s_slc, mask, s_count, elist, upper, ptab, lscr,
+            (e = tc_launch_link(ss, c, lk, gram, s_slc, mask, s_count, &eq, upper, ptab, lscr,
                                 s_coh, spairs,
                                 phases ? phases + (size_t)r0 * cols * n : nullptr,
                                 status ? status + (size_t)r0 * cols : nullptr, sms, st)) !=
-                cudaSuccess)
+                cudaSuccess ||
+            (eq.buf &&
+             (e = tc_flush_exact(ss, lk, &eq, s_slc, s_count, upper, ptab, lscr, s_coh, spairs,
+                                 phases ? phases + (size_t)r0 * cols * n : nullptr,
+                                 status ? status + (size_t)r0 * cols : nullptr, sms, st)) !=
+                 cudaSuccess))
             return tc_error(TC_ERR_CUDA, "sub-strip at row %d: %s", r0, cudaGetErrorString(e));
         if (s->npairs &&
             (e = cudaMemcpy2DAsync(pairs + (size_t)r0 * cols, sizeof(float) * (size_t)rows * cols,

@@ -81,6 +81,34 @@ __host__ __device__ inline void tc_pixel_yx(const TcChunk &c, int p, int &y, int
     x = tx * TC_TILE_W + (w & 7);
 }
 
+/* The pixels handed to the exact tier, queued across the chunks of a strip
+   so that one launch of the exact kernel takes many chunks' pixels: buf[0]
+   counts the entries; entry e (buf + 1 + e * stride, stride = 1 +
+   mask_words) holds the pixel's output index y * cols + x and its SHP-mask
+   words, copied from the chunk's mask (which the next chunk overwrites).
+   The float link kernels append to it; the host flushes it
+   (tc_flush_exact) before a chunk could overflow it and at the end of the
+   strip, and counts in `pending` an upper bound on the entries queued. */
+struct TcExactQueue {
+    int *buf;
+    int stride;
+    long long capacity; /* entries */
+    long long pending;
+};
+
+#ifdef __CUDACC__
+/* Appends pixel p of a chunk (output index out) with its mask words. */
+__device__ __forceinline__ void tc_exact_push(int *q, int stride, long long out,
+                                              const uint32_t *mask, long long npix, int p)
+{
+    int *e = q + 1 + (long long)atomicAdd(q, 1) * stride;
+
+    e[0] = (int)out;
+    for (int w = 1; w < stride; w++)
+        e[w] = (int)mask[(long long)(w - 1) * npix + p];
+}
+#endif
+
 /* Geometry (geometry.cu): the device copy of struct tc_geometry with the
    grid shape, and the orbits of all dates concatenated. */
 struct TcGeo {
@@ -214,21 +242,34 @@ int tc_gram_block_for(int n);
    coherence sums (gram), or, for EMI, from the samples (slc, AoS) and SHP
    masks in double precision where float sums are not accurate enough:
    every pixel above 32 dates (the Gram stage is then skipped, see
-   tc_link_needs_gram), the ill-conditioned ones up to 32 dates. exact_list
-   holds 1 + npix ints of device memory (EMI; null otherwise). */
+   tc_link_needs_gram), the flagged ones otherwise: those of EMI and of the
+   bias correction go to the queue q (tc_link_queues), which must have
+   room for the chunk's npix entries; the caller flushes it. */
 cudaError_t tc_launch_link(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
                            const float2 *gram, const float *slc, const uint32_t *mask,
-                           const int *count, int *exact_list,
+                           const int *count, TcExactQueue *q,
                            const unsigned short *upper_tab, const unsigned short *pair_tab,
                            double *scratch, float *coh, float *pairs, float *phases,
                            unsigned char *status, int sms, cudaStream_t st);
+/* Whether tc_launch_link queues pixels for the exact tier. */
+bool tc_link_queues(int n, const TcLinkConst &k);
+/* Device bytes of a queue of `capacity` entries. */
+size_t tc_exact_queue_bytes(int mask_words, long long capacity);
+/* Runs the exact tier on the queued pixels (strip-level outputs) and
+   empties the queue; nothing to do when it is empty. */
+cudaError_t tc_flush_exact(const TcStrip &s, const TcLinkConst &k, TcExactQueue *q,
+                           const float *slc, const int *count, const unsigned short *upper_tab,
+                           const unsigned short *pair_tab, double *scratch, float *coh,
+                           float *pairs, float *phases, unsigned char *status, int sms,
+                           cudaStream_t st);
 bool tc_link_needs_gram(int n, int emi);
 size_t tc_link_scratch_bytes(int n, int sms);
+/* queue, when not null: its buffer (TcExactQueue::buf) and stride. */
 cudaError_t tc_launch_link_half(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
-                                const float2 *gram, const int *count,
+                                const float2 *gram, const uint32_t *mask, const int *count,
                                 const unsigned short *upper_tab, const unsigned short *pair_tab,
                                 double *scratch, float *coh, float *pairs, float *phases,
-                                unsigned char *status, int *exact_list, int sms,
+                                unsigned char *status, int *queue, int qstride, int sms,
                                 cudaStream_t st);
 size_t tc_link_half_scratch_bytes(int n, int sms);
 /* The link stage with the adjoint (n <= 32): gamma into coh, and into gbar

@@ -248,8 +248,11 @@ int tc_adjoint_raw(struct ocl *o, const float *re, const float *im, const double
    of kernel launches: [0] strip preparation, [1] SHP selection,
    [2] coherence matrices, [3] phase linking and coherence (with the
    adjoint: and its backward pass), [4] host<->device copies (ms only),
-   [5] the adjoint's scatter onto the samples. Returns the number of stages
-   written (at most n). */
+   [5] the adjoint's scatter onto the samples, [6] the exact tier's
+   launches over the pixels the float kernels queued for it (up to 16
+   chunks' pixels per launch; the exact tier of every pixel, EMI above 32
+   dates, counts in [3]). Returns the number of stages written (at most
+   n). */
 int tc_set_timing(struct ocl *o, int on);
 int tc_stage_stats(const struct ocl *o, float *ms, int *launches, int n);
 
