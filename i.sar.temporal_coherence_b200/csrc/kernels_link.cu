@@ -995,10 +995,15 @@ tc_link_smem_kernel(TcStrip s, TcChunk c, TcLinkConst k, LinkLayout L,
    time. */
 
 constexpr int EX_THREADS = 128;
-constexpr int EX_CTAS = 3;        /* CTAs per SM */
+/* CTAs per SM: register blocks of the sums per thread NB = 1 (up to 32
+   dates, 71 blocks of 2 x 4 entries at most) leave room for 6, NB = 3 (up
+   to 64 dates) for 3 */
+__host__ __device__ constexpr int ex_ctas(int nb) { return nb == 1 ? 6 : 3; }
+constexpr int EX_CTAS_MAX = 6;
 constexpr int EX_KC = 16;         /* candidates per staging block */
 constexpr int EX_BC = 4;          /* columns per register block (2 rows x 4) */
 constexpr int EX_NB = 3;          /* register blocks per thread, n <= 64 */
+__host__ __device__ constexpr int ex_nb_for(int n) { return n <= 32 ? 1 : EX_NB; }
 
 struct ExLayout {
     int n, npu, nblk, ld;
@@ -1148,16 +1153,18 @@ __device__ int ex_candidates(const TcStrip &s, const uint32_t *words, long long 
     return w.ints[0];
 }
 
-/* C = sum of s_q s_q^H over the candidates, in double, into w.T (packed). */
+/* C = sum of s_q s_q^H over the candidates, in double, into w.T (packed);
+   NB register blocks per thread (L.nblk <= NB * EX_THREADS). */
+template <int NB>
 __device__ void ex_gram(const TcStrip &s, const float2 *slc, int py0, int px0, int ncand,
                         const ExWs &w, const ExLayout &L)
 {
     const int n = s.n, t = threadIdx.x;
-    double2 acc[EX_NB][2][EX_BC];
-    int bi[EX_NB], bj[EX_NB];
+    double2 acc[NB][2][EX_BC];
+    int bi[NB], bj[NB];
 
 #pragma unroll
-    for (int b = 0; b < EX_NB; b++) {
+    for (int b = 0; b < NB; b++) {
         const int id = t + b * EX_THREADS;
 
         bi[b] = bj[b] = -1;
@@ -1188,7 +1195,7 @@ __device__ void ex_gram(const TcStrip &s, const float2 *slc, int py0, int px0, i
         }
         __syncthreads();
 #pragma unroll
-        for (int b = 0; b < EX_NB; b++) {
+        for (int b = 0; b < NB; b++) {
             if (bi[b] < 0)
                 continue;
             for (int q = 0; q < kc; q++) {
@@ -1220,7 +1227,7 @@ __device__ void ex_gram(const TcStrip &s, const float2 *slc, int py0, int px0, i
         __syncthreads();
     }
 #pragma unroll
-    for (int b = 0; b < EX_NB; b++) {
+    for (int b = 0; b < NB; b++) {
         if (bi[b] < 0)
             continue;
 #pragma unroll
@@ -1955,7 +1962,8 @@ __device__ float ex_gamma(int n, int npu, const ExWs &w)
 
 /* queue: null for every pixel of the chunk c (with its mask), else the
    queue's entries (TcExactQueue, any pixels of the strip; c unused). */
-__global__ void __launch_bounds__(EX_THREADS, EX_CTAS)
+template <int NB>
+__global__ void __launch_bounds__(EX_THREADS, ex_ctas(NB))
 tc_link_exact_kernel(TcStrip s, TcChunk c, TcLinkConst k, ExLayout L,
                      const float2 *__restrict__ slc, const uint32_t *__restrict__ mask,
                      const int *__restrict__ count, const int *__restrict__ queue, int qstride,
@@ -2015,7 +2023,7 @@ tc_link_exact_kernel(TcStrip s, TcChunk c, TcLinkConst k, ExLayout L,
             entry ? ex_candidates(s, (const uint32_t *)entry + 1, 1, w)
                   : ex_candidates(s, mask + it, c.npix, w);
 
-        ex_gram(s, slc, y, x, ncand, w, L);
+        ex_gram<NB>(s, slc, y, x, ncand, w, L);
         ex_coherence(n, npu, k, looks, w);
         for (int q = t; q < k.npairs; q += EX_THREADS) {
             const int i = pair_tab[q] >> 8, j = pair_tab[q] & 255;
@@ -2101,7 +2109,34 @@ static size_t exact_scratch_bytes(int n, int sms)
 {
     /* per CTA: |T| and the Jacobi eigenvectors in full storage, and the
        eigenvalues, for the pseudo-inverse tier */
-    return (size_t)sms * EX_CTAS * (2 * n * (n | 1) + 64) * sizeof(double);
+    return (size_t)sms * ex_ctas(ex_nb_for(n)) * (2 * n * (n | 1) + 64) * sizeof(double);
+}
+
+template <int NB>
+static cudaError_t launch_exact_nb(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
+                                   const float *slc, const uint32_t *mask, const int *count,
+                                   const TcExactQueue *q, const unsigned short *upper_tab,
+                                   const unsigned short *pair_tab, double *scratch, float *coh,
+                                   float *pairs, float *phases, unsigned char *status, int sms,
+                                   cudaStream_t st)
+{
+    const ExLayout L = ex_layout(s.n, s.area);
+    const int ctas = sms * ex_ctas(NB);
+    int blocks = ctas;
+
+    if (!q && c.npix < ctas)
+        blocks = c.npix;
+    if (q && q->pending < ctas)
+        blocks = (int)q->pending;
+    cudaError_t e = cudaFuncSetAttribute(tc_link_exact_kernel<NB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, L.bytes);
+
+    if (e != cudaSuccess)
+        return e;
+    tc_link_exact_kernel<NB><<<blocks, EX_THREADS, L.bytes, st>>>(
+        s, c, k, L, (const float2 *)slc, mask, count, q ? q->buf : nullptr, q ? q->stride : 0,
+        upper_tab, pair_tab, scratch, coh, pairs, phases, status);
+    return cudaGetLastError();
 }
 
 static cudaError_t launch_exact(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
@@ -2111,23 +2146,11 @@ static cudaError_t launch_exact(const TcStrip &s, const TcChunk &c, const TcLink
                                 float *pairs, float *phases, unsigned char *status, int sms,
                                 cudaStream_t st)
 {
-    const ExLayout L = ex_layout(s.n, s.area);
-    const int ctas = sms * EX_CTAS;
-    int blocks = ctas;
-
-    if (!q && c.npix < ctas)
-        blocks = c.npix;
-    if (q && q->pending < ctas)
-        blocks = (int)q->pending;
-    cudaError_t e = cudaFuncSetAttribute(tc_link_exact_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, L.bytes);
-
-    if (e != cudaSuccess)
-        return e;
-    tc_link_exact_kernel<<<blocks, EX_THREADS, L.bytes, st>>>(
-        s, c, k, L, (const float2 *)slc, mask, count, q ? q->buf : nullptr, q ? q->stride : 0,
-        upper_tab, pair_tab, scratch, coh, pairs, phases, status);
-    return cudaGetLastError();
+    if (ex_nb_for(s.n) == 1)
+        return launch_exact_nb<1>(s, c, k, slc, mask, count, q, upper_tab, pair_tab, scratch,
+                                  coh, pairs, phases, status, sms, st);
+    return launch_exact_nb<EX_NB>(s, c, k, slc, mask, count, q, upper_tab, pair_tab, scratch,
+                                  coh, pairs, phases, status, sms, st);
 }
 
 bool tc_link_needs_gram(int n, int emi)
