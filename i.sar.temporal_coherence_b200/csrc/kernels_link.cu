@@ -168,6 +168,41 @@ __device__ __forceinline__ int sturmd(const double *d, const double *e2, int n, 
     return c;
 }
 
+/* sturmd's count from the three-term recurrence of the leading principal
+   minors, p_i = (d_i - x) p_{i-1} - e2_{i-1} p_{i-2}, whose ratios
+   q_i = p_i / p_{i-1} are sturmd's pivots (a negative pivot is a sign
+   change between consecutive minors): one FMA on the dependency chain per
+   step, no division. The minors are rescaled by powers of two to stay in
+   range; a pivot of magnitude below pivmin becomes -pivmin, as in sturmd. */
+__device__ __forceinline__ int sturmd_minors(const double *d, const double *e2, int n, double x,
+                                             double pivmin)
+{
+    double pm = 1.0, p = d[0] - x;
+
+    if (fabs(p) < pivmin)
+        p = -pivmin;
+    int c = p < 0.0;
+
+    for (int i = 1; i < n; i++) {
+        double pn = fma(d[i] - x, p, -e2[i - 1] * pm);
+
+        if (fabs(pn) < pivmin * fabs(p))
+            pn = -pivmin * p;
+        c += (pn < 0.0) != (p < 0.0);
+        pm = p;
+        p = pn;
+        const double a = fabs(p);
+
+        if (a > 0x1p400 || a < 0x1p-400) {
+            const double sc = a > 1.0 ? 0x1p-400 : 0x1p400;
+
+            p *= sc;
+            pm *= sc;
+        }
+    }
+    return c;
+}
+
 __device__ __forceinline__ int sturmf(const float *d, const float *e2, int n, float x,
                                       float pivmin)
 {
@@ -990,9 +1025,10 @@ tc_link_smem_kernel(TcStrip s, TcChunk c, TcLinkConst k, LinkLayout L,
    storage (index tc_pidx) in shared memory, so that three pixels fit an
    SM at 60 dates: the sums and T (then M, in place) in complex double,
    |T| and its inverse in double (then a float copy of T for gamma in the
-   same place). The sums accumulate in registers, each thread a few 2 x 4
-   blocks of the triangle, over the SHP samples staged 16 candidates at a
-   time. */
+   same place). The sums accumulate in registers, each thread one to three
+   2 x BC blocks of the triangle, over the SHP samples staged 16 candidates
+   at a time, converted to double once at staging (a conversion costs four
+   double FMAs' issue). */
 
 constexpr int EX_THREADS = 128;
 /* CTAs per SM: register blocks of the sums per thread NB = 1 (up to 32
@@ -1001,9 +1037,25 @@ constexpr int EX_THREADS = 128;
 __host__ __device__ constexpr int ex_ctas(int nb) { return nb == 1 ? 6 : 3; }
 constexpr int EX_CTAS_MAX = 6;
 constexpr int EX_KC = 16;         /* candidates per staging block */
-constexpr int EX_BC = 4;          /* columns per register block (2 rows x 4) */
+/* the multisection's spacing: EX_THREADS points split an interval into
+   EX_THREADS + 1 parts */
+constexpr double EX_INV_POINTS = 1.0 / (EX_THREADS + 1);
 constexpr int EX_NB = 3;          /* register blocks per thread, n <= 64 */
 __host__ __device__ constexpr int ex_nb_for(int n) { return n <= 32 ? 1 : EX_NB; }
+/* Columns per register block (2 rows x BC): 2 while the triangle's blocks
+   fit one per thread (up to 30 dates), else 4. */
+__host__ __device__ inline int ex_blocks(int n, int bc)
+{
+    const int rp = (n + 1) / 2, cg = (n + bc - 1) / bc;
+    int nb = 0;
+
+    for (int ip = 0; ip < rp; ip++)
+        nb += cg - (2 * ip) / bc;
+    return nb;
+}
+__host__ __device__ inline int ex_bc_for(int n) { return ex_blocks(n, 2) <= EX_THREADS ? 2 : 4; }
+/* Row stride of the staged samples: n rounded up to 4, zero-padded. */
+__host__ __device__ inline int ex_sld(int n) { return (n + 3) & ~3; }
 
 struct ExLayout {
     int n, npu, nblk, ld;
@@ -1016,7 +1068,7 @@ struct ExWs {
     double *G;        /* [npu] |T|, then its inverse */
     float2 *Tf;       /* [npu] T in float, over G once M is formed */
     unsigned short *tab, *blk, *cand;
-    float2 *stage;    /* [EX_KC][n] */
+    double2 *stage;   /* [EX_KC][ex_sld(n)] */
     double *d, *e, *e2, *y, *lu, *rrow, *nrm, *red;
     double2 *v, *w, *tau, *z;
     float2 *zs;
@@ -1034,23 +1086,20 @@ __host__ __device__ inline ExLayout ex_layout(int n, int area)
         off += (bytes + 15) & ~15;
         return o;
     };
-    const int rp = (n + 1) / 2, cg = (n + EX_BC - 1) / EX_BC;
-
     L.n = n;
     L.npu = tc_npu(n);
     L.ld = n | 1;
-    L.nblk = 0;
-    for (int ip = 0; ip < rp; ip++)
-        L.nblk += cg - (2 * ip) / EX_BC;
+    L.nblk = ex_blocks(n, ex_bc_for(n));
     L.off_T = take(16 * L.npu);
     L.off_G = take(8 * L.npu);
     L.off_tab = take(2 * L.npu);
     L.off_blk = take(2 * L.nblk);
     /* the staged samples; once the sums are formed, up to 32 dates, the
        full |T| of the Gauss-Jordan inverse tier */
-    L.off_stage = take(n <= 32 && 8 * n * n > 8 * EX_KC * n ? 8 * n * n : 8 * EX_KC * n);
+    L.off_stage = take(n <= 32 && 8 * n * n > 16 * EX_KC * ex_sld(n) ? 8 * n * n
+                                                                      : 16 * EX_KC * ex_sld(n));
     L.off_cand = take(2 * area);
-    L.off_vec = take(8 * (8 * 64 + 8 + 4 * 64) + 16 * 5 * 64 + 8 * 64 + 16);
+    L.off_vec = take(8 * (8 * 64 + 16 + 4 * 64) + 16 * 5 * 64 + 8 * 64 + 16);
     L.off_adj = take(8 * 64);
     L.bytes = off;
     return L;
@@ -1066,7 +1115,7 @@ __device__ __forceinline__ ExWs ex_ws(unsigned char *base, const ExLayout &L)
     w.Tf = (float2 *)(base + L.off_G);
     w.tab = (unsigned short *)(base + L.off_tab);
     w.blk = (unsigned short *)(base + L.off_blk);
-    w.stage = (float2 *)(base + L.off_stage);
+    w.stage = (double2 *)(base + L.off_stage);
     w.cand = (unsigned short *)(base + L.off_cand);
     w.d = v;
     w.e = v + 64;
@@ -1074,9 +1123,9 @@ __device__ __forceinline__ ExWs ex_ws(unsigned char *base, const ExLayout &L)
     w.y = v + 192;
     w.rrow = v + 256;
     w.nrm = v + 320;
-    w.red = v + 384;        /* 8 */
-    w.lu = v + 392;         /* 4 x 64 */
-    double2 *c = (double2 *)(v + 392 + 256);
+    w.red = v + 384;        /* 2 x 8 */
+    w.lu = v + 400;         /* 4 x 64 */
+    double2 *c = (double2 *)(v + 400 + 256);
 
     w.v = c;
     w.w = c + 64;
@@ -1088,12 +1137,50 @@ __device__ __forceinline__ ExWs ex_ws(unsigned char *base, const ExLayout &L)
     return w;
 }
 
+/* 1 / x in double: a float reciprocal refined by two Newton steps
+   r <- r (2 - x r), each doubling the correct bits (24 -> 48 -> 96, so
+   within an ulp or two of 1 / x). For |x| in the float range: the LU
+   pivots here, clamped to at least 1e-13 of the tridiagonal's norm, which
+   is of order 1 or more (T has a unit diagonal, |T|^-1 o T one of 1 or
+   more, a pseudo-inverse's at least about 1 / n^2). */
+__device__ __forceinline__ double ex_rcp(double x)
+{
+    double r = (double)__frcp_rn((float)x);
+
+    r = r * fma(-x, r, 2.0);
+    return r * fma(-x, r, 2.0);
+}
+
+/* 1 / x for any x: ex_rcp inside [1e-30, 1e30] in magnitude, else the
+   division. */
+__device__ __forceinline__ double ex_rcp_any(double x)
+{
+    const double a = fabs(x);
+
+    return a > 1.0e-30 && a < 1.0e30 ? ex_rcp(x) : 1.0 / x;
+}
+
 /* Block sums over the CTA (every thread gets them); red holds 8 doubles. */
 __device__ __forceinline__ double2 ex_sum2(double a, double b, double *red)
 {
     a = wsum<double>(a);
     b = wsum<double>(b);
     __syncthreads();
+    if ((threadIdx.x & 31) == 0) {
+        red[threadIdx.x >> 5] = a;
+        red[4 + (threadIdx.x >> 5)] = b;
+    }
+    __syncthreads();
+    return make_double2(red[0] + red[1] + red[2] + red[3], red[4] + red[5] + red[6] + red[7]);
+}
+
+/* The same without the leading barrier, for callers that alternate
+   between two halves of red (red + 8 * parity) with a barrier between two
+   uses of one half. */
+__device__ __forceinline__ double2 ex_sum2p(double a, double b, double *red)
+{
+    a = wsum<double>(a);
+    b = wsum<double>(b);
     if ((threadIdx.x & 31) == 0) {
         red[threadIdx.x >> 5] = a;
         red[4 + (threadIdx.x >> 5)] = b;
@@ -1155,12 +1242,13 @@ __device__ int ex_candidates(const TcStrip &s, const uint32_t *words, long long 
 
 /* C = sum of s_q s_q^H over the candidates, in double, into w.T (packed);
    NB register blocks per thread (L.nblk <= NB * EX_THREADS). */
-template <int NB>
+template <int NB, int BC>
 __device__ void ex_gram(const TcStrip &s, const float2 *slc, int py0, int px0, int ncand,
                         const ExWs &w, const ExLayout &L)
 {
     const int n = s.n, t = threadIdx.x;
-    double2 acc[NB][2][EX_BC];
+    const int sld = ex_sld(n);
+    double2 acc[NB][2][BC];
     int bi[NB], bj[NB];
 
 #pragma unroll
@@ -1170,12 +1258,12 @@ __device__ void ex_gram(const TcStrip &s, const float2 *slc, int py0, int px0, i
         bi[b] = bj[b] = -1;
         if (id < L.nblk) {
             bi[b] = 2 * (w.blk[id] >> 8);
-            bj[b] = EX_BC * (w.blk[id] & 255);
+            bj[b] = BC * (w.blk[id] & 255);
         }
 #pragma unroll
         for (int r = 0; r < 2; r++)
 #pragma unroll
-            for (int q = 0; q < EX_BC; q++)
+            for (int q = 0; q < BC; q++)
                 acc[b][r][q] = make_double2(0.0, 0.0);
     }
     for (int c0 = 0; c0 < ncand; c0 += EX_KC) {
@@ -1185,12 +1273,12 @@ __device__ void ex_gram(const TcStrip &s, const float2 *slc, int py0, int px0, i
             const int u = w.cand[c0 + q], dy = u / s.wr, dx = u - dy * s.wr;
             const float2 *src = slc + ((long long)(py0 + dy) * s.W + px0 + dx) * n;
 
-            for (int d = t & 31; d < n; d += 32) {
-                float2 v = src[d];
+            for (int d = t & 31; d < sld; d += 32) {
+                float2 v = d < n ? src[d] : make_float2(0.f, 0.f);
 
                 if (!isfinite(v.x) || !isfinite(v.y))
                     v = make_float2(0.f, 0.f);
-                w.stage[q * n + d] = v;
+                w.stage[q * sld + d] = make_double2(v.x, v.y);
             }
         }
         __syncthreads();
@@ -1199,25 +1287,19 @@ __device__ void ex_gram(const TcStrip &s, const float2 *slc, int py0, int px0, i
             if (bi[b] < 0)
                 continue;
             for (int q = 0; q < kc; q++) {
-                const float2 *row = w.stage + q * n;
-                double2 a[2], cj[EX_BC];
+                const double2 *row = w.stage + q * sld;
+                double2 a[2], cj[BC];
 
 #pragma unroll
-                for (int r = 0; r < 2; r++) {
-                    const float2 f = bi[b] + r < n ? row[bi[b] + r] : make_float2(0.f, 0.f);
-
-                    a[r] = make_double2(f.x, f.y);
-                }
+                for (int r = 0; r < 2; r++)
+                    a[r] = row[bi[b] + r];
 #pragma unroll
-                for (int jj = 0; jj < EX_BC; jj++) {
-                    const float2 f = bj[b] + jj < n ? row[bj[b] + jj] : make_float2(0.f, 0.f);
-
-                    cj[jj] = make_double2(f.x, f.y);
-                }
+                for (int jj = 0; jj < BC; jj++)
+                    cj[jj] = row[bj[b] + jj];
 #pragma unroll
                 for (int r = 0; r < 2; r++)
 #pragma unroll
-                    for (int jj = 0; jj < EX_BC; jj++) {
+                    for (int jj = 0; jj < BC; jj++) {
                         /* a conj(b) */
                         acc[b][r][jj].x = fma(a[r].x, cj[jj].x, fma(a[r].y, cj[jj].y, acc[b][r][jj].x));
                         acc[b][r][jj].y = fma(a[r].y, cj[jj].x, fma(-a[r].x, cj[jj].y, acc[b][r][jj].y));
@@ -1233,7 +1315,7 @@ __device__ void ex_gram(const TcStrip &s, const float2 *slc, int py0, int px0, i
 #pragma unroll
         for (int r = 0; r < 2; r++)
 #pragma unroll
-            for (int jj = 0; jj < EX_BC; jj++) {
+            for (int jj = 0; jj < BC; jj++) {
                 const int i = bi[b] + r, j = bj[b] + jj;
 
                 if (i < n && j < n && i <= j)
@@ -1252,7 +1334,7 @@ __device__ void ex_coherence(int n, int npu, const TcLinkConst &k, int looks, co
     for (int i = t; i < n; i += EX_THREADS)
         w.nrm[i] = sqrt(w.T[tc_pidx(n, i, i)].x);
     __syncthreads();
-    const double fl = (double)looks;
+    const double fl = (double)looks, ifl1 = looks > 1 ? 1.0 / (fl - 1.0) : 0.0;
 
     for (int q = t; q < npu; q += EX_THREADS) {
         const int i = w.tab[q] >> 8, j = w.tab[q] & 255;
@@ -1264,11 +1346,13 @@ __device__ void ex_coherence(int n, int npu, const TcLinkConst &k, int looks, co
 
             v = make_double2(0.0, 0.0);
             if (dd > 0.0) {
-                v = make_double2(cs.x / dd, cs.y / dd);
+                const double rdd = ex_rcp_any(dd);
+
+                v = make_double2(cs.x * rdd, cs.y * rdd);
                 if (k.bias && looks > 1) {
                     const double m2 = v.x * v.x + v.y * v.y;
-                    const double m2c = (fl * m2 - 1.0) / (fl - 1.0);
-                    const double f = (m2 > 0.0 && m2c > 0.0) ? sqrt(m2c / m2) : 0.0;
+                    const double m2c = (fl * m2 - 1.0) * ifl1;
+                    const double f = (m2 > 0.0 && m2c > 0.0) ? sqrt(m2c * ex_rcp_any(m2)) : 0.0;
 
                     v.x *= f;
                     v.y *= f;
@@ -1340,7 +1424,7 @@ __device__ bool ex_sweep(int n, int npu, const ExWs &w, double *A, double floor_
             __syncthreads();
             return false;
         }
-        const double id = 1.0 / d;
+        const double id = ex_rcp_any(d);
 
         for (int j = t; j < n; j += EX_THREADS)
             w.rrow[j] = A[ex_sym(n, kp, j)] * id;
@@ -1548,7 +1632,8 @@ __device__ void ex_householder(int n, int npu, const ExWs &w)
 
             xn2 = a.x * a.x + a.y * a.y;
         }
-        xn2 = ex_sum2(xn2, 0.0, w.red).x;
+        /* two barriers separate this half of red from its last use */
+        xn2 = ex_sum2p(xn2, 0.0, w.red).x;
         const double2 am = w.T[tc_pidx(n, k, k + 1)];
         const double ax = am.x, ay = -am.y; /* alpha = x_k+1 */
         double beta, tr = 0.0, ti = 0.0, sr = 0.0, si = 0.0;
@@ -1557,12 +1642,14 @@ __device__ void ex_householder(int n, int npu, const ExWs &w)
             beta = ax;
         else {
             beta = -copysign(sqrt(ax * ax + ay * ay + xn2), ax);
-            tr = (beta - ax) / beta;
-            ti = -ay / beta;
-            const double dr = ax - beta, di = ay, den = dr * dr + di * di;
+            const double rb = ex_rcp_any(beta);
 
-            sr = dr / den;
-            si = -di / den;
+            tr = (beta - ax) * rb;
+            ti = -ay * rb;
+            const double dr = ax - beta, di = ay, rden = ex_rcp_any(dr * dr + di * di);
+
+            sr = dr * rden;
+            si = -di * rden;
         }
         const bool reflect = tr != 0.0 || ti != 0.0;
 
@@ -1624,7 +1711,7 @@ __device__ void ex_householder(int n, int npu, const ExWs &w)
             pr = wl.x * v.x + wl.y * v.y;
             pi = wl.x * v.y - wl.y * v.x;
         }
-        const double2 pp = ex_sum2(pr, pi, w.red);
+        const double2 pp = ex_sum2p(pr, pi, w.red + 8);
         const double hr = -0.5 * (tr * pp.x - ti * pp.y), hi = -0.5 * (tr * pp.y + ti * pp.x);
 
         if (i < n && h == 0) {
@@ -1702,7 +1789,7 @@ __device__ unsigned ex_eigvec(int n, int index, const ExWs &w)
     }
     __syncthreads();
     for (int fr = 0; fr < 4 && hi - lo > 1.0e-6 * norm; fr++) {
-        const double xq = lo + (hi - lo) * ((double)(t + 1) / (double)(EX_THREADS + 1));
+        const double xq = lo + (hi - lo) * ((double)(t + 1) * EX_INV_POINTS);
         const bool gt = sturmf(df, e2f, n, (float)xq, 1.0e-30f + 1.0e-14f * (float)norm) > index;
         const unsigned bal = __ballot_sync(FULL, gt);
 
@@ -1710,9 +1797,9 @@ __device__ unsigned ex_eigvec(int n, int index, const ExWs &w)
             w.ints[2 + (t >> 5)] = bal ? (t & ~31) + __ffs(bal) - 1 : EX_THREADS;
         __syncthreads();
         const int f = min(min(w.ints[2], w.ints[3]), min(w.ints[4], w.ints[5]));
-        const double nlo = f == 0 ? lo : lo + (hi - lo) * ((double)f / (double)(EX_THREADS + 1));
+        const double nlo = f == 0 ? lo : lo + (hi - lo) * ((double)f * EX_INV_POINTS);
         const double nhi =
-            f == EX_THREADS ? hi : lo + (hi - lo) * ((double)(f + 1) / (double)(EX_THREADS + 1));
+            f == EX_THREADS ? hi : lo + (hi - lo) * ((double)(f + 1) * EX_INV_POINTS);
 
         __syncthreads();
         lo = nlo;
@@ -1726,8 +1813,8 @@ __device__ unsigned ex_eigvec(int n, int index, const ExWs &w)
     for (; round < 12; round++) {
         if (hi - lo <= 2.0e-15 * norm)
             break;
-        const double xq = lo + (hi - lo) * ((double)(t + 1) / (double)(EX_THREADS + 1));
-        const bool gt = sturmd(w.d, w.e2, n, xq, pivmin) > index;
+        const double xq = lo + (hi - lo) * ((double)(t + 1) * EX_INV_POINTS);
+        const bool gt = sturmd_minors(w.d, w.e2, n, xq, pivmin) > index;
         const unsigned bal = __ballot_sync(FULL, gt);
 
         if ((t & 31) == 0)
@@ -1737,12 +1824,12 @@ __device__ unsigned ex_eigvec(int n, int index, const ExWs &w)
         double nlo, nhi;
 
         if (f == EX_THREADS) {
-            nlo = lo + (hi - lo) * ((double)EX_THREADS / (double)(EX_THREADS + 1));
+            nlo = lo + (hi - lo) * ((double)EX_THREADS * EX_INV_POINTS);
             nhi = hi;
         }
         else {
-            nhi = lo + (hi - lo) * ((double)(f + 1) / (double)(EX_THREADS + 1));
-            nlo = f == 0 ? lo : lo + (hi - lo) * ((double)f / (double)(EX_THREADS + 1));
+            nhi = lo + (hi - lo) * ((double)(f + 1) * EX_INV_POINTS);
+            nlo = f == 0 ? lo : lo + (hi - lo) * ((double)f * EX_INV_POINTS);
         }
         __syncthreads();
         if (!(nlo > lo || nhi < hi))
@@ -1755,21 +1842,26 @@ __device__ unsigned ex_eigvec(int n, int index, const ExWs &w)
     const double lambda = 0.5 * (lo + hi);
 
     /* Inverse iteration: LU of T - lambda I with partial pivoting, three
-       solves from a vector of ones (the method of tcoh.cl:342-410). */
+       solves from a vector of ones (the method of tcoh.cl:342-410). The
+       recurrences carry their running values in registers; the shared
+       arrays only hold what a later pass reads. */
     if (t == 0) {
         const double tiny = 1.0e-13 * (norm > 1e-300 ? norm : 1e-300);
-        double *lu = w.lu, *y = w.y;
+        double *__restrict__ lu = w.lu;
+        double *__restrict__ y = w.y;
+        const double *__restrict__ dg = w.d;
+        const double *__restrict__ eg = w.e;
         unsigned long long piv = 0ull;
-        double dd = w.d[0] - lambda, s1 = n > 1 ? w.e[0] : 0.0;
+        double dd = dg[0] - lambda, s1 = n > 1 ? eg[0] : 0.0;
 
         for (int kk = 0; kk < n - 1; kk++) {
-            const double sub = w.e[kk], nd = w.d[kk + 1] - lambda;
-            const double ns = kk + 1 < n - 1 ? w.e[kk + 1] : 0.0;
+            const double sub = eg[kk], nd = dg[kk + 1] - lambda;
+            const double ns = kk + 1 < n - 1 ? eg[kk + 1] : 0.0;
 
             if (fabs(dd) >= fabs(sub)) {
                 if (fabs(dd) < tiny)
                     dd = dd < 0.0 ? -tiny : tiny;
-                const double rd = 1.0 / dd, l = sub * rd;
+                const double rd = ex_rcp(dd), l = sub * rd;
 
                 lu[4 * kk] = rd;
                 lu[4 * kk + 1] = s1;
@@ -1779,7 +1871,7 @@ __device__ unsigned ex_eigvec(int n, int index, const ExWs &w)
                 s1 = ns;
             }
             else {
-                const double rs = 1.0 / sub, l = dd * rs;
+                const double rs = ex_rcp(sub), l = dd * rs;
 
                 piv |= 1ull << kk;
                 lu[4 * kk] = rs;
@@ -1792,41 +1884,52 @@ __device__ unsigned ex_eigvec(int n, int index, const ExWs &w)
         }
         if (fabs(dd) < tiny)
             dd = dd < 0.0 ? -tiny : tiny;
-        lu[4 * (n - 1)] = 1.0 / dd;
+        lu[4 * (n - 1)] = ex_rcp(dd);
         lu[4 * (n - 1) + 1] = 0.0;
         lu[4 * (n - 1) + 2] = 0.0;
         for (int kk = 0; kk < n; kk++)
             y[kk] = 1.0;
         for (int it = 0; it < 3; it++) {
-            double nrm = 0.0;
+            /* forward: the row interchanges and L, y[kk] final once the
+               step leaves it */
+            double cur = y[0];
 
             for (int kk = 0; kk < n - 1; kk++) {
+                double a = cur, b = y[kk + 1];
+
                 if ((piv >> kk) & 1ull) {
-                    const double tmp = y[kk];
+                    const double tmp = a;
 
-                    y[kk] = y[kk + 1];
-                    y[kk + 1] = tmp;
+                    a = b;
+                    b = tmp;
                 }
-                y[kk + 1] -= lu[4 * kk + 3] * y[kk];
+                y[kk] = a;
+                cur = b - lu[4 * kk + 3] * a;
             }
-            for (int kk = n - 1; kk >= 0; kk--) {
-                double v = y[kk];
+            y[n - 1] = cur;
+            /* backward: U, the next two solution entries in registers */
+            double y1 = 0.0, y2 = 0.0, nrm = 0.0;
 
-                if (kk + 1 < n)
-                    v -= lu[4 * kk + 1] * y[kk + 1];
-                if (kk + 2 < n)
-                    v -= lu[4 * kk + 2] * y[kk + 2];
-                y[kk] = v * lu[4 * kk];
-                nrm = fmax(nrm, fabs(y[kk]));
+            for (int kk = n - 1; kk >= 0; kk--) {
+                const double v = (y[kk] - lu[4 * kk + 1] * y1 - lu[4 * kk + 2] * y2) * lu[4 * kk];
+
+                y[kk] = v;
+                y2 = y1;
+                y1 = v;
+                nrm = fmax(nrm, fabs(v));
             }
-            const double inv = 1.0 / nrm;
+            const double inv = 1.0 / nrm; /* may exceed the float range */
 
             for (int kk = 0; kk < n; kk++)
                 y[kk] *= inv;
         }
     }
     __syncthreads();
-    /* z = H_0 ... H_n-2 y (warp 0, rows lane and lane + 32) */
+    /* z = H_0 ... H_n-2 y (warp 0, rows lane and lane + 32), two
+       reflectors at a time in application order (H_n-2 first): with
+       a = v_0^H z, b = v_1^H z and g = v_1^H v_0 reduced over the warp at
+       once, h_0 = tau_0 a, h_1 = tau_1 (b - g h_0), z -= v_0 h_0 + v_1 h_1,
+       which is the one-by-one application rearranged. */
     if (t < 32) {
         double2 z[2];
 
@@ -1836,35 +1939,56 @@ __device__ unsigned ex_eigvec(int n, int index, const ExWs &w)
 
             z[q] = make_double2(r < n ? w.y[r] : 0.0, 0.0);
         }
-        for (int kk = n - 2; kk >= 0; kk--) {
-            const double2 ta = w.tau[kk];
+        for (int b0 = n - 2; b0 >= 0; b0 -= 2) {
+            double2 vq[2][2], ta[2];
 
-            if (ta.x == 0.0 && ta.y == 0.0)
-                continue;
-            double sr = 0.0, si = 0.0;
-            double2 vq[2];
+#pragma unroll
+            for (int m = 0; m < 2; m++) {
+                const int kk = b0 - m;
+
+                ta[m] = kk >= 0 ? w.tau[kk] : make_double2(0.0, 0.0);
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    const int r = t + 32 * q;
+
+                    vq[m][q] = make_double2(0.0, 0.0);
+                    if (kk >= 0 && r == kk + 1)
+                        vq[m][q] = make_double2(1.0, 0.0);
+                    else if (kk >= 0 && r > kk + 1 && r < n)
+                        vq[m][q] = w.T[tc_pidx(n, kk, r)];
+                }
+            }
+            double rd[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 
 #pragma unroll
             for (int q = 0; q < 2; q++) {
-                const int r = t + 32 * q;
-
-                vq[q] = make_double2(0.0, 0.0);
-                if (r == kk + 1)
-                    vq[q] = make_double2(1.0, 0.0);
-                else if (r > kk + 1 && r < n)
-                    vq[q] = w.T[tc_pidx(n, kk, r)];
-                sr += vq[q].x * z[q].x + vq[q].y * z[q].y;
-                si += vq[q].x * z[q].y - vq[q].y * z[q].x;
-            }
-            sr = wsum<double>(sr);
-            si = wsum<double>(si);
-            const double hr = ta.x * sr - ta.y * si, hi2 = ta.x * si + ta.y * sr;
-
 #pragma unroll
-            for (int q = 0; q < 2; q++) {
-                z[q].x -= vq[q].x * hr - vq[q].y * hi2;
-                z[q].y -= vq[q].x * hi2 + vq[q].y * hr;
+                for (int m = 0; m < 2; m++) {
+                    rd[2 * m] += vq[m][q].x * z[q].x + vq[m][q].y * z[q].y;
+                    rd[2 * m + 1] += vq[m][q].x * z[q].y - vq[m][q].y * z[q].x;
+                }
+                rd[4] += vq[1][q].x * vq[0][q].x + vq[1][q].y * vq[0][q].y;
+                rd[5] += vq[1][q].x * vq[0][q].y - vq[1][q].y * vq[0][q].x;
             }
+#pragma unroll
+            for (int e = 0; e < 6; e++)
+                rd[e] = wsum<double>(rd[e]);
+            double2 h[2];
+
+            h[0] = make_double2(ta[0].x * rd[0] - ta[0].y * rd[1], ta[0].x * rd[1] + ta[0].y * rd[0]);
+            {
+                const double sx = rd[2] - (rd[4] * h[0].x - rd[5] * h[0].y);
+                const double sy = rd[3] - (rd[4] * h[0].y + rd[5] * h[0].x);
+
+                h[1] = make_double2(ta[1].x * sx - ta[1].y * sy, ta[1].x * sy + ta[1].y * sx);
+            }
+#pragma unroll
+            for (int m = 0; m < 2; m++)
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    z[q].x -= vq[m][q].x * h[m].x - vq[m][q].y * h[m].y;
+                    z[q].y -= vq[m][q].x * h[m].y + vq[m][q].y * h[m].x;
+                }
         }
 #pragma unroll
         for (int q = 0; q < 2; q++) {
@@ -1962,7 +2086,7 @@ __device__ float ex_gamma(int n, int npu, const ExWs &w)
 
 /* queue: null for every pixel of the chunk c (with its mask), else the
    queue's entries (TcExactQueue, any pixels of the strip; c unused). */
-template <int NB>
+template <int NB, int BC>
 __global__ void __launch_bounds__(EX_THREADS, ex_ctas(NB))
 tc_link_exact_kernel(TcStrip s, TcChunk c, TcLinkConst k, ExLayout L,
                      const float2 *__restrict__ slc, const uint32_t *__restrict__ mask,
@@ -1981,11 +2105,11 @@ tc_link_exact_kernel(TcStrip s, TcChunk c, TcLinkConst k, ExLayout L,
     for (int q = t; q < npu; q += EX_THREADS)
         w.tab[q] = upper_tab[q];
     if (t == 0) {
-        const int rp = (n + 1) / 2, cg = (n + EX_BC - 1) / EX_BC;
+        const int rp = (n + 1) / 2, cg = (n + BC - 1) / BC;
         int b = 0;
 
         for (int ip = 0; ip < rp; ip++)
-            for (int jg = (2 * ip) / EX_BC; jg < cg; jg++)
+            for (int jg = (2 * ip) / BC; jg < cg; jg++)
                 w.blk[b++] = (unsigned short)(ip << 8 | jg);
     }
     __syncthreads();
@@ -2023,7 +2147,7 @@ tc_link_exact_kernel(TcStrip s, TcChunk c, TcLinkConst k, ExLayout L,
             entry ? ex_candidates(s, (const uint32_t *)entry + 1, 1, w)
                   : ex_candidates(s, mask + it, c.npix, w);
 
-        ex_gram<NB>(s, slc, y, x, ncand, w, L);
+        ex_gram<NB, BC>(s, slc, y, x, ncand, w, L);
         ex_coherence(n, npu, k, looks, w);
         for (int q = t; q < k.npairs; q += EX_THREADS) {
             const int i = pair_tab[q] >> 8, j = pair_tab[q] & 255;
@@ -2112,7 +2236,7 @@ static size_t exact_scratch_bytes(int n, int sms)
     return (size_t)sms * ex_ctas(ex_nb_for(n)) * (2 * n * (n | 1) + 64) * sizeof(double);
 }
 
-template <int NB>
+template <int NB, int BC>
 static cudaError_t launch_exact_nb(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
                                    const float *slc, const uint32_t *mask, const int *count,
                                    const TcExactQueue *q, const unsigned short *upper_tab,
@@ -2128,12 +2252,12 @@ static cudaError_t launch_exact_nb(const TcStrip &s, const TcChunk &c, const TcL
         blocks = c.npix;
     if (q && q->pending < ctas)
         blocks = (int)q->pending;
-    cudaError_t e = cudaFuncSetAttribute(tc_link_exact_kernel<NB>,
+    cudaError_t e = cudaFuncSetAttribute(tc_link_exact_kernel<NB, BC>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, L.bytes);
 
     if (e != cudaSuccess)
         return e;
-    tc_link_exact_kernel<NB><<<blocks, EX_THREADS, L.bytes, st>>>(
+    tc_link_exact_kernel<NB, BC><<<blocks, EX_THREADS, L.bytes, st>>>(
         s, c, k, L, (const float2 *)slc, mask, count, q ? q->buf : nullptr, q ? q->stride : 0,
         upper_tab, pair_tab, scratch, coh, pairs, phases, status);
     return cudaGetLastError();
@@ -2146,11 +2270,14 @@ static cudaError_t launch_exact(const TcStrip &s, const TcChunk &c, const TcLink
                                 float *pairs, float *phases, unsigned char *status, int sms,
                                 cudaStream_t st)
 {
+    if (ex_nb_for(s.n) == 1 && ex_bc_for(s.n) == 2)
+        return launch_exact_nb<1, 2>(s, c, k, slc, mask, count, q, upper_tab, pair_tab, scratch,
+                                     coh, pairs, phases, status, sms, st);
     if (ex_nb_for(s.n) == 1)
-        return launch_exact_nb<1>(s, c, k, slc, mask, count, q, upper_tab, pair_tab, scratch,
-                                  coh, pairs, phases, status, sms, st);
-    return launch_exact_nb<EX_NB>(s, c, k, slc, mask, count, q, upper_tab, pair_tab, scratch,
-                                  coh, pairs, phases, status, sms, st);
+        return launch_exact_nb<1, 4>(s, c, k, slc, mask, count, q, upper_tab, pair_tab, scratch,
+                                     coh, pairs, phases, status, sms, st);
+    return launch_exact_nb<EX_NB, 4>(s, c, k, slc, mask, count, q, upper_tab, pair_tab, scratch,
+                                     coh, pairs, phases, status, sms, st);
 }
 
 bool tc_link_needs_gram(int n, int emi)
