@@ -19,13 +19,15 @@
  * EMI: |T| is inverted in double (Gauss-Jordan when every pivot exceeds
  * 1e-5; through |T|^2 when |T| is indefinite; Jacobi pseudo-inverse with the
  * absolute floor 1e-9 of tests/reference.py:151-156 when it is close to
- * singular). M = |T|^-1 o T is reduced in float, like T for EVD. The float
- * eigen-solve adds less to gamma's error than the float coherence sums do
- * (on the 30-date AD / EMI / -b stacks, a refinement of the eigenvector
- * against M in double left the largest error to the FP64 oracle unchanged
- * at 3.2e-5, and the per-date phases of pixels with gamma >= 0.2 within
- * 2.5e-4 rad instead of 0.85e-4); the pixels whose gamma the float
- * arithmetic may move by more than about 1e-5 go to the exact tier.
+ * singular). M = |T|^-1 o T is reduced in float. Where the gap of its two
+ * smallest eigenvalues is small against its norm, the float eigenvector is
+ * then refined in double: the residual r = M x - mu x (M and mu in double)
+ * is mapped by the float Householder basis Q onto the tridiagonal, the
+ * correction solves (tri - mu) t = Q^H r off the eigen-direction, and
+ * x -= Q t; this step gives double accuracy whenever the float rounding of
+ * M is small against that gap (one step squares the relative error).
+ * Elsewhere the float eigen-solve adds less to gamma's error than the float
+ * coherence sums do.
  */
 #include "tcoh_internal.h"
 
@@ -1015,6 +1017,78 @@ __device__ void solve_off(int n, int ld, const HWs &w, const Grp &g, const float
     apply_q(n, ld, w, g, false, t0, t1);
 }
 
+/* One refinement step of the eigenpair of M for the eigenvector (z0, z1)
+   of rows (i0, i1): see the file comment. tri and Q are the float
+   reduction of M; y is the tridiagonal eigenvector. The residual is formed
+   in double; the correction, a small vector that needs only float relative
+   accuracy, is mapped through Q in float after scaling the residual to a
+   unit maximum. */
+__device__ void refine(int n, int ld, const HWs &w, const Grp &g, double2 &x0, double2 &x1,
+                       const float (&yr)[32], unsigned long long piv)
+{
+    const int i0 = g.gl, i1 = g.gl + 16;
+
+    /* normalize, publish x */
+    double nn = x0.x * x0.x + x0.y * x0.y + x1.x * x1.x + x1.y * x1.y;
+
+    nn = gsum(nn, g);
+    const double inrm = 1.0 / sqrt(nn);
+
+    x0.x *= inrm;
+    x0.y *= inrm;
+    x1.x *= inrm;
+    x1.y *= inrm;
+    w.x[i0] = x0;
+    w.x[i1] = x1;
+    gsync(g);
+    /* u = M x (rows i0, i1), mu = x^H u */
+    double2 u0 = make_double2(0.0, 0.0), u1 = u0;
+
+    for (int j = 0; j < n; j++) {
+        const double2 xj = w.x[j];
+
+        if (i0 < n) {
+            const double2 m = mval(w, ld, i0, j);
+
+            u0.x += m.x * xj.x - m.y * xj.y;
+            u0.y += m.x * xj.y + m.y * xj.x;
+        }
+        if (i1 < n) {
+            const double2 m = mval(w, ld, i1, j);
+
+            u1.x += m.x * xj.x - m.y * xj.y;
+            u1.y += m.x * xj.y + m.y * xj.x;
+        }
+    }
+    double mu = x0.x * u0.x + x0.y * u0.y + x1.x * u1.x + x1.y * u1.y;
+
+    mu = gsum(mu, g);
+    /* r = u - mu x, scaled to a unit maximum */
+    double2 r0 = make_double2(u0.x - mu * x0.x, u0.y - mu * x0.y);
+    double2 r1 = make_double2(u1.x - mu * x1.x, u1.y - mu * x1.y);
+
+    if (i0 >= n)
+        r0 = make_double2(0.0, 0.0);
+    if (i1 >= n)
+        r1 = make_double2(0.0, 0.0);
+    const double rmax = gmaxd(fmax(fmax(fabs(r0.x), fabs(r0.y)), fmax(fabs(r1.x), fabs(r1.y))), g);
+
+    gsync(g);
+    if (!(rmax > 0.0))
+        return;
+    const double sc = 1.0 / rmax;
+    float2 t0, t1;
+
+    solve_off(n, ld, w, g, yr, piv, make_float2((float)(r0.x * sc), (float)(r0.y * sc)),
+              make_float2((float)(r1.x * sc), (float)(r1.y * sc)), t0, t1);
+    /* x -= Q (tri - mu)^+ Q^H r */
+    x0.x -= rmax * t0.x;
+    x0.y -= rmax * t0.y;
+    x1.x -= rmax * t1.x;
+    x1.y -= rmax * t1.y;
+    gsync(g);
+}
+
 /* ------------------------------------------------------------------ */
 /* Common stages.                                                      */
 /* ------------------------------------------------------------------ */
@@ -1730,11 +1804,22 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
                 householder(r0, r1, n, w, ld, g);
             }
             __syncthreads();
-            /* stage 4: eigenvector of the smallest eigenvalue */
+            /* stage 4: eigenvector of the smallest eigenvalue, refined
+               where its gap is small */
             if (run) {
                 st |= eigvec(n, 0, w, ld, g, f0, f1, yr, lambda, norm, piv);
                 z0 = make_double2(f0.x, f0.y);
                 z1 = make_double2(f1.x, f1.y);
+                /* The float eigen-solve's error in gamma is about
+                   3 eps_f norm / gap (gap between the two smallest
+                   eigenvalues of M); above 1e-5 where the relative gap is
+                   below 0.016. Pixels whose gap is below 0.02 of the norm
+                   (two eigenvalues under lambda + 0.02 norm) refine their
+                   eigenvector once in double: a few percent of the pixels
+                   of coherent stacks, most of those of incoherent ones. */
+                if (active && sturm16(w.d, w.e2f, n, lambda + 0.02f * norm,
+                                      1.0e-30f + 1.0e-14f * norm) >= 2)
+                    refine(n, ld, w, g, z0, z1, yr, piv);
                 /* Pixels whose gamma the float rounding of T may move by
                    more than ~1e-5 go to the exact tier: the first-order
                    sensitivity of M's eigenvector to T grows with
