@@ -405,40 +405,17 @@ __device__ void apply_q(int n, int ld, const HWs &w, const Grp &g, bool adjoint,
 }
 
 
-/* The number of eigenvalues of the tridiagonal (d, e2 = e^2) below x: the
-   sign changes of its leading principal minors
-   p_i = (d_i - x) p_{i-1} - e2_{i-1} p_{i-2}, whose ratios are the pivots
-   of the LDL^T factorization of tri - x (a pivot of magnitude below pivmin
-   counts as -pivmin). One FMA per step on the dependency chain and no
-   division; the minors are rescaled by powers of two to stay within
-   2^-40 .. 2^40, which holds for tridiagonal norms up to 2^35 (the
-   matrices here: T, norm <= n; M, norm <= n max|inv| < 1e8, or a pixel
-   that the exact tier recomputes). */
 __device__ __forceinline__ int sturm16(const float *d, const float *e2, int n, float x,
                                        float pivmin)
 {
-    float pm = 1.f, p = d[0] - x;
-
-    if (fabsf(p) < pivmin)
-        p = -pivmin;
-    int c = p < 0.f;
+    float q = d[0] - x;
+    int c = q < 0.f;
 
     for (int i = 1; i < n; i++) {
-        float pn = fmaf(d[i] - x, p, -e2[i - 1] * pm);
-
-        if (fabsf(pn) < pivmin * fabsf(p))
-            pn = -pivmin * p;
-        c += (pn < 0.f) != (p < 0.f);
-        pm = p;
-        p = pn;
-        const float a = fabsf(p);
-
-        if (a > 0x1p40f || a < 0x1p-40f) {
-            const float sc = a > 1.f ? 0x1p-40f : 0x1p40f;
-
-            p *= sc;
-            pm *= sc;
-        }
+        if (fabsf(q) < pivmin)
+            q = -pivmin;
+        q = d[i] - x - __fdividef(e2[i - 1], q);
+        c += q < 0.f;
     }
     return c;
 }
@@ -1170,27 +1147,27 @@ __device__ __forceinline__ void load_T_batch(const float2 (&gv)[B], int t0, int 
     }
 }
 
-/* T of the group's pixel from its packed Gram sums (tcoh.cl:611-636), at
-   row (global memory, or the shared copy prefetched by prefetch_gram);
+/* T of the group's pixel from its packed Gram sums (tcoh.cl:611-636);
    identity for an inactive group. The entries come in two batches of 17
    and 16 per lane, each batch's loads issued before any use (one batch
    of 33 held 66 registers through the processing and spilled); upper_tab
    is the CTA's shared-memory copy of the packed-entry table. */
-__device__ void load_T(const TcStrip &s, const TcLinkConst &k, bool active, int looks,
-                       const float2 *row, const unsigned short *upper_tab, const HWs &w, int ld,
-                       const Grp &g, bool &boundary)
+__device__ void load_T(const TcStrip &s, const TcChunk &c, const TcLinkConst &k, int p, bool active,
+                       int looks, const float2 *__restrict__ gram,
+                       const unsigned short *upper_tab, const HWs &w, int ld, const Grp &g,
+                       bool &boundary)
 {
     const int n = s.n, npu = tc_npu(n);
     const int i0 = g.gl, i1 = g.gl + 16;
     float2 ga[17], gb[16];
 
-    const float d0 = (active && i0 < n) ? row[tc_pidx(n, i0, i0)].x : 1.f;
-    const float d1 = (active && i1 < n) ? row[tc_pidx(n, i1, i1)].x : 1.f;
+    const float d0 = (active && i0 < n) ? gram[tc_gram_at(npu, p, tc_pidx(n, i0, i0))].x : 1.f;
+    const float d1 = (active && i1 < n) ? gram[tc_gram_at(npu, p, tc_pidx(n, i1, i1))].x : 1.f;
 #pragma unroll
     for (int t = 0; t < 17; t++) {
         const int q = g.gl + 16 * t;
 
-        ga[t] = (active && q < npu) ? row[q] : make_float2(0.f, 0.f);
+        ga[t] = (active && q < npu) ? gram[tc_gram_at(npu, p, q)] : make_float2(0.f, 0.f);
     }
     if (i0 < n)
         w.nrm[i0] = d0 > 0.f ? __frcp_rn(__fsqrt_rn(d0)) : 0.f;
@@ -1202,28 +1179,11 @@ __device__ void load_T(const TcStrip &s, const TcLinkConst &k, bool active, int 
     for (int t = 0; t < 16; t++) {
         const int q = g.gl + 16 * (17 + t);
 
-        gb[t] = (active && q < npu) ? row[q] : make_float2(0.f, 0.f);
+        gb[t] = (active && q < npu) ? gram[tc_gram_at(npu, p, q)] : make_float2(0.f, 0.f);
     }
     load_T_batch<16>(gb, 17, n, npu, active, looks, k, upper_tab, w, ld, g, boundary);
     gsync(g);
     boundary = __any_sync(g.mask, boundary);
-}
-
-/* Asynchronous copy of pixel p's packed Gram sums (npu entries of 8 bytes,
-   at 8-byte alignment only: npu is odd) into dst in shared memory, entry
-   q by lane q mod 16 of the group, the lane that load_T has read it; one
-   commit group per call (empty when the pixel does not exist). */
-__device__ __forceinline__ void prefetch_gram(const float2 *__restrict__ gram, int npu, int p,
-                                              bool exists, float2 *dst, const Grp &g)
-{
-    if (exists)
-        for (int q = g.gl; q < npu; q += 16) {
-            const unsigned d = (unsigned)__cvta_generic_to_shared(dst + q);
-
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;"
-                         :: "r"(d), "l"(gram + tc_gram_at(npu, p, q)) : "memory");
-        }
-    asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
 /* Whether the non-zero coherences link all dates (n <= 32). */
@@ -1718,8 +1678,6 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
        than the instruction cache, and warps in different stages would keep
        evicting each other's instructions. */
     const int nq = (c.npix + 1) / 2;
-    /* EMI: whether this group's sums were prefetched into shared memory */
-    bool prefetched = false;
 
     for (int qb = blockIdx.x * wpb; qb < nq; qb += gridDim.x * wpb) {
         const int q = qb + warp;
@@ -1748,24 +1706,13 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
         }
         bool run = __any_sync(FULL, active);
 
-        if (prefetched) {
-            /* the copies issued during the previous pixel's last stage have
-               landed (waited for even when nothing reads them: a later
-               prefetch writes the same place) */
-            asm volatile("cp.async.wait_all;" ::: "memory");
-            gsync(g);
-        }
         /* stage 1: coherence matrix, pair coherences, connectivity */
         bool sent = false; /* the pixel is on the exact tier's list */
 
         if (run) {
             bool boundary = false;
 
-            /* with a prefetch, this pixel's sums are in the |T|^-1 region */
-            const float2 *row =
-                prefetched ? (const float2 *)w.G : gram + tc_gram_at(tc_npu(n), p, 0);
-
-            load_T(s, k, active, looks, row, s_upper, w, ld, g, boundary);
+            load_T(s, c, k, p, active, looks, gram, s_upper, w, ld, g, boundary);
             if (queue && active && boundary) {
                 sent = true;
                 if (g.gl == 0)
@@ -1894,16 +1841,6 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
                 }
             }
             __syncthreads();
-            /* |T|^-1 is no longer read (by the adjoint, after the last
-               stage): the next pixel's sums go there while the last stage
-               runs */
-            if (!ADJ) {
-                const int qn = qb + gridDim.x * wpb + warp;
-                const int pn = 2 * qn + (lane >> 4);
-
-                prefetch_gram(gram, tc_npu(n), pn, qn < nq && pn < c.npix, (float2 *)w.G, g);
-                prefetched = true;
-            }
         }
         /* last stage: phasors, temporal coherence, outputs */
         float2 ssum = make_float2(0.f, 0.f);
