@@ -456,6 +456,11 @@ __device__ unsigned tridiag_vector(int n, int index, const Ws &w, int lane)
 /* Shared-memory path (N <= 64).                                       */
 /* ------------------------------------------------------------------ */
 
+/* The eigenvector of rank `index` of the Hermitian matrix held in the lower
+   triangle (with the diagonal) of A (n x ld): Householder reduction in
+   place on that triangle, the reflectors' vectors left in its columns; the
+   strict upper triangle is neither read nor written (it keeps T for
+   gamma). */
 template <typename R>
 __device__ unsigned heig_smem(int n, int ld, typename Cx<R>::T *A, int index, const Ws &ws,
                               int lane, typename Cx<R>::T (&zo)[2])
@@ -518,11 +523,16 @@ __device__ unsigned heig_smem(int n, int ld, typename Cx<R>::T *A, int index, co
             wl[t] = mk<R>(0, 0);
             if (r > k && r < n) {
                 R sr = 0, si = 0;
-                const C *row = A + r * ld;
 
+                /* M_rj from the lower triangle: A[r][j] for j <= r, the
+                   conjugate of A[j][r] above */
                 for (int j = k + 1; j < n; j++) {
-                    const C a = row[j], v = vv[j];
+                    const bool low = j <= r;
+                    C a = A[low ? r * ld + j : j * ld + r];
+                    const C v = vv[j];
 
+                    if (!low)
+                        a.y = -a.y;
                     sr += a.x * v.x - a.y * v.y;
                     si += a.x * v.y + a.y * v.x;
                 }
@@ -558,7 +568,7 @@ __device__ unsigned heig_smem(int n, int ld, typename Cx<R>::T *A, int index, co
                 const C vr = vv[r], wr = wwv[r];
                 C *row = A + r * ld;
 
-                for (int j = k + 1; j < n; j++) {
+                for (int j = k + 1; j <= r; j++) {
                     const C vj = vv[j], wj = wwv[j];
                     C a = row[j];
 
@@ -972,16 +982,11 @@ tc_link_smem_kernel(TcStrip s, TcChunk c, TcLinkConst k, LinkLayout L,
             __syncwarp();
             continue;
         }
-        /* EVD (the EMI path of this many dates is tc_link_exact_kernel) */
-        float2 *A = (float2 *)w.A;
-
-        for (int r = lane; r < n; r += 32)
-            for (int j = 0; j < n; j++)
-                A[r * ld + j] = w.T[r * ld + j];
-        __syncwarp();
+        /* EVD (the EMI path of this many dates is tc_link_exact_kernel),
+           reduced in place on T's lower triangle */
         float2 z[2];
 
-        st |= heig_smem<float>(n, ld, A, n - 1, w, lane, z);
+        st |= heig_smem<float>(n, ld, w.T, n - 1, w, lane, z);
         const float gamma = phasors_and_gamma<float>(n, ld, w, z, upper_tab, lane);
 
         if (lane == 0)
@@ -1035,7 +1040,6 @@ constexpr int EX_THREADS = 128;
    dates, 71 blocks of 2 x 4 entries at most) leave room for 6, NB = 3 (up
    to 64 dates) for 3 */
 __host__ __device__ constexpr int ex_ctas(int nb) { return nb == 1 ? 6 : 3; }
-constexpr int EX_CTAS_MAX = 6;
 constexpr int EX_KC = 16;         /* candidates per staging block */
 /* the multisection's spacing: EX_THREADS points split an interval into
    EX_THREADS + 1 parts */
@@ -2204,25 +2208,19 @@ tc_link_exact_kernel(TcStrip s, TcChunk c, TcLinkConst k, ExLayout L,
     }
 }
 
-LinkLayout layout_for(int n, int emi, bool regs)
+LinkLayout layout_for(int n)
 {
     LinkLayout L;
 
     L.n = n;
     L.ld = n | 1;
     L.nv = even(n > 32 ? n : 32);
+    /* T in full storage: the strict upper triangle keeps T for the pair
+       coherences and gamma, the Householder reduction works in place on
+       the lower one */
     L.off_T = 0;
-    if (emi && !regs) {
-        /* |T| and its inverse share the working matrix's region */
-        L.off_A = even(n * L.ld);
-        L.off_G = L.off_A;
-        L.off_vec = even(L.off_A + 2 * n * L.ld);
-    }
-    else {
-        L.off_G = even(n * L.ld);
-        L.off_A = even(L.off_G + (emi ? n * L.ld : 0));
-        L.off_vec = even(L.off_A + (regs ? 0 : (emi ? 2 : 1) * n * L.ld));
-    }
+    L.off_G = L.off_A = 0;
+    L.off_vec = even(n * L.ld);
     L.per_warp = even(L.off_vec + VEC_UNITS(n, L.nv));
     return L;
 }
@@ -2347,7 +2345,7 @@ cudaError_t tc_launch_link(const TcStrip &s, const TcChunk &c, const TcLinkConst
         e = tc_launch_link_half(s, c, k, gram, mask, count, upper_tab, pair_tab, scratch, coh,
                                 pairs, phases, status, qb, qs, sms, st);
     else {
-        const LinkLayout L = layout_for(s.n, 0, false);
+        const LinkLayout L = layout_for(s.n);
         const size_t per_warp = (size_t)L.per_warp * sizeof(double);
         int wpb = (int)((227 * 1024) / per_warp);
 
