@@ -850,12 +850,16 @@ def main():
         ms = float(t.item())
         dist.barrier()
 
-    # Per-stage device time of one more step (events around every launch).
+    # Per-stage device time of one more step (events around every launch),
+    # with the per-pixel status bits of the whole strip.
+    status = torch.empty((rows, cols), dtype=torch.uint8, device=dev)
     be.set_timing(True)
-    step()
+    be.run_device(slc, amp, valid, rows, cols, coh, count, status=status, stream=stream)
     torch.cuda.synchronize()
     stages = be.stage_stats()
     be.set_timing(False)
+    status_h = status.cpu().numpy()
+    del status
     launches = sum(v[1] for k, v in stages.items() if k != "copy")
 
     npix = rows * cols
@@ -923,6 +927,9 @@ def main():
             "stages": kernels,
             "mean_shp_count": lbar,
             "estimated_fraction": float(estimated.mean()),
+            # pixels of the whole strip that the FP64 exact tier computed
+            "fp64_tier_fraction": float(((status_h & tcoh_b200.STATUS_FP64) != 0)[estimated].mean())
+            if estimated.any() else 0.0,
             "mean_coherence": float(np.nanmean(coh_h)) if np.isfinite(coh_h).any() else None,
             "clocks": ck}
 

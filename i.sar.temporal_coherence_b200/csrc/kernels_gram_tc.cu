@@ -20,15 +20,20 @@
  *   sum of the exact FP32 products. With two terms the last 8 bits are
  *   dropped: a relative error below 2^-16 per product.
  *
- * Per CTA (256 threads, two CTAs per SM): the packed entries are taken 128 at
- * a time ("phases"); a phase's accumulator is 128 lanes x 2h columns of TMEM
- * (re of entry r in column r, im in column h + r, h = entries rounded up to
- * 16). For each block of 32 candidates the CTA stages their samples in
- * shared memory, builds A and the B terms in the canonical K-major layout
- * without swizzle (8-row x 16-byte core matrices), and one thread issues the
- * MMAs (M = 128, N = 2h, K = 16) and commits them to an mbarrier; the next
- * block's samples load while they run. The epilogue reads the accumulator
- * with tcgen05.ld and writes gram[p][pidx] (float2), the layout the linking
+ * Per CTA (256 threads, two CTAs per SM, persistent): the packed entries are
+ * taken 128 at a time ("phases"); a phase's accumulator is 128 lanes x 2h
+ * columns of TMEM (re of entry r in column r, im in column h + r, h =
+ * entries rounded up to 16). The CTAs take (tile, phase) items in turn, so
+ * that the last round of a launch is split four ways instead of leaving
+ * whole tiles on a fraction of the SMs. For each block of 16 candidates
+ * (one MMA K step) the CTA builds A and the B terms in the canonical
+ * K-major layout without swizzle (8-row x 16-byte core matrices) into one
+ * of two operand buffers, and one thread issues the MMAs (M = 128,
+ * N = 2h, K = 16) and commits them to that buffer's mbarrier: block kb is
+ * built while block kb - 1 multiplies, and a buffer is rebuilt once the
+ * MMAs that read it (block kb - 2) have completed. The next block's samples
+ * load into registers meanwhile. The epilogue reads the accumulator with
+ * tcgen05.ld and writes gram[p][pidx] (float2), the layout the linking
  * kernels read.
  *
  * Candidates that are not finite contribute zero: a product with A = 0 must
@@ -45,8 +50,9 @@
 
 namespace {
 
-constexpr int KB = 32;            /* candidates per K block */
+constexpr int KB = 16;            /* candidates per K block: one MMA K step */
 constexpr int KCH = KB / 8;       /* 16-byte K chunks per K block */
+constexpr int STAGES = 2;         /* operand buffers */
 constexpr int THREADS = 256;
 constexpr int PHASE = 128;        /* packed entries per accumulator phase */
 constexpr int TMEM_COLS = 256;    /* 2 x PHASE FP32 columns */
@@ -58,32 +64,37 @@ constexpr int MAX_WA = 64;
 
 /* Shared-memory carve-up (byte offsets). */
 struct GramSmem {
-    int b;       /* 3 terms x KCH chunks x 256 rows x 16 B */
-    int a;       /* KCH chunks x 128 rows x 16 B */
+    int ops;     /* STAGES x (3 B terms x KCH chunks x 256 rows x 16 B, then A:
+                    KCH chunks x 128 rows x 16 B) */
     int stage;   /* n x STAGE_LD float2 */
+    int uyx;     /* K x u16: union row << 8 | union column of candidate u */
     int rows;    /* wa x 128 u32: SHP bits of each window row of each pixel */
     int pair;    /* npu x u16 */
     int expand;  /* 16 x uint2: four mask bits -> four BF16 0/1 */
-    int bar;     /* mbarrier (8 B), TMEM address (4 B), drain mbarrier (8 B) */
+    int bar;     /* STAGES mbarriers (16 B), TMEM address (4 B + pad), drain mbarrier (8 B) */
     int bytes;
 };
 
 constexpr int TERM_BYTES = KCH * 2 * PHASE * 16;
+constexpr int OP_BYTES = 3 * TERM_BYTES + KCH * 128 * 16;
+/* the epilogue stages each warp's 32 pixels x 16 entries (+1 pad) in the
+   idle operand buffers */
+static_assert(8 * 32 * 17 * 8 <= STAGES * OP_BYTES, "epilogue staging exceeds the operand buffers");
 
 __host__ __device__ inline int up16(int x) { return (x + 15) & ~15; }
 
-__host__ __device__ inline GramSmem gram_smem(int n, int wa)
+__host__ __device__ inline GramSmem gram_smem(int n, int wa, int wr)
 {
     GramSmem g;
 
-    g.b = 0;
-    g.a = g.b + 3 * TERM_BYTES;
-    g.stage = g.a + KCH * 128 * 16;
-    g.rows = g.stage + up16(n * STAGE_LD * 8);
+    g.ops = 0;
+    g.stage = g.ops + STAGES * OP_BYTES;
+    g.uyx = g.stage + up16(n * STAGE_LD * 8);
+    g.rows = g.uyx + up16((TC_TILE_H + wa - 1) * (TC_TILE_W + wr - 1) * 2);
     g.pair = g.rows + wa * 128 * 4;
     g.expand = g.pair + up16(tc_npu(n) * 2);
     g.bar = g.expand + 16 * 8;
-    g.bytes = g.bar + 24;
+    g.bytes = g.bar + 32;
     return g;
 }
 
@@ -200,28 +211,29 @@ __device__ __forceinline__ void split_store(const float (&v)[8], unsigned char *
         *(uint4 *)(dst + 2 * TERM_BYTES) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
 }
 
-/* Samples of this thread's share of K block kb: candidate t / 8 of the
-   block, dates t % 8 + 8 i. Zero outside the strip and for non-finite
-   values. */
+/* Samples of this thread's share of K block kb: candidate t / 16 of the
+   block, dates t % 16 + 16 i (16 lanes read one candidate's 128 contiguous
+   bytes). Zero outside the strip and the union, and for non-finite values. */
 struct Prefetch {
-    float2 v[TC_MAX_DATES / 8];
+    float2 v[TC_MAX_DATES / 16];
 };
 
 __device__ __forceinline__ void prefetch(Prefetch &f, const TcStrip &s, const float2 *slc,
-                                         int kb, int K, int UW, int y0, int x0, int t)
+                                         const unsigned short *uyx, int kb, int K, int y0,
+                                         int x0, int t)
 {
-    const int u = kb * KB + (t >> 3), sub = t & 7;
+    const int u = kb * KB + (t >> 4), sub = t & 15;
     const float2 *src = nullptr;
 
     if (u < K) {
-        const int uy = u / UW, py = y0 + uy, px = x0 + (u - uy * UW);
+        const int c = uyx[u], py = y0 + (c >> 8), px = x0 + (c & 255);
 
         if (py < s.padded_rows && px < s.W)
             src = slc + ((long long)py * s.W + px) * s.n;
     }
 #pragma unroll
-    for (int i = 0; i < TC_MAX_DATES / 8; i++) {
-        const int d = sub + 8 * i;
+    for (int i = 0; i < TC_MAX_DATES / 16; i++) {
+        const int d = sub + 16 * i;
 
         f.v[i] = src && d < s.n ? __ldg(src + d) : make_float2(0.f, 0.f);
     }
@@ -229,11 +241,11 @@ __device__ __forceinline__ void prefetch(Prefetch &f, const TcStrip &s, const fl
 
 __device__ __forceinline__ void stage_store(const Prefetch &f, float2 *stage, int n, int t)
 {
-    const int kk = t >> 3, sub = t & 7;
+    const int kk = t >> 4, sub = t & 15;
 
 #pragma unroll
-    for (int i = 0; i < TC_MAX_DATES / 8; i++) {
-        const int d = sub + 8 * i;
+    for (int i = 0; i < TC_MAX_DATES / 16; i++) {
+        const int d = sub + 16 * i;
 
         if (d < n) {
             float2 v = f.v[i];
@@ -245,47 +257,44 @@ __device__ __forceinline__ void stage_store(const Prefetch &f, float2 *stage, in
     }
 }
 
+/* Bounded wait for the MMAs that last read operand buffer b (if any). */
+__device__ __forceinline__ bool buffer_free(uint32_t bar0, int b, uint32_t &parity,
+                                            uint32_t &pending)
+{
+    if (!(pending >> b & 1u))
+        return true;
+    if (!mbar_wait(bar0 + 8 * b, parity >> b & 1u))
+        return false;
+    parity ^= 1u << b;
+    pending &= ~(1u << b);
+    return true;
+}
+
 __global__ void __launch_bounds__(THREADS, 2)
 tc_gram_tc_kernel(TcStrip s, TcChunk c, int terms, const float2 *__restrict__ slc,
                   const uint32_t *__restrict__ mask, float2 *__restrict__ gram)
 {
     extern __shared__ __align__(1024) unsigned char sm[];
     const int n = s.n, npu = tc_npu(n);
-    const GramSmem L = gram_smem(n, s.wa);
-    unsigned char *sB = sm + L.b, *sA = sm + L.a;
+    const GramSmem L = gram_smem(n, s.wa, s.wr);
     float2 *stage = (float2 *)(sm + L.stage);
+    unsigned short *s_uyx = (unsigned short *)(sm + L.uyx);
     uint32_t *s_rows = (uint32_t *)(sm + L.rows);
     unsigned short *s_pair = (unsigned short *)(sm + L.pair);
     uint2 *s_expand = (uint2 *)(sm + L.expand);
-    uint32_t *s_taddr = (uint32_t *)(sm + L.bar + 8);
-    const uint32_t bar = smem_u32(sm + L.bar);
+    uint32_t *s_taddr = (uint32_t *)(sm + L.bar + 8 * STAGES);
+    const uint32_t bar0 = smem_u32(sm + L.bar);
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-    const int tile = blockIdx.x;
-    const int ty = tile / c.tiles_x, tx = tile - ty * c.tiles_x;
-    const int y0 = c.row0 + ty * TC_TILE_H; /* padded row of union row 0 */
-    const int x0 = tx * TC_TILE_W;          /* padded column of union column 0 */
     const int UW = TC_TILE_W + s.wr - 1, K = (TC_TILE_H + s.wa - 1) * UW;
     const int nkb = (K + KB - 1) / KB;
+    const int nph = (npu + PHASE - 1) / PHASE;
+    const int items = c.npix / TC_TILE_PIX * nph;
     const uint32_t wr_mask = (1u << s.wr) - 1u;
-    Prefetch pf;
 
-    prefetch(pf, s, slc, 0, K, UW, y0, x0, t);
-    /* SHP bits of window row dy of pixel m (bit dx), zero for pixels outside
-       the output */
-    for (int e = t; e < s.wa * TC_TILE_PIX; e += THREADS) {
-        const int dy = e >> 7, m = e & 127;
-        const int y = y0 + (m >> 3), x = x0 + (m & 7);
-        uint32_t f = 0u;
+    for (int u = t; u < K; u += THREADS) {
+        const int uy = u / UW;
 
-        if (y < c.row0 + c.nrows && y < s.rows && x < s.cols) {
-            const int b = dy * s.wr, w = b >> 5, o = b & 31;
-            const long long p = (long long)tile * TC_TILE_PIX + m;
-            const uint32_t lo = mask[(long long)w * c.npix + p];
-            const uint32_t hi = o + s.wr > 32 ? mask[(long long)(w + 1) * c.npix + p] : 0u;
-
-            f = (uint32_t)(((unsigned long long)hi << 32 | lo) >> o) & wr_mask;
-        }
-        s_rows[e] = f;
+        s_uyx[u] = (unsigned short)(uy << 8 | (u - uy * UW));
     }
     for (int q = t; q < npu; q += THREADS) {
         int i = 0, r = q;
@@ -299,139 +308,156 @@ tc_gram_tc_kernel(TcStrip s, TcChunk c, int terms, const float2 *__restrict__ sl
     if (t < 16)
         s_expand[t] = make_uint2((t & 1 ? 0x3f80u : 0u) | (t & 2 ? 0x3f800000u : 0u),
                                  (t & 4 ? 0x3f80u : 0u) | (t & 8 ? 0x3f800000u : 0u));
-    stage_store(pf, stage, n, t);
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                      ::"r"(smem_u32(s_taddr)), "r"(TMEM_COLS) : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (t == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(1) : "memory");
+        for (int b = 0; b < STAGES; b++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar0 + 8 * b), "r"(1)
+                         : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     fence_before();
     __syncthreads();
     fence_after();
     const uint32_t tmem = *s_taddr;
-    uint32_t parity = 0;
-    bool ok = true, pending = false;
-    /* this thread's A rows and B items: pixel / entry t % 128, chunks
-       t / 128 and t / 128 + 2 */
-    const int m = t & 127, py = m >> 3, px = m & 7, g0 = t >> 7;
+    uint32_t parity = 0u, pending = 0u; /* bit b: operand buffer b */
+    bool ok = true;
+    int it = 0; /* K blocks issued by this CTA: block it uses buffer it % 2 */
+    /* this thread's A row and B item: pixel / entry t % 128, chunk t / 128 */
+    const int m = t & 127, py = m >> 3, px = m & 7, g = t >> 7;
+    Prefetch pf;
+    int item = blockIdx.x;
 
-    for (int P0 = 0; P0 < npu && ok; P0 += PHASE) {
+    for (; item < items; item += gridDim.x) {
+        const int tile = item / nph, P0 = (item - tile * nph) * PHASE;
+        const int ty = tile / c.tiles_x, tx = tile - ty * c.tiles_x;
+        const int y0 = c.row0 + ty * TC_TILE_H; /* padded row of union row 0 */
+        const int x0 = tx * TC_TILE_W;          /* padded column of union column 0 */
         const int np = min(PHASE, npu - P0), h = up16(np);
         const uint32_t lbo_b = 2 * h * 16;
         const uint32_t idesc = instr_desc(2 * h);
+        int pi = 0, pj = 0;
 
-        for (int kb = 0; kb < nkb; kb++) {
-            /* stage holds block kb; fetch the next block (of this phase, or
-               block 0 for the next phase) while this one is built */
-            const int next = kb + 1 < nkb ? kb + 1 : (P0 + PHASE < npu ? 0 : -1);
+        if (m < np) {
+            const int pr = s_pair[P0 + m];
 
-            if (next >= 0)
-                prefetch(pf, s, slc, next, K, UW, y0, x0, t);
-            if (pending) { /* the previous block's MMAs still read A and B */
-                ok = mbar_wait(bar, parity);
-                if (ok) {
-                    parity ^= 1;
-                    pending = false;
-                }
+            pi = pr >> 8;
+            pj = pr & 255;
+        }
+        prefetch(pf, s, slc, s_uyx, 0, K, y0, x0, t);
+        /* SHP bits of window row dy of pixel e % 128 (bit dx), zero for
+           pixels outside the output */
+        for (int e = t; e < s.wa * TC_TILE_PIX; e += THREADS) {
+            const int dy = e >> 7, q = e & 127;
+            const int y = y0 + (q >> 3), x = x0 + (q & 7);
+            uint32_t f = 0u;
+
+            if (y < c.row0 + c.nrows && y < s.rows && x < s.cols) {
+                const int b = dy * s.wr, w = b >> 5, o = b & 31;
+                const long long p = (long long)tile * TC_TILE_PIX + q;
+                const uint32_t lo = mask[(long long)w * c.npix + p];
+                const uint32_t hi = o + s.wr > 32 ? mask[(long long)(w + 1) * c.npix + p] : 0u;
+
+                f = (uint32_t)(((unsigned long long)hi << 32 | lo) >> o) & wr_mask;
             }
+            s_rows[e] = f;
+        }
+        stage_store(pf, stage, n, t);
+
+        for (int kb = 0; kb < nkb; kb++, it++) {
+            const int b = it & 1;
+            unsigned char *sB = sm + L.ops + b * OP_BYTES, *sA = sB + 3 * TERM_BYTES;
+
+            /* stage holds block kb; fetch block kb + 1 while it is built */
+            if (kb + 1 < nkb)
+                prefetch(pf, s, slc, s_uyx, kb + 1, K, y0, x0, t);
+            if (!buffer_free(bar0, b, parity, pending))
+                ok = false;
             if (!__syncthreads_and(ok)) {
                 ok = false;
                 break;
             }
-            /* A: pixel m, candidates 8g .. 8g + 7 of the block -> 16 bytes.
-               The 8 candidates span at most two union rows (UW >= 8). */
-#pragma unroll
-            for (int gi = 0; gi < 2; gi++) {
-                const int g = g0 + 2 * gi, u0 = kb * KB + g * 8;
-                const int uy = u0 / UW, ux = u0 - uy * UW, cnt = min(8, UW - ux);
+            /* A: pixel m, candidates u0 .. u0 + 7 -> 16 bytes. The 8
+               candidates span at most two union rows (UW >= 8). */
+            {
+                const int u0 = kb * KB + g * 8;
                 uint32_t bits = 0u;
-                int dy = uy - py;
 
-                if (dy >= 0 && dy < s.wa) {
-                    const uint32_t f = s_rows[dy * TC_TILE_PIX + m];
-                    const int sh = ux - px;
+                if (u0 < K) {
+                    const int cu = s_uyx[u0], ux = cu & 255, cnt = min(8, UW - ux);
+                    int dy = (cu >> 8) - py;
 
-                    bits = (sh >= 0 ? f >> sh : f << -sh) & ((1u << cnt) - 1u);
+                    if (dy >= 0 && dy < s.wa) {
+                        const uint32_t f = s_rows[dy * TC_TILE_PIX + m];
+                        const int sh = ux - px;
+
+                        bits = (sh >= 0 ? f >> sh : f << -sh) & ((1u << cnt) - 1u);
+                    }
+                    dy++;
+                    if (cnt < 8 && dy >= 0 && dy < s.wa)
+                        bits |= ((s_rows[dy * TC_TILE_PIX + m] << px) & ((1u << (8 - cnt)) - 1u))
+                                << cnt;
                 }
-                dy++;
-                if (cnt < 8 && dy >= 0 && dy < s.wa)
-                    bits |= ((s_rows[dy * TC_TILE_PIX + m] << px) & ((1u << (8 - cnt)) - 1u)) << cnt;
                 const uint2 lo = s_expand[bits & 15u], hi = s_expand[bits >> 4];
 
                 *(uint4 *)(sA + (g * TC_TILE_PIX + m) * 16) = make_uint4(lo.x, lo.y, hi.x, hi.y);
             }
-            /* B: entry r of the phase, candidates 8g .. 8g + 7; re in row r,
-               im in row h + r of each term */
+            /* B: entry r = m of the phase, candidates 8g .. 8g + 7; re in row
+               r, im in row h + r of each term */
             if (m < h) {
-                const int r = m;
-                int i = 0, j = 0;
+                float re[8], im[8];
 
-                if (r < np) {
-                    const int pr = s_pair[P0 + r];
-
-                    i = pr >> 8;
-                    j = pr & 255;
-                }
-#pragma unroll
-                for (int gi = 0; gi < 2; gi++) {
-                    const int g = g0 + 2 * gi;
-                    float re[8], im[8];
-
-                    if (r < np) {
-                        const float4 *si = (const float4 *)(stage + i * STAGE_LD + g * 8);
-                        const float4 *sj = (const float4 *)(stage + j * STAGE_LD + g * 8);
+                if (m < np) {
+                    const float4 *si = (const float4 *)(stage + pi * STAGE_LD + g * 8);
+                    const float4 *sj = (const float4 *)(stage + pj * STAGE_LD + g * 8);
 
 #pragma unroll
-                        for (int k = 0; k < 4; k++) {
-                            const float4 a = si[k], b = sj[k];
+                    for (int k = 0; k < 4; k++) {
+                        const float4 a = si[k], bb = sj[k];
 
-                            re[2 * k] = fmaf(a.x, b.x, a.y * b.y);
-                            im[2 * k] = fmaf(a.y, b.x, -(a.x * b.y));
-                            re[2 * k + 1] = fmaf(a.z, b.z, a.w * b.w);
-                            im[2 * k + 1] = fmaf(a.w, b.z, -(a.z * b.w));
-                        }
-                    } else {
-#pragma unroll
-                        for (int k = 0; k < 8; k++)
-                            re[k] = im[k] = 0.f;
+                        re[2 * k] = fmaf(a.x, bb.x, a.y * bb.y);
+                        im[2 * k] = fmaf(a.y, bb.x, -(a.x * bb.y));
+                        re[2 * k + 1] = fmaf(a.z, bb.z, a.w * bb.w);
+                        im[2 * k + 1] = fmaf(a.w, bb.z, -(a.z * bb.w));
                     }
-                    split_store(re, sB + (g * 2 * h + r) * 16, terms);
-                    split_store(im, sB + (g * 2 * h + h + r) * 16, terms);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 8; k++)
+                        re[k] = im[k] = 0.f;
                 }
+                split_store(re, sB + (g * 2 * h + m) * 16, terms);
+                split_store(im, sB + (g * 2 * h + h + m) * 16, terms);
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncthreads();
             if (t == 0) {
                 fence_after();
-#pragma unroll
-                for (int ks = 0; ks < KB / 16; ks++) {
-                    const uint64_t adesc =
-                        smem_desc(smem_u32(sA + ks * 2 * TC_TILE_PIX * 16), TC_TILE_PIX * 16, 128);
+                const uint64_t adesc = smem_desc(smem_u32(sA), TC_TILE_PIX * 16, 128);
 
-                    for (int term = 0; term < terms; term++) {
-                        const uint64_t bdesc =
-                            smem_desc(smem_u32(sB + term * TERM_BYTES + ks * 2 * lbo_b), lbo_b, 128);
+                for (int term = 0; term < terms; term++) {
+                    const uint64_t bdesc =
+                        smem_desc(smem_u32(sB + term * TERM_BYTES), lbo_b, 128);
 
-                        mma_bf16(tmem, adesc, bdesc, idesc, (kb | ks | term) != 0);
-                    }
+                    mma_bf16(tmem, adesc, bdesc, idesc, (kb | term) != 0);
                 }
-                mma_commit(bar);
+                mma_commit(bar0 + 8 * b);
             }
-            pending = true;
+            pending |= 1u << b;
             /* the B build above was the last reader of stage */
-            if (next >= 0)
+            if (kb + 1 < nkb)
                 stage_store(pf, stage, n, t);
         }
         if (!ok)
             break;
-        ok = mbar_wait(bar, parity);
-        if (ok) {
-            parity ^= 1;
-            pending = false;
+        /* every MMA of the phase has completed before TMEM is read */
+        for (int bb = 0; bb < STAGES; bb++) {
+            const int b = (it + bb) & 1; /* the older block first */
+
+            if (!buffer_free(bar0, b, parity, pending))
+                ok = false;
         }
         if (!__syncthreads_and(ok)) {
             ok = false;
@@ -445,10 +471,10 @@ tc_gram_tc_kernel(TcStrip s, TcChunk c, int terms, const float2 *__restrict__ sl
             const uint32_t lane_addr = tmem + ((uint32_t)(lg * 32) << 16);
 
             /* The warp's 32 pixels x 16 entries go through shared memory
-               (the B operand's region, idle until the next phase's first
+               (the operand buffers, idle until the next item's first
                barrier) so that each store writes two pixels' 16
                consecutive entries: whole 128-byte lines. */
-            float2 *stg = (float2 *)sB + warp * 32 * 17;
+            float2 *stg = (float2 *)(sm + L.ops) + warp * 32 * 17;
 
             for (int cg = warp >> 2; cg * 16 < np; cg += 2) {
                 uint32_t vr[16], vi[16];
@@ -468,28 +494,37 @@ tc_gram_tc_kernel(TcStrip s, TcChunk c, int terms, const float2 *__restrict__ sl
                 const int k = lane & 15, r = cg * 16 + k;
 
 #pragma unroll 4
-                for (int it = 0; it < 16; it++) {
-                    const int px = 2 * it + (lane >> 4);
+                for (int q = 0; q < 16; q++) {
+                    const int pxl = 2 * q + (lane >> 4);
 
                     if (r < np)
-                        gram[tc_gram_at(npu, (long long)tile * TC_TILE_PIX + lg * 32 + px,
-                                        P0 + r)] = stg[px * 17 + k];
+                        gram[tc_gram_at(npu, (long long)tile * TC_TILE_PIX + lg * 32 + pxl,
+                                        P0 + r)] = stg[pxl * 17 + k];
                 }
                 __syncwarp();
             }
         }
         fence_before();
+        /* the next item's first barrier orders these TMEM reads and staging
+           loads before its MMAs and operand stores */
+        __syncthreads();
     }
     if (!ok) {
         if (t == 0) {
             atomicOr(&g_gram_fault, 1);
-            if (!drain_mmas(smem_u32(sm + L.bar + 16)))
+            if (!drain_mmas(smem_u32(sm + L.bar + 8 * STAGES + 8)))
                 atomicOr(&g_gram_fault, 2);
         }
         __syncthreads();
-        for (int e = t; e < npu * TC_TILE_PIX; e += THREADS)
-            gram[tc_gram_at(npu, (long long)tile * TC_TILE_PIX + (e & 127), e >> 7)] =
-                make_float2(__int_as_float(0x7fc00000), __int_as_float(0x7fc00000));
+        /* the items this CTA did not finish: their entries read NaN */
+        for (; item < items; item += gridDim.x) {
+            const int tile = item / nph, P0 = (item - tile * nph) * PHASE;
+            const int np = min(PHASE, npu - P0);
+
+            for (int e = t; e < np * TC_TILE_PIX; e += THREADS)
+                gram[tc_gram_at(npu, (long long)tile * TC_TILE_PIX + (e & 127), P0 + (e >> 7))] =
+                    make_float2(__int_as_float(0x7fc00000), __int_as_float(0x7fc00000));
+        }
     }
     __syncthreads();
     fence_after();
@@ -802,15 +837,24 @@ cudaError_t tc_launch_gram_tensor(const TcStrip &s, const TcChunk &c, int split_
                                   const float *slc, const uint32_t *mask, float2 *gram,
                                   cudaStream_t st)
 {
-    const GramSmem L = gram_smem(s.n, s.wa);
+    const GramSmem L = gram_smem(s.n, s.wa, s.wr);
     const int bytes = L.bytes < MIN_SMEM ? MIN_SMEM : L.bytes;
+    const int items = c.npix / TC_TILE_PIX * ((tc_npu(s.n) + PHASE - 1) / PHASE);
+    int dev = 0, sms = 0;
     cudaError_t e;
 
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return e;
     if ((e = cudaFuncSetAttribute(tc_gram_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   bytes)) != cudaSuccess)
         return e;
-    tc_gram_tc_kernel<<<c.npix / TC_TILE_PIX, THREADS, bytes, st>>>(
-        s, c, split_terms < 3 ? 2 : 3, (const float2 *)slc, mask, gram);
+    /* persistent: two CTAs per SM (the TMEM of two accumulators) */
+    const int grid = items < 2 * sms ? items : 2 * sms;
+
+    if (grid > 0)
+        tc_gram_tc_kernel<<<grid, THREADS, bytes, st>>>(s, c, split_terms < 3 ? 2 : 3,
+                                                        (const float2 *)slc, mask, gram);
     return cudaGetLastError();
 }
 
