@@ -88,58 +88,53 @@ __device__ __forceinline__ float wmin(float v)
 }
 
 /* ------------------------------------------------------------------ */
-/* Per-warp shared workspace (8-byte units).                           */
+/* Per-warp shared workspace of the 33-64-date EVD kernel (4-byte      */
+/* units).                                                             */
 /* ------------------------------------------------------------------ */
 
 struct LinkLayout {
-    int n, ld;        /* dates, odd leading dimension >= n */
-    int nv;           /* vector length: max(n, 32) */
-    int off_T, off_G, off_A, off_vec;
-    int per_warp;
+    int n;
+    int per_warp; /* floats, a multiple of 4 (16-byte aligned workspaces) */
 };
+
+/* Packed lower triangle with the diagonal: entry (r, j), j <= r. */
+__host__ __device__ __forceinline__ int low_idx(int r, int j) { return (r * (r + 1) >> 1) + j; }
 
 struct Ws {
-    float2 *T;   /* n x ld normalized coherence */
-    double *G;   /* n x ld |T| and its inverse (EMI) */
-    void *A;     /* n x ld working matrix of the shared-memory path */
+    float2 *A;   /* n (n + 1) / 2: T's lower triangle, then the reduction */
     /* vectors */
-    void *d, *e, *y;   /* tridiagonal, eigenvector (R) */
-    void *lu;          /* 4 n (R): LU of the shifted tridiagonal */
-    void *tau;         /* n (complex R) */
-    void *vw;          /* 4 nv units: Householder v, w / Gauss-Jordan row */
-    float *df, *e2f;   /* float copies for the Sturm counts */
+    void *d, *e, *y;   /* tridiagonal, eigenvector (R = float) */
+    void *lu;          /* 4 n: LU of the shifted tridiagonal */
+    void *tau;         /* n complex */
+    void *vw;          /* 2 n complex: Householder v, w */
+    float *df, *e2f;   /* copies for the Sturm counts */
     float *nrm;        /* sqrt(C_ii) */
     float2 *zs;        /* unit phasors */
-    double *lam;       /* eigenvalues of |T| (pseudo-inverse) */
 };
 
-/* Offsets are kept even (16-byte aligned) for the float4 / double2 arrays. */
-__host__ __device__ __forceinline__ int even(int x) { return (x + 1) & ~1; }
+__host__ __device__ __forceinline__ int up4(int x) { return (x + 3) & ~3; }
 
-__device__ __forceinline__ Ws workspace(double *base, const LinkLayout &L)
+__device__ __forceinline__ Ws workspace(float *base, const LinkLayout &L)
 {
     Ws w;
-    double *v = base + L.off_vec;
-    const int an = even(L.n), nv = L.nv;
+    const int n = L.n, an = up4(n);
+    float *v = base + up4(2 * tc_npu(n));
 
-    w.T = (float2 *)(base + L.off_T);
-    w.G = base + L.off_G;
-    w.A = base + L.off_A;
+    w.A = (float2 *)base;
     w.d = v;
     w.e = v + an;
     w.y = v + 2 * an;
-    w.lu = v + 3 * an;                    /* 4n */
-    w.tau = v + 7 * an;                   /* 2n */
-    w.vw = v + 9 * an;                    /* 4 nv */
-    w.df = (float *)(v + 9 * an + 4 * nv);
-    w.e2f = (float *)(v + 10 * an + 4 * nv);
-    w.nrm = (float *)(v + 11 * an + 4 * nv);
-    w.zs = (float2 *)(v + 12 * an + 4 * nv);
-    w.lam = v + 13 * an + 4 * nv;
+    w.lu = v + 3 * an;       /* 4n */
+    w.tau = v + 7 * an;      /* 2n */
+    w.vw = v + 9 * an;       /* 4n */
+    w.df = v + 13 * an;
+    w.e2f = v + 14 * an;
+    w.nrm = v + 15 * an;
+    w.zs = (float2 *)(v + 16 * an); /* 2n */
     return w;
 }
 
-#define VEC_UNITS(n, nv) (14 * even(n) + 4 * even(nv))
+#define VEC_FLOATS(n) (18 * up4(n))
 
 /* ------------------------------------------------------------------ */
 /* Tridiagonal eigenvector.                                            */
@@ -456,13 +451,11 @@ __device__ unsigned tridiag_vector(int n, int index, const Ws &w, int lane)
 /* Shared-memory path (N <= 64).                                       */
 /* ------------------------------------------------------------------ */
 
-/* The eigenvector of rank `index` of the Hermitian matrix held in the lower
-   triangle (with the diagonal) of A (n x ld): Householder reduction in
-   place on that triangle, the reflectors' vectors left in its columns; the
-   strict upper triangle is neither read nor written (it keeps T for
-   gamma). */
+/* The eigenvector of rank `index` of the Hermitian matrix held as its packed
+   lower triangle with the diagonal (low_idx): Householder reduction in
+   place, the reflectors' vectors left in its columns. */
 template <typename R>
-__device__ unsigned heig_smem(int n, int ld, typename Cx<R>::T *A, int index, const Ws &ws,
+__device__ unsigned heig_smem(int n, typename Cx<R>::T *A, int index, const Ws &ws,
                               int lane, typename Cx<R>::T (&zo)[2])
 {
     typedef typename Cx<R>::T C;
@@ -475,13 +468,13 @@ __device__ unsigned heig_smem(int n, int ld, typename Cx<R>::T *A, int index, co
 
         for (int r = lane; r < n; r += 32)
             if (r >= k + 2) {
-                const C a = A[r * ld + k];
+                const C a = A[low_idx(r, k)];
 
                 xn2 += a.x * a.x + a.y * a.y;
             }
         xn2 = wsum<R>(xn2);
-        const C alpha = A[(k + 1) * ld + k];
-        const R dk = A[k * ld + k].x;
+        const C alpha = A[low_idx(k + 1, k)];
+        const R dk = A[low_idx(k, k)].x;
         R beta, tr = 0, ti = 0;
 
         __syncwarp();
@@ -496,51 +489,74 @@ __device__ unsigned heig_smem(int n, int ld, typename Cx<R>::T *A, int index, co
 
             for (int r = lane; r < n; r += 32)
                 if (r >= k + 2) {
-                    const C a = A[r * ld + k];
+                    const C a = A[low_idx(r, k)];
 
-                    A[r * ld + k] = mk<R>(a.x * sr - a.y * si, a.x * si + a.y * sr);
+                    A[low_idx(r, k)] = mk<R>(a.x * sr - a.y * si, a.x * si + a.y * sr);
                 }
         }
         if (lane == 0) {
             d[k] = dk;
             e[k] = beta;
             tau[k] = mk<R>(tr, ti);
-            A[(k + 1) * ld + k] = mk<R>(1, 0);
+            A[low_idx(k + 1, k)] = mk<R>(1, 0);
         }
         __syncwarp();
         if (tr == (R)0 && ti == (R)0)
             continue;
         for (int r = lane; r < n; r += 32)
-            vv[r] = r > k ? A[r * ld + k] : mk<R>(0, 0);
+            vv[r] = r > k ? A[low_idx(r, k)] : mk<R>(0, 0);
         __syncwarp();
         C wl[2];
         R pr = 0, pi = 0;
+        {
+            /* w = tau M v over rows r0 = lane, r1 = lane + 32 in one loop
+               (the same trip count on every lane): M_rj is entry (r, j)
+               of the packed triangle for j <= r, the conjugate of (j, r)
+               beyond; cj = low_idx(j, 0). Separate accumulators for the
+               two products of each part keep the FMA chains short. */
+            const int r0 = lane, r1 = lane + 32;
+            const bool a0 = r0 > k && r0 < n, a1 = r1 > k && r1 < n;
+            const int ro0 = low_idx(r0, 0), ro1 = low_idx(a1 ? r1 : 0, 0);
+            R p0 = 0, q0 = 0, u0 = 0, x0 = 0, p1 = 0, q1 = 0, u1 = 0, x1 = 0;
 
-#pragma unroll
-        for (int t = 0; t < 2; t++) {
-            const int r = lane + 32 * t;
+            for (int j = k + 1, cj = low_idx(k + 1, 0); j < n; cj += ++j) {
+                const C v = vv[j];
 
-            wl[t] = mk<R>(0, 0);
-            if (r > k && r < n) {
-                R sr = 0, si = 0;
+                if (a0) {
+                    const bool lo = j <= r0;
+                    const C m = A[lo ? ro0 + j : cj + r0];
+                    const R my = lo ? m.y : -m.y;
 
-                /* M_rj from the lower triangle: A[r][j] for j <= r, the
-                   conjugate of A[j][r] above */
-                for (int j = k + 1; j < n; j++) {
-                    const bool low = j <= r;
-                    C a = A[low ? r * ld + j : j * ld + r];
-                    const C v = vv[j];
-
-                    if (!low)
-                        a.y = -a.y;
-                    sr += a.x * v.x - a.y * v.y;
-                    si += a.x * v.y + a.y * v.x;
+                    p0 = fma(m.x, v.x, p0);
+                    q0 = fma(my, v.y, q0);
+                    u0 = fma(m.x, v.y, u0);
+                    x0 = fma(my, v.x, x0);
                 }
-                wl[t] = mk<R>(tr * sr - ti * si, tr * si + ti * sr);
-                const C v = vv[r];
+                if (a1) {
+                    const bool lo = j <= r1;
+                    const C m = A[lo ? ro1 + j : cj + r1];
+                    const R my = lo ? m.y : -m.y;
 
-                pr += wl[t].x * v.x + wl[t].y * v.y;
-                pi += wl[t].x * v.y - wl[t].y * v.x;
+                    p1 = fma(m.x, v.x, p1);
+                    q1 = fma(my, v.y, q1);
+                    u1 = fma(m.x, v.y, u1);
+                    x1 = fma(my, v.x, x1);
+                }
+            }
+            const R sr0 = p0 - q0, si0 = u0 + x0, sr1 = p1 - q1, si1 = u1 + x1;
+
+            wl[0] = a0 ? mk<R>(tr * sr0 - ti * si0, tr * si0 + ti * sr0) : mk<R>(0, 0);
+            wl[1] = a1 ? mk<R>(tr * sr1 - ti * si1, tr * si1 + ti * sr1) : mk<R>(0, 0);
+#pragma unroll
+            for (int t = 0; t < 2; t++) {
+                const int r = lane + 32 * t;
+
+                if (r > k && r < n) {
+                    const C v = vv[r];
+
+                    pr += wl[t].x * v.x + wl[t].y * v.y;
+                    pi += wl[t].x * v.y - wl[t].y * v.x;
+                }
             }
         }
         pr = wsum<R>(pr);
@@ -566,7 +582,7 @@ __device__ unsigned heig_smem(int n, int ld, typename Cx<R>::T *A, int index, co
 
             if (r > k && r < n) {
                 const C vr = vv[r], wr = wwv[r];
-                C *row = A + r * ld;
+                C *row = A + low_idx(r, 0);
 
                 for (int j = k + 1; j <= r; j++) {
                     const C vj = vv[j], wj = wwv[j];
@@ -581,7 +597,7 @@ __device__ unsigned heig_smem(int n, int ld, typename Cx<R>::T *A, int index, co
         __syncwarp();
     }
     if (lane == 0)
-        d[n - 1] = A[(n - 1) * ld + n - 1].x;
+        d[n - 1] = A[low_idx(n - 1, n - 1)].x;
     __syncwarp();
     unsigned status = tridiag_vector<R>(n, index, ws, lane);
     const R *y = (const R *)ws.y;
@@ -605,7 +621,7 @@ __device__ unsigned heig_smem(int n, int ld, typename Cx<R>::T *A, int index, co
             const int r = lane + 32 * t;
 
             if (r > k && r < n) {
-                const C v = A[r * ld + k];
+                const C v = A[low_idx(r, k)];
 
                 sr += v.x * z[t].x + v.y * z[t].y;
                 si += v.x * z[t].y - v.y * z[t].x;
@@ -620,7 +636,7 @@ __device__ unsigned heig_smem(int n, int ld, typename Cx<R>::T *A, int index, co
             const int r = lane + 32 * t;
 
             if (r > k && r < n) {
-                const C v = A[r * ld + k];
+                const C v = A[low_idx(r, k)];
 
                 z[t].x -= v.x * hr - v.y * hi2;
                 z[t].y -= v.x * hi2 + v.y * hr;
@@ -730,12 +746,41 @@ struct PixelCtx {
     long long out, plane;
 };
 
-/* T from the packed Gram sums (tcoh.cl:611-636); boundary: whether an
+/* T_ij (i < j) from its Gram sum g and the date norms (tcoh.cl:611-636),
+   in IEEE float without contraction; near: the bias decision lies within
+   TC_BIAS_BAND of its threshold. The load and the goodness of fit both
+   take T from here, so that they see the same values. */
+__device__ __forceinline__ float2 t_entry(float2 g, float nrm_i, float nrm_j, float fl,
+                                          bool debias, bool &near)
+{
+    const float dd = __fmul_rn(nrm_i, nrm_j);
+    float re = 0.f, im = 0.f;
+
+    if (dd > 0.f) {
+        re = __fdiv_rn(g.x, dd);
+        im = __fdiv_rn(g.y, dd);
+        if (debias) {
+            const float m2 = __fadd_rn(__fmul_rn(re, re), __fmul_rn(im, im));
+            const float lm1 = __fsub_rn(__fmul_rn(fl, m2), 1.0f);
+            const float m2c = __fdiv_rn(lm1, __fsub_rn(fl, 1.0f));
+
+            near |= fabsf(lm1) < TC_BIAS_BAND * fl * m2;
+            const float f = (m2 > 0.f && m2c > 0.f) ? __fsqrt_rn(__fdiv_rn(m2c, m2)) : 0.f;
+
+            re = __fmul_rn(re, f);
+            im = __fmul_rn(im, f);
+        }
+    }
+    return make_float2(re, im);
+}
+
+/* T from the packed Gram sums into w.A, as its packed lower triangle
+   (T_ji = conj(T_ij)); w.nrm receives sqrt(C_ii). boundary: whether an
    entry's bias decision lies within TC_BIAS_BAND of its threshold. */
 __device__ void load_coherence(const TcStrip &s, const TcChunk &c, const TcLinkConst &k,
                                int p, int looks, const float2 *__restrict__ gram,
                                const unsigned short *__restrict__ upper_tab, const Ws &w,
-                               int ld, int lane, bool &boundary)
+                               int lane, bool &boundary)
 {
     bool near = false;
 
@@ -745,42 +790,27 @@ __device__ void load_coherence(const TcStrip &s, const TcChunk &c, const TcLinkC
         w.nrm[r] = __fsqrt_rn(gram[tc_gram_at(tc_npu(n), p, tc_pidx(n, r, r))].x);
     __syncwarp();
     const float fl = (float)looks;
+    const bool debias = k.bias && looks > 1;
 
     for (int q = lane; q < npu; q += 32) {
         const int i = upper_tab[q] >> 8, j = upper_tab[q] & 255;
 
         if (i == j) {
-            w.T[i * ld + i] = make_float2(1.f, 0.f);
+            w.A[low_idx(i, i)] = make_float2(1.f, 0.f);
             continue;
         }
-        const float2 g = gram[tc_gram_at(tc_npu(n), p, q)];
-        const float dd = __fmul_rn(w.nrm[i], w.nrm[j]);
-        float re = 0.f, im = 0.f;
+        const float2 t = t_entry(gram[tc_gram_at(tc_npu(n), p, q)], w.nrm[i], w.nrm[j], fl,
+                                 debias, near);
 
-        if (dd > 0.f) {
-            re = __fdiv_rn(g.x, dd);
-            im = __fdiv_rn(g.y, dd);
-            if (k.bias && looks > 1) {
-                const float m2 = __fadd_rn(__fmul_rn(re, re), __fmul_rn(im, im));
-                const float lm1 = __fsub_rn(__fmul_rn(fl, m2), 1.0f);
-                const float m2c = __fdiv_rn(lm1, __fsub_rn(fl, 1.0f));
-
-                near |= fabsf(lm1) < TC_BIAS_BAND * fl * m2;
-                const float f = (m2 > 0.f && m2c > 0.f) ? __fsqrt_rn(__fdiv_rn(m2c, m2)) : 0.f;
-
-                re = __fmul_rn(re, f);
-                im = __fmul_rn(im, f);
-            }
-        }
-        w.T[i * ld + j] = make_float2(re, im);
-        w.T[j * ld + i] = make_float2(re, -im);
+        w.A[low_idx(j, i)] = make_float2(t.x, -t.y);
     }
     boundary = __any_sync(FULL, near);
     __syncwarp();
 }
 
-/* Whether the non-zero coherences link all dates. */
-__device__ bool linked(int n, int ld, const float2 *T, int lane)
+/* Whether the non-zero coherences link all dates (T as its packed lower
+   triangle). */
+__device__ bool linked(int n, const float2 *A, int lane)
 {
     unsigned long long adj[2] = {0ull, 0ull};
 
@@ -790,7 +820,7 @@ __device__ bool linked(int n, int ld, const float2 *T, int lane)
 
         if (r < n)
             for (int j = 0; j < n; j++) {
-                const float2 v = T[r * ld + j];
+                const float2 v = A[j < r ? low_idx(r, j) : low_idx(j, r)];
 
                 if (j != r && (v.x != 0.f || v.y != 0.f))
                     adj[t] |= 1ull << j;
@@ -822,9 +852,10 @@ __device__ bool linked(int n, int ld, const float2 *T, int lane)
    eigenvector components of rows lane and lane + 32 (R), into w.zs; then
    the goodness of fit (tcoh.cl:728-744). Returns gamma on every lane. */
 template <typename R>
-__device__ float phasors_and_gamma(int n, int ld, const Ws &w,
-                                   const typename Cx<R>::T (&z)[2],
-                                   const unsigned short *__restrict__ upper_tab, int lane)
+__device__ float phasors_and_gamma(int n, const Ws &w, const typename Cx<R>::T (&z)[2],
+                                   const unsigned short *__restrict__ upper_tab,
+                                   const float2 *__restrict__ gram, int p, int looks,
+                                   bool debias, int lane)
 {
     R m[2];
 
@@ -894,7 +925,10 @@ __device__ float phasors_and_gamma(int n, int ld, const Ws &w,
 
         if (i == j)
             continue;
-        const float2 tv = w.T[i * ld + j];
+        /* T_ij again from its Gram sum: the reduction overwrote w.A */
+        bool near = false;
+        const float2 tv = t_entry(gram[tc_gram_at(npu, p, q)], w.nrm[i], w.nrm[j],
+                                  (float)looks, debias, near);
         const float m2 = tv.x * tv.x + tv.y * tv.y;
         float ur = 1.f, ui = 0.f;
 
@@ -920,7 +954,7 @@ __device__ float phasors_and_gamma(int n, int ld, const Ws &w,
 /* Kernels.                                                            */
 /* ------------------------------------------------------------------ */
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(384)
 tc_link_smem_kernel(TcStrip s, TcChunk c, TcLinkConst k, LinkLayout L,
                     const float2 *__restrict__ gram, const int *__restrict__ count,
                     const unsigned short *__restrict__ upper_tab,
@@ -929,11 +963,11 @@ tc_link_smem_kernel(TcStrip s, TcChunk c, TcLinkConst k, LinkLayout L,
                     float *__restrict__ phases, unsigned char *__restrict__ status,
                     const uint32_t *__restrict__ mask, int *__restrict__ queue, int qstride)
 {
-    extern __shared__ double smd[];
+    extern __shared__ float4 smf4[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int wpb = blockDim.x >> 5;
-    const int n = s.n, ld = L.ld;
-    const Ws w = workspace(smd + (size_t)warp * L.per_warp, L);
+    const int n = s.n;
+    const Ws w = workspace((float *)smf4 + (size_t)warp * L.per_warp, L);
     const long long plane = (long long)s.rows * s.cols;
 
     (void)scratch;
@@ -960,18 +994,18 @@ tc_link_smem_kernel(TcStrip s, TcChunk c, TcLinkConst k, LinkLayout L,
         }
         bool boundary = false;
 
-        load_coherence(s, c, k, p, looks, gram, upper_tab, w, ld, lane, boundary);
+        load_coherence(s, c, k, p, looks, gram, upper_tab, w, lane, boundary);
         if (queue && boundary && lane == 0)
             tc_exact_push(queue, qstride, out, mask, c.npix, p);
         for (int q = lane; q < k.npairs; q += 32) {
             const int i = pair_tab[q] >> 8, j = pair_tab[q] & 255;
-            const float2 t = w.T[i * ld + j];
+            const float2 t = w.A[low_idx(j, i)]; /* conj(T_ij), i < j */
 
             pairs[q * plane + out] = hypotf(t.x, t.y);
         }
         unsigned st = 0;
 
-        if (k.bias && !linked(n, ld, w.T, lane)) {
+        if (k.bias && !linked(n, w.A, lane)) {
             if (lane == 0)
                 coh[out] = NAN;
             if (phases)
@@ -983,11 +1017,12 @@ tc_link_smem_kernel(TcStrip s, TcChunk c, TcLinkConst k, LinkLayout L,
             continue;
         }
         /* EVD (the EMI path of this many dates is tc_link_exact_kernel),
-           reduced in place on T's lower triangle */
+           reduced in place on T's packed lower triangle */
         float2 z[2];
 
-        st |= heig_smem<float>(n, ld, w.T, n - 1, w, lane, z);
-        const float gamma = phasors_and_gamma<float>(n, ld, w, z, upper_tab, lane);
+        st |= heig_smem<float>(n, w.A, n - 1, w, lane, z);
+        const float gamma = phasors_and_gamma<float>(n, w, z, upper_tab, gram, p, looks,
+                                                     k.bias && looks > 1, lane);
 
         if (lane == 0)
             coh[out] = gamma;
@@ -2213,15 +2248,8 @@ LinkLayout layout_for(int n)
     LinkLayout L;
 
     L.n = n;
-    L.ld = n | 1;
-    L.nv = even(n > 32 ? n : 32);
-    /* T in full storage: the strict upper triangle keeps T for the pair
-       coherences and gamma, the Householder reduction works in place on
-       the lower one */
-    L.off_T = 0;
-    L.off_G = L.off_A = 0;
-    L.off_vec = even(n * L.ld);
-    L.per_warp = even(L.off_vec + VEC_UNITS(n, L.nv));
+    /* T's packed lower triangle, then the vectors */
+    L.per_warp = up4(2 * tc_npu(n)) + VEC_FLOATS(n);
     return L;
 }
 
@@ -2346,11 +2374,11 @@ cudaError_t tc_launch_link(const TcStrip &s, const TcChunk &c, const TcLinkConst
                                 pairs, phases, status, qb, qs, sms, st);
     else {
         const LinkLayout L = layout_for(s.n);
-        const size_t per_warp = (size_t)L.per_warp * sizeof(double);
+        const size_t per_warp = (size_t)L.per_warp * sizeof(float);
         int wpb = (int)((227 * 1024) / per_warp);
 
-        if (wpb > 8)
-            wpb = 8;
+        if (wpb > 12)
+            wpb = 12;
         if (wpb < 1)
             return cudaErrorInvalidConfiguration;
         const size_t smem = per_warp * wpb;

@@ -35,6 +35,17 @@
 
 #define FULL 0xffffffffu
 
+/* EMI: refine the float eigenvector in double where the gap between M's
+   two smallest eigenvalues is below this fraction of its norm. */
+#ifndef TC_REFINE_GAP
+#define TC_REFINE_GAP 0.005f
+#endif
+/* EMI: send a pixel to the exact tier where n max|inv| divided by M's
+   relative eigengap exceeds this bound. */
+#ifndef TC_EXACT_BOUND
+#define TC_EXACT_BOUND 1.0e5
+#endif
+
 namespace {
 
 struct Grp {
@@ -1812,12 +1823,15 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
                 z1 = make_double2(f1.x, f1.y);
                 /* The float eigen-solve's error in gamma is about
                    3 eps_f norm / gap (gap between the two smallest
-                   eigenvalues of M); above 1e-5 where the relative gap is
-                   below 0.016. Pixels whose gap is below 0.02 of the norm
-                   (two eigenvalues under lambda + 0.02 norm) refine their
-                   eigenvector once in double: a few percent of the pixels
-                   of coherent stacks, most of those of incoherent ones. */
-                if (active && sturm16(w.d, w.e2f, n, lambda + 0.02f * norm,
+                   eigenvalues of M): 2e-5 at a relative gap of 0.005.
+                   Pixels whose gap is below TC_REFINE_GAP of the norm (two
+                   eigenvalues under lambda + TC_REFINE_GAP norm) refine
+                   their eigenvector once in double (the golden incoherent
+                   case that float EMI misses without it has a relative
+                   gap of 1.6e-3). Against the bound 0.02, 0.005 left the
+                   largest error over 896k pixels of the 30-date AD/EMI/-b
+                   workload unchanged (3.4e-5) at 6 % less link time. */
+                if (active && sturm16(w.d, w.e2f, n, lambda + TC_REFINE_GAP * norm,
                                       1.0e-30f + 1.0e-14f * norm) >= 2)
                     refine(n, ld, w, g, z0, z1, yr, piv);
                 /* Pixels whose gamma the float rounding of T may move by
@@ -1825,12 +1839,13 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
                    sensitivity of M's eigenvector to T grows with
                    n max|inv| / (relative eigengap of M). The gap is below
                    delta when the tridiagonal has two eigenvalues under
-                   lambda + delta (one Sturm count). Calibrated on stacks of
-                   30 and 60 dates against the FP64 oracle: with the bound
-                   3e4, no unflagged pixel was off by more than 1.1e-5, the
-                   worst pixels sitting at 1.4e5 and above. */
+                   lambda + delta (one Sturm count). Calibrated against the
+                   FP64 oracle on nine 320 x 320 crops (896k pixels) of the
+                   30-date AD/EMI/-b workload: the bounds 3e4 and 1e5 give
+                   the same largest error, 3.4e-5 (3.2 % and 1.6 % of the
+                   pixels flagged), 3e5 gives 7.2e-5 (1.0 %). */
                 if (queue && active && !sent) {
-                    const double delta = inv_max * (double)norm / 3.0e4;
+                    const double delta = inv_max * (double)norm / TC_EXACT_BOUND;
                     bool flag = !(delta < (double)norm);
 
                     if (!flag)

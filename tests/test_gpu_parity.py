@@ -140,9 +140,17 @@ def test_synthetic_vs_oracle(case, gram):
     m = ~np.isnan(o["coh"])
     err = np.abs(r["coh"][m] - o["coh"][m])
     assert err.max() <= TOLERANCE, err.max()
-    # Per-date phases, relative to the reference date.
+    # Per-date phases, relative to the reference date. The reference writes
+    # no phases (its tests check gamma and the pair coherences only), so
+    # this bound is this backend's own: every phase of a pixel whose
+    # coherence is at least 0.2 within 1e-3 rad of the oracle's, and 99 %
+    # of all. Below 0.2 the eigenvector's phases are set by noise-level
+    # differences between nearly equal eigenvalues and move by more.
     dph = np.abs(wrap(r["phases"][m].astype(np.float64) - o["phases"][m]))
     assert np.percentile(dph, 99) < 1e-3, np.percentile(dph, 99)
+    strong = o["coh"][m] >= 0.2
+    if strong.any():
+        assert dph[strong].max() < 1e-3, dph[strong].max()
 
 
 @pytest.mark.parametrize("gram", GRAMS)
