@@ -1158,34 +1158,52 @@ __device__ __forceinline__ void load_T_batch(const float2 (&gv)[B], int t0, int 
     }
 }
 
+/* The first batch of a pixel's packed Gram sums (entries gl + 16 t, t < 17)
+   and its two diagonal sums, loaded for load_T (zero where out of range).
+   The link kernel issues these loads for the next pixel pair during the
+   last stage of the current one, so that they arrive while gamma runs. */
+struct TFirst {
+    float2 ga[17];
+    float d0, d1;
+};
+
+__device__ __forceinline__ void t_first(TFirst &f, int n, int p, bool inrange,
+                                        const float2 *__restrict__ gram, const Grp &g)
+{
+    const int npu = tc_npu(n), i0 = g.gl, i1 = g.gl + 16;
+
+    f.d0 = (inrange && i0 < n) ? gram[tc_gram_at(npu, p, tc_pidx(n, i0, i0))].x : 1.f;
+    f.d1 = (inrange && i1 < n) ? gram[tc_gram_at(npu, p, tc_pidx(n, i1, i1))].x : 1.f;
+#pragma unroll
+    for (int t = 0; t < 17; t++) {
+        const int q = g.gl + 16 * t;
+
+        f.ga[t] = (inrange && q < npu) ? gram[tc_gram_at(npu, p, q)] : make_float2(0.f, 0.f);
+    }
+}
+
 /* T of the group's pixel from its packed Gram sums (tcoh.cl:611-636);
    identity for an inactive group. The entries come in two batches of 17
-   and 16 per lane, each batch's loads issued before any use (one batch
-   of 33 held 66 registers through the processing and spilled); upper_tab
-   is the CTA's shared-memory copy of the packed-entry table. */
+   (f, loaded ahead) and 16 per lane, each batch's loads issued before any
+   use (one batch of 33 held 66 registers through the processing and
+   spilled); upper_tab is the CTA's shared-memory copy of the packed-entry
+   table. */
 __device__ void load_T(const TcStrip &s, const TcChunk &c, const TcLinkConst &k, int p, bool active,
-                       int looks, const float2 *__restrict__ gram,
+                       int looks, const float2 *__restrict__ gram, const TFirst &f,
                        const unsigned short *upper_tab, const HWs &w, int ld, const Grp &g,
                        bool &boundary)
 {
     const int n = s.n, npu = tc_npu(n);
     const int i0 = g.gl, i1 = g.gl + 16;
-    float2 ga[17], gb[16];
+    float2 gb[16];
+    const float d0 = active ? f.d0 : 1.f, d1 = active ? f.d1 : 1.f;
 
-    const float d0 = (active && i0 < n) ? gram[tc_gram_at(npu, p, tc_pidx(n, i0, i0))].x : 1.f;
-    const float d1 = (active && i1 < n) ? gram[tc_gram_at(npu, p, tc_pidx(n, i1, i1))].x : 1.f;
-#pragma unroll
-    for (int t = 0; t < 17; t++) {
-        const int q = g.gl + 16 * t;
-
-        ga[t] = (active && q < npu) ? gram[tc_gram_at(npu, p, q)] : make_float2(0.f, 0.f);
-    }
     if (i0 < n)
         w.nrm[i0] = d0 > 0.f ? __frcp_rn(__fsqrt_rn(d0)) : 0.f;
     if (i1 < n)
         w.nrm[i1] = d1 > 0.f ? __frcp_rn(__fsqrt_rn(d1)) : 0.f;
     gsync(g);
-    load_T_batch<17>(ga, 0, n, npu, active, looks, k, upper_tab, w, ld, g, boundary);
+    load_T_batch<17>(f.ga, 0, n, npu, active, looks, k, upper_tab, w, ld, g, boundary);
 #pragma unroll
     for (int t = 0; t < 16; t++) {
         const int q = g.gl + 16 * (17 + t);
@@ -1690,17 +1708,31 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
        evicting each other's instructions. */
     const int nq = (c.npix + 1) / 2;
 
-    for (int qb = blockIdx.x * wpb; qb < nq; qb += gridDim.x * wpb) {
+    /* pixel of this group in the pair block starting at qb: its output
+       index (-1 outside the output) */
+    auto locate = [&](int qb, int &p) -> long long {
         const int q = qb + warp;
-        const int p = 2 * q + (lane >> 4);
         int y = 0, x = 0;
 
+        p = 2 * q + (lane >> 4);
         if (q < nq)
             tc_pixel_yx(c, p, y, x);
         const bool inrange =
             q < nq && p < c.npix && y < c.row0 + c.nrows && y < s.rows && x < s.cols;
-        const long long out = inrange ? (long long)y * s.cols + x : 0;
-        const int looks = inrange ? count[out] : -1;
+        return inrange ? (long long)y * s.cols + x : -1ll;
+    };
+    TFirst tf;
+    int next_p = 0;
+    long long next_out = locate(blockIdx.x * wpb, next_p);
+    int next_looks = next_out >= 0 ? count[next_out] : -1;
+
+    t_first(tf, n, next_p, next_out >= 0, gram, g);
+    for (int qb = blockIdx.x * wpb; qb < nq; qb += gridDim.x * wpb) {
+        const int q = qb + warp;
+        const int p = next_p;
+        const bool inrange = next_out >= 0;
+        const long long out = inrange ? next_out : 0;
+        const int looks = next_looks;
         bool active = inrange && looks >= k.min_looks;
         unsigned st = 0;
 
@@ -1723,7 +1755,7 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
         if (run) {
             bool boundary = false;
 
-            load_T(s, c, k, p, active, looks, gram, s_upper, w, ld, g, boundary);
+            load_T(s, c, k, p, active, looks, gram, tf, s_upper, w, ld, g, boundary);
             if (queue && active && boundary) {
                 sent = true;
                 if (g.gl == 0)
@@ -1857,7 +1889,16 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
             }
             __syncthreads();
         }
-        /* last stage: phasors, temporal coherence, outputs */
+        /* last stage: phasors, temporal coherence, outputs; the next pair's
+           first sums load meanwhile (after the backward stage with ADJ,
+           which needs the registers) */
+        auto prefetch_next = [&]() {
+            next_out = locate(qb + gridDim.x * wpb, next_p);
+            next_looks = next_out >= 0 ? count[next_out] : -1;
+            t_first(tf, n, next_p, next_out >= 0, gram, g);
+        };
+        if (!ADJ)
+            prefetch_next();
         float2 ssum = make_float2(0.f, 0.f);
 
         if (run) {
@@ -1890,6 +1931,8 @@ tc_link_half_kernel(TcStrip s, TcChunk c, TcLinkConst k, HalfLayout L,
                 for (int t = g.gl; t < tc_npu(n); t += 16)
                     gbar[(long long)t * c.npix + p] = make_float2(0.f, 0.f);
         }
+        if (ADJ)
+            prefetch_next();
         __syncthreads();
     }
 }
