@@ -14,11 +14,12 @@
  * - a column is the real or the imaginary part of one packed upper-triangle
  *   entry (i, j), and B[k][col] the same part of the candidate's product
  *   s_k,i conj(s_k,j). The product is formed once in FP32 and split exactly
- *   into BF16 terms by truncation: hi = its top 8 significand bits, mid the
- *   next 8, lo the last 8 (hi + mid + lo == the FP32 product, bit for bit).
- *   Each term is one MMA pass into the same FP32 accumulator, so D is an FP32
- *   sum of the exact FP32 products. With two terms the last 8 bits are
- *   dropped: a relative error below 2^-16 per product.
+ *   into BF16 terms by rounding to nearest: hi = the product to 8
+ *   significant bits, mid = the remainder to 8 bits, lo = the rest, exact
+ *   (hi + mid + lo == the FP32 product, bit for bit). Each term is one MMA
+ *   pass into the same FP32 accumulator, so D is an FP32 sum of the exact
+ *   FP32 products. With two terms lo is dropped: a relative error of at
+ *   most 2^-17 per product.
  *
  * Per CTA (256 threads, two CTAs per SM, persistent): the packed entries are
  * taken 128 at a time ("phases"); a phase's accumulator is 128 lanes x 2h
@@ -186,24 +187,37 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16])
                  : "r"(taddr));
 }
 
-/* Splits 8 FP32 values into truncated BF16 terms and stores each term's 16
-   bytes; term t goes to dst + t * TERM_BYTES. */
+/* Splits 8 FP32 values into BF16 terms and stores each term's 16 bytes;
+   term t goes to dst + t * TERM_BYTES. Rounding to nearest: hi = x to 8
+   significant bits, mid = the remainder x - hi to 8 bits, lo = what is
+   left, at most 8 significant bits, so exact; hi + mid + lo == x for every
+   finite x whose rounding to 8 bits stays finite (|x| below 3.39e38).
+   The pair conversion (cvt.rn.bf16x2.f32) packs two values at once. */
+__device__ __forceinline__ uint32_t bf16x2(float lo_half, float hi_half)
+{
+    uint32_t d;
+
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi_half), "f"(lo_half));
+    return d;
+}
+
 __device__ __forceinline__ void split_store(const float (&v)[8], unsigned char *dst, int terms)
 {
     uint32_t hi[4], mid[4], lo[4];
 
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-        const uint32_t a = __float_as_uint(v[2 * k]), b = __float_as_uint(v[2 * k + 1]);
-        const float ra = v[2 * k] - __uint_as_float(a & 0xffff0000u);
-        const float rb = v[2 * k + 1] - __uint_as_float(b & 0xffff0000u);
-        const uint32_t ua = __float_as_uint(ra), ub = __float_as_uint(rb);
-        const float la = ra - __uint_as_float(ua & 0xffff0000u);
-        const float lb = rb - __uint_as_float(ub & 0xffff0000u);
+        const float a = v[2 * k], b = v[2 * k + 1];
 
-        hi[k] = __byte_perm(a, b, 0x7632);
-        mid[k] = __byte_perm(ua, ub, 0x7632);
-        lo[k] = __byte_perm(__float_as_uint(la), __float_as_uint(lb), 0x7632);
+        hi[k] = bf16x2(a, b);
+        const float ra = a - __uint_as_float(hi[k] << 16);
+        const float rb = b - __uint_as_float(hi[k] & 0xffff0000u);
+
+        mid[k] = bf16x2(ra, rb);
+        const float la = ra - __uint_as_float(mid[k] << 16);
+        const float lb = rb - __uint_as_float(mid[k] & 0xffff0000u);
+
+        lo[k] = bf16x2(la, lb);
     }
     *(uint4 *)dst = make_uint4(hi[0], hi[1], hi[2], hi[3]);
     *(uint4 *)(dst + TERM_BYTES) = make_uint4(mid[0], mid[1], mid[2], mid[3]);
