@@ -638,7 +638,16 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
     const int tiles_x = (cols + TC_TILE_W - 1) / TC_TILE_W;
     const long long max_npix = (long long)(crows / TC_TILE_H) * tiles_x * TC_TILE_PIX;
 
-    CK(ensure(o->mask, sizeof(uint32_t) * s.mask_words * max_npix));
+    /* SHP masks are selected for blocks of up to 16 chunks at once (each
+       pair of the block's pixels tested once): about 64 MB of masks */
+    const long long chunk_words = (long long)s.mask_words * max_npix;
+    long long shp_chunks = (64ll << 20) / (4 * chunk_words);
+
+    if (shp_chunks > 16)
+        shp_chunks = 16;
+    if (shp_chunks < 1)
+        shp_chunks = 1;
+    CK(ensure(o->mask, sizeof(uint32_t) * chunk_words * shp_chunks));
     CK(ensure(o->gram, sizeof(float2) * tc_npu(o->n) * max_npix));
     CK(ensure(o->link_scratch, tc_link_scratch_bytes(o->n, o->sms)));
     TcLinkConst lk;
@@ -737,18 +746,41 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
             CK(cudaStreamWaitEvent(st, ready->done[b], 0));
         }
 
-        t = tm.begin(ST_SHP);
-        CK(tc_launch_shp(s, c, o->shp, amp, valid, (const float2 *)o->logstat.p,
-                         (uint32_t *)o->mask.p, count, o->sms, st));
-        tm.end(t);
+        if (chunk % shp_chunks == 0) {
+            TcShpBlock b;
+
+            b.row0 = row0;
+            b.nrows = rows - row0 < shp_chunks * crows ? rows - row0 : (int)(shp_chunks * crows);
+            b.crows = crows;
+            b.tiles_x = tiles_x;
+            b.chunk_words = chunk_words;
+            if (ready) {
+                const int last = row0 + b.nrows + o->wa - 2;
+                int rb = last / ready->block_rows;
+
+                if (rb >= ready->nblocks)
+                    rb = ready->nblocks - 1;
+                CK(cudaStreamWaitEvent(st, ready->done[rb], 0));
+            }
+            t = tm.begin(ST_SHP);
+            CK(cudaMemsetAsync(o->mask.p, 0,
+                               sizeof(uint32_t) * chunk_words *
+                                   ((b.nrows + crows - 1) / crows), st));
+            CK(tc_launch_shp_block(s, b, o->shp, amp, valid, (const float2 *)o->logstat.p,
+                                   (uint32_t *)o->mask.p, count, o->sms, st));
+            tm.end(t);
+        }
+        /* this chunk's masks in the block's region */
+        const uint32_t *cmask = (const uint32_t *)o->mask.p + (chunk % shp_chunks) * chunk_words;
+
         if (adj || tc_link_needs_gram(o->n, o->emi)) {
             t = tm.begin(ST_GRAM);
             if (o->opt.gram == TC_GRAM_FP32)
                 CK(tc_launch_gram_fp32(s, c, o->gram_block, (const float2 *)o->soa.p,
-                                       (const uint32_t *)o->mask.p, (float2 *)o->gram.p, st));
+                                       cmask, (float2 *)o->gram.p, st));
             else
                 CK(tc_launch_gram_tensor(s, c, o->opt.split_terms, slc,
-                                         (const uint32_t *)o->mask.p, (float2 *)o->gram.p, st));
+                                         cmask, (float2 *)o->gram.p, st));
             tm.end(t);
         }
         if (q.buf && q.pending + c.npix > q.capacity) {
@@ -760,7 +792,7 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
         t = tm.begin(ST_LINK);
         if (!adj)
             CK(tc_launch_link(s, c, lk, (const float2 *)o->gram.p, slc,
-                              (const uint32_t *)o->mask.p, count, &q,
+                              cmask, count, &q,
                               (const unsigned short *)o->upper_tab.p,
                               (const unsigned short *)o->pair_tab.p,
                               (double *)o->link_scratch.p, coh, pairs, phases, status, o->sms,
@@ -775,11 +807,11 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
             t = tm.begin(ST_ADJOINT);
             if (o->opt.gram == TC_GRAM_TENSOR && tc_gram_adjoint_tensor_supported(o->n, o->wa, o->wr))
                 CK(tc_launch_adjoint_scatter_tensor(s, c, o->wr / 2, adj->gbar,
-                                                    (const uint32_t *)o->mask.p, slc, adj->dtheta,
+                                                    cmask, slc, adj->dtheta,
                                                     st));
             else
                 CK(tc_launch_adjoint_scatter(s, c, o->wr / 2, adj->gbar,
-                                             (const uint32_t *)o->mask.p, slc, adj->dtheta, st));
+                                             cmask, slc, adj->dtheta, st));
         }
         tm.end(t);
         if (!q.buf) {

@@ -219,6 +219,25 @@ cudaError_t tc_launch_shp(const TcStrip &s, const TcChunk &c, const TcShpConst &
                           const float *amp, const unsigned char *valid,
                           const float2 *logstat, uint32_t *mask, int *count,
                           int sms, cudaStream_t st);
+
+/* A block of consecutive chunks whose SHP masks are selected together
+   (tc_launch_shp_block): output rows row0 .. row0 + nrows - 1, chunks of
+   crows rows (a multiple of TC_TILE_H) whose masks lie chunk_words u32
+   apart, chunk j's in the layout of a chunk (word w of its pixel p at
+   w * npix_j + p). */
+struct TcShpBlock {
+    int row0, nrows, crows, tiles_x;
+    long long chunk_words;
+};
+
+/* SHP masks and counts of a block of chunks with every unordered pair of
+   output pixels of the block tested once (the tests are symmetric when
+   the two series share no value; pairs with a tie are tested both ways).
+   The block's mask region must be zero on entry (the kernels OR bits in). */
+cudaError_t tc_launch_shp_block(const TcStrip &s, const TcShpBlock &b, const TcShpConst &k,
+                                const float *amp, const unsigned char *valid,
+                                const float2 *logstat, uint32_t *mask, int *count, int sms,
+                                cudaStream_t st);
 cudaError_t tc_launch_gram_fp32(const TcStrip &s, const TcChunk &c, int block,
                                 const float2 *soa, const uint32_t *mask,
                                 float2 *gram, cudaStream_t st);
