@@ -166,6 +166,35 @@ def test_chunking_is_invisible(gram):
     assert np.array_equal(outs[0]["coh"], outs[1]["coh"], equal_nan=True)
 
 
+@pytest.mark.parametrize("test", ["ks", "ad", "tlog"])
+@pytest.mark.parametrize("chunk", [0, 256])
+def test_shp_with_tied_amplitudes(test, chunk):
+    """Amplitudes rounded to a coarse grid, so that most pairs of
+    series share values: each pair is tested once in a block of chunks and
+    its other direction taken from the same test when the series share no
+    value, walked again the other way when they do. The counts must still
+    be the reference kernel's, bit for bit; with chunks of 256 pixels the
+    300 rows make 19 chunks of 16 rows, two blocks of at most 16 chunks,
+    so that pairs also cross a block edge."""
+    n, rows, cols = 10, 300, 20
+    stack = syn.generate(n, rows, cols, seed=11, null_frac=0.0)
+    # amplitudes on multiples of 64 (about a tenth of their mean) and phases
+    # on multiples of pi / 2, so that the float amplitudes sqrt(re^2 + im^2)
+    # are those multiples exactly
+    q = np.maximum(np.round(np.abs(stack) / 64.0) * 64.0, 64.0)
+    quarter = np.round(np.angle(stack) / (np.pi / 2)).astype(int) % 4
+    stack = (q * np.array([1, 1j, -1, -1j])[quarter]).astype(np.complex64)
+    slc, amp, valid = tcoh_b200.read_strip(stack.real, stack.imag, -10, rows + 20, 3)
+    kw = dict(window=(21, 7), shp_test=test, alpha=0.05, min_shp=n, estimator="evd")
+    a = amp.reshape(-1, n)
+    assert sum(np.intersect1d(a[1000], a[1000 + k]).size > 0 for k in range(1, 8)) > 4
+    with backend_for(n, cols, "fp32", chunk_pixels=chunk, **kw) as be:
+        r = be.run(slc, amp, valid, rows, cols)
+    o = oracle.run_oracle(slc, amp, valid, rows, cols, shp_fp32=True, **kw)
+    assert np.array_equal(r["count"], o["count"])
+    assert_close(r["coh"], o["coh"])
+
+
 @pytest.mark.parametrize("gram", GRAMS)
 @pytest.mark.parametrize("rows,cols", [(1, 1), (1, 9), (17, 1), (3, 200)])
 def test_tiny_and_ragged_regions(rows, cols, gram):
