@@ -1714,33 +1714,48 @@ __device__ void ex_householder(int n, int npu, const ExWs &w)
         __syncthreads();
         if (!reflect)
             continue;
-        /* p = M22 v over rows k+1 .. n-1, two threads per row (columns of
-           one parity each): M_ij = conj(P(j, i)) for j < i, at
-           rb(j) + i - j with rb(j) = j (2n - j + 1) / 2, then P(i, j) for
-           j >= i, contiguous */
-        const int i = k + 1 + (t >> 1), h = t & 1;
+        /* p = M22 v over rows k+1 .. n-1, R threads per row (R = 4 up to 32
+           dates, else 2; thread h takes the columns j = h mod R): M_ij =
+           conj(P(j, i)) for j < i, at rb(j) + i - j with rb(j) = j (2n - j
+           + 1) / 2, then P(i, j) for j >= i, contiguous. Separate
+           accumulators for the two products of each part keep the FMA
+           chains one deep. */
+        const int lr = n <= 32 ? 2 : 1, R = 1 << lr;
+        const int i = k + 1 + (t >> lr), h = t & (R - 1);
         double sx = 0.0, sy = 0.0;
 
         if (i < n) {
             int j = k + 1 + h;
             int idx = j * (2 * n - j + 1) / 2 + (i - j);
+            double ax = 0.0, bx = 0.0, ay = 0.0, by = 0.0;
 
-            for (; j < i; j += 2) {
+            for (; j < i; j += R) {
                 const double2 m = w.T[idx], v = w.v[j];
 
-                sx = fma(m.x, v.x, fma(m.y, v.y, sx));
-                sy = fma(m.x, v.y, fma(-m.y, v.x, sy));
-                idx += 2 * (n - j) - 3;
+                ax = fma(m.x, v.x, ax);
+                bx = fma(m.y, v.y, bx);
+                ay = fma(m.x, v.y, ay);
+                by = fma(m.y, v.x, by);
+                idx += R * (2 * n - 2 * j - R + 1) / 2 - R;
             }
-            for (idx = i * (2 * n - i + 1) / 2 + (j - i); j < n; j += 2, idx += 2) {
+            sx = ax + bx;
+            sy = ay - by;
+            ax = bx = ay = by = 0.0;
+            for (idx = i * (2 * n - i + 1) / 2 + (j - i); j < n; j += R, idx += R) {
                 const double2 m = w.T[idx], v = w.v[j];
 
-                sx = fma(m.x, v.x, fma(-m.y, v.y, sx));
-                sy = fma(m.x, v.y, fma(m.y, v.x, sy));
+                ax = fma(m.x, v.x, ax);
+                bx = fma(m.y, v.y, bx);
+                ay = fma(m.x, v.y, ay);
+                by = fma(m.y, v.x, by);
             }
+            sx += ax - bx;
+            sy += ay + by;
         }
-        sx += __shfl_xor_sync(FULL, sx, 1);
-        sy += __shfl_xor_sync(FULL, sy, 1);
+        for (int o = 1; o < R; o <<= 1) {
+            sx += __shfl_xor_sync(FULL, sx, o);
+            sy += __shfl_xor_sync(FULL, sy, o);
+        }
         const double2 wl = make_double2(tr * sx - ti * sy, tr * sy + ti * sx);
         double pr = 0.0, pi = 0.0;
 

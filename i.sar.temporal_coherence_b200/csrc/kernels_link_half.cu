@@ -1258,16 +1258,20 @@ __device__ bool linked16(int n, int ld, const float2 *T, const Grp &g)
 /* Unit phasors relative to the median date (tcoh.cl:700-724) into w.zs,
    then the goodness of fit (tcoh.cl:728-744), pairs spread evenly over the
    lanes. */
-__device__ float gamma16(int n, int ld, const HWs &w, const Grp &g, double2 z0, double2 z1,
+__device__ float gamma16(int n, int ld, const HWs &w, const Grp &g, double2 z0d, double2 z1d,
                          const unsigned short *__restrict__ upper_tab, float2 *sum = nullptr)
 {
+    /* the phasors in float, as the reference kernel forms them: the
+       eigenvector's components carry float accuracy at best */
+    const float2 z0 = make_float2((float)z0d.x, (float)z0d.y);
+    const float2 z1 = make_float2((float)z1d.x, (float)z1d.y);
     const int i0 = g.gl, i1 = g.gl + 16;
-    const double m0 = i0 < n ? hypot(z0.x, z0.y) : 0.0, m1 = i1 < n ? hypot(z1.x, z1.y) : 0.0;
-    const double mx = gmaxd(fmax(m0, m1), g);
+    const float m0 = i0 < n ? hypotf(z0.x, z0.y) : 0.f, m1 = i1 < n ? hypotf(z1.x, z1.y) : 0.f;
+    const float mx = gmaxf(fmaxf(m0, m1), g);
     int ref = n / 2;
-    const double mref = gbcast(ref < 16 ? m0 : m1, ref, g);
+    const float mref = gbcast(ref < 16 ? m0 : m1, ref, g);
 
-    if (mref <= 1.0e-3 * mx) {
+    if (mref <= 1.0e-3f * mx) {
         int last = -1;
 
         if (i0 < n && m0 == mx)
@@ -1279,23 +1283,22 @@ __device__ float gamma16(int n, int ld, const HWs &w, const Grp &g, double2 z0, 
             last = max(last, __shfl_xor_sync(g.mask, last, o));
         ref = last;
     }
-    const double zrx = gbcast(ref < 16 ? z0.x : z1.x, ref, g);
-    const double zry = gbcast(ref < 16 ? z0.y : z1.y, ref, g);
-    const double refm = hypot(zrx, zry);
-    const double refr = zrx / refm, refi = -zry / refm;
-    const double floor_ = mx * 1.0e-3;
+    const float zrx = gbcast(ref < 16 ? z0.x : z1.x, ref, g);
+    const float zry = gbcast(ref < 16 ? z0.y : z1.y, ref, g);
+    const float refm = hypotf(zrx, zry);
+    const float refr = zrx / refm, refi = -zry / refm;
+    const float floor_ = mx * 1.0e-3f;
 
 #pragma unroll
     for (int t = 0; t < 2; t++) {
         const int r = t ? i1 : i0;
-        const double2 z = t ? z1 : z0;
+        const float2 z = t ? z1 : z0;
 
         if (r < n) {
-            const double re = z.x * refr - z.y * refi, im = z.x * refi + z.y * refr;
-            const double mm = hypot(re, im);
+            const float re = z.x * refr - z.y * refi, im = z.x * refi + z.y * refr;
+            const float mm = hypotf(re, im);
 
-            w.zs[r] = mm > floor_ ? make_float2((float)(re / mm), (float)(im / mm))
-                                  : make_float2(1.f, 0.f);
+            w.zs[r] = mm > floor_ ? make_float2(re / mm, im / mm) : make_float2(1.f, 0.f);
         }
     }
     gsync(g);
@@ -1382,25 +1385,27 @@ __device__ void backward16(int n, int ld, const HWs &w, const Grp &g, double2 z0
     const int i0 = g.gl, i1 = g.gl + 16;
 
     /* unit-norm z in float; the phasor decisions (reference date, floor)
-       are those of gamma16, from the double rows */
+       are those of gamma16, made on the rows rounded to float */
+    const float mf0 = i0 < n ? hypotf((float)z0d.x, (float)z0d.y) : 0.f;
+    const float mf1 = i1 < n ? hypotf((float)z1d.x, (float)z1d.y) : 0.f;
+    const float mxf = gmaxf(fmaxf(mf0, mf1), g);
     const double m0 = i0 < n ? hypot(z0d.x, z0d.y) : 0.0, m1 = i1 < n ? hypot(z1d.x, z1d.y) : 0.0;
-    const double mx = gmaxd(fmax(m0, m1), g);
     int ref = n / 2;
-    const double mref = gbcast(ref < 16 ? m0 : m1, ref, g);
+    const float mref = gbcast(ref < 16 ? mf0 : mf1, ref, g);
 
-    if (mref <= 1.0e-3 * mx) {
+    if (mref <= 1.0e-3f * mxf) {
         int last = -1;
 
-        if (i0 < n && m0 == mx)
+        if (i0 < n && mf0 == mxf)
             last = i0;
-        if (i1 < n && m1 == mx)
+        if (i1 < n && mf1 == mxf)
             last = i1;
 #pragma unroll
         for (int o = 8; o; o >>= 1)
             last = max(last, __shfl_xor_sync(g.mask, last, o));
         ref = last;
     }
-    const bool big0 = i0 < n && m0 > mx * 1.0e-3, big1 = i1 < n && m1 > mx * 1.0e-3;
+    const bool big0 = i0 < n && mf0 > mxf * 1.0e-3f, big1 = i1 < n && mf1 > mxf * 1.0e-3f;
     const double nn = gsum(m0 * m0 + m1 * m1, g);
     const double inv = nn > 0.0 ? 1.0 / sqrt(nn) : 0.0;
     const float2 z0 = make_float2((float)(z0d.x * inv), (float)(z0d.y * inv));
