@@ -1451,8 +1451,12 @@ __device__ bool ex_linked(int n, const ExWs &w)
    sweeping pivot k maps a_ij -> a_ij - a_ik a_kj / a_kk,
    a_ik, a_kj -> a_ik / a_kk, a_kk -> -1 / a_kk, and all pivots leave
    -A^-1, negated back at the end. It takes indefinite matrices. False when
-   a pivot's magnitude is not above floor_ (A is then undefined). */
-__device__ bool ex_sweep(int n, int npu, const ExWs &w, double *A, double floor_)
+   a pivot's magnitude is not above floor_ (A is then undefined).
+   Two forms: up to 32 dates the scaled pivot row goes to w.rrow behind its
+   own barrier (ex_sweep_rows); above, each step copies the next pivot row
+   as it updates it, one barrier a pivot (ex_sweep_lean), which pays where
+   the pivots are many. */
+__device__ bool ex_sweep_rows(int n, int npu, const ExWs &w, double *A, double floor_)
 {
     const int t = threadIdx.x;
 
@@ -1486,6 +1490,68 @@ __device__ bool ex_sweep(int n, int npu, const ExWs &w, double *A, double floor_
         A[q] = -A[q];
     __syncthreads();
     return true;
+}
+
+__device__ bool ex_sweep_lean(int n, int npu, const ExWs &w, double *A, double floor_)
+{
+    const int t = threadIdx.x;
+    /* the pivot row as it stands before its step, in one of two buffers
+       (w.lu, free until the eigenvector): the step that updates row kp + 1
+       also copies it to the other buffer, so that one barrier a pivot
+       suffices */
+    double *raw[2] = {w.lu, w.lu + 64};
+
+    for (int j = t; j < n; j += EX_THREADS)
+        raw[0][j] = A[ex_sym(n, 0, j)];
+    __syncthreads();
+    for (int kp = 0; kp < n; kp++) {
+        const double *rk = raw[kp & 1];
+        double *rn = raw[(kp + 1) & 1];
+        const double d = rk[kp];
+
+        if (!(fabs(d) > floor_)) {
+            __syncthreads();
+            return false;
+        }
+        const double id = ex_rcp_any(d);
+
+        for (int q = t; q < npu; q += EX_THREADS) {
+            const int i = w.tab[q] >> 8, j = w.tab[q] & 255;
+            const double ri = rk[i] * id, rj = rk[j] * id;
+            double a;
+
+            if (i == kp && j == kp)
+                a = -id;
+            else if (i == kp)
+                a = rj;
+            else if (j == kp)
+                a = ri;
+            else
+                a = fma(-ri * d, rj, A[q]);
+            A[q] = a;
+            if (i == kp + 1)
+                rn[j] = a;
+            else if (j == kp + 1)
+                rn[i] = a;
+        }
+        __syncthreads();
+    }
+    for (int q = t; q < npu; q += EX_THREADS)
+        A[q] = -A[q];
+    __syncthreads();
+    return true;
+}
+
+/* LEAN: the form above 32 dates, chosen at compile time so that each
+   kernel holds only the code it runs (the chains here are latency-bound
+   and sensitive to instruction-cache misses). */
+template <bool LEAN>
+__device__ bool ex_sweep(int n, int npu, const ExWs &w, double *A, double floor_)
+{
+    if constexpr (LEAN)
+        return ex_sweep_lean(n, npu, w, A, floor_);
+    else
+        return ex_sweep_rows(n, npu, w, A, floor_);
 }
 
 /* Whether the packed inverse is finite and moderate: n max|inv_ij| < 1e8,
@@ -1605,11 +1671,12 @@ __device__ bool ex_gauss_jordan(int n, const ExWs &w, double *A)
    dates; in the CTA's global scratch W above); else, or when the inverse is
    not moderate, the Jacobi eigen-pseudo-inverse with the absolute floor
    1e-9 (tests/reference.py:151-156) on warp 0. Returns status bits. */
+template <bool LEAN>
 __device__ unsigned ex_inverse(int n, int npu, int ld, const ExWs &w, double *W)
 {
     const int t = threadIdx.x;
 
-    if (ex_sweep(n, npu, w, w.G, 1.0e-5) && ex_moderate(n, npu, w, w.G))
+    if (ex_sweep<LEAN>(n, npu, w, w.G, 1.0e-5) && ex_moderate(n, npu, w, w.G))
         return 0;
     double *A = n <= 32 ? (double *)w.stage : W;
 
@@ -1654,11 +1721,62 @@ __device__ unsigned ex_inverse(int n, int npu, int ld, const ExWs &w, double *W)
     return (unsigned)w.ints[1];
 }
 
+/* Row i = k + 1 + t / R of M22 v (the trailing block at step k, v in w.v),
+   R threads per row, thread h = t % R taking the columns j = h mod R: M_ij
+   = conj(P(j, i)) for j < i, at rb(j) + i - j with rb(j) = j (2n - j + 1) /
+   2, then P(i, j) for j >= i, contiguous. Separate accumulators for the two
+   products of each part keep the FMA chains one deep; the R threads' sums
+   are combined by shuffles (every thread gets its row's). */
+template <int R>
+__device__ __forceinline__ void ex_matvec_rows(int n, int k, const ExWs &w, int t, int &i, int &h,
+                                               double &sx, double &sy)
+{
+    i = k + 1 + t / R;
+    h = t % R;
+    sx = sy = 0.0;
+    if (i < n) {
+        int j = k + 1 + h;
+        int idx = j * (2 * n - j + 1) / 2 + (i - j);
+        double ax = 0.0, bx = 0.0, ay = 0.0, by = 0.0;
+
+        for (; j < i; j += R) {
+            const double2 m = w.T[idx], v = w.v[j];
+
+            ax = fma(m.x, v.x, ax);
+            bx = fma(m.y, v.y, bx);
+            ay = fma(m.x, v.y, ay);
+            by = fma(m.y, v.x, by);
+            idx += R * (n - j) - R * (R + 1) / 2;
+        }
+        sx = ax + bx;
+        sy = ay - by;
+        ax = bx = ay = by = 0.0;
+        for (idx = i * (2 * n - i + 1) / 2 + (j - i); j < n; j += R, idx += R) {
+            const double2 m = w.T[idx], v = w.v[j];
+
+            ax = fma(m.x, v.x, ax);
+            bx = fma(m.y, v.y, bx);
+            ay = fma(m.x, v.y, ay);
+            by = fma(m.y, v.x, by);
+        }
+        sx += ax - bx;
+        sy += ay + by;
+    }
+#pragma unroll
+    for (int o = 1; o < R; o <<= 1) {
+        sx += __shfl_xor_sync(FULL, sx, o);
+        sy += __shfl_xor_sync(FULL, sy, o);
+    }
+}
+
 /* Householder reduction of the packed Hermitian M (w.T) to the real
    tridiagonal (w.d, w.e), zhetd2 form; reflector k's vector is left in
    packed row k (entries k + 2 ..; its entry k + 1 is 1) and its scalar in
-   w.tau[k]. */
-__device__ void ex_householder(int n, int npu, const ExWs &w)
+   w.tau[k]. Two forms: up to 32 dates five CTA barriers a step
+   (ex_householder_cta); above, three (ex_householder_lean: every warp
+   reduces the pivot column itself, and w = p + h v is formed where the
+   rank-2 update reads it), which pays where the steps are many. */
+__device__ void ex_householder_cta(int n, int npu, const ExWs &w)
 {
     const int t = threadIdx.x;
 
@@ -1714,48 +1832,11 @@ __device__ void ex_householder(int n, int npu, const ExWs &w)
         __syncthreads();
         if (!reflect)
             continue;
-        /* p = M22 v over rows k+1 .. n-1, R threads per row (R = 4 up to 32
-           dates, else 2; thread h takes the columns j = h mod R): M_ij =
-           conj(P(j, i)) for j < i, at rb(j) + i - j with rb(j) = j (2n - j
-           + 1) / 2, then P(i, j) for j >= i, contiguous. Separate
-           accumulators for the two products of each part keep the FMA
-           chains one deep. */
-        const int lr = n <= 32 ? 2 : 1, R = 1 << lr;
-        const int i = k + 1 + (t >> lr), h = t & (R - 1);
-        double sx = 0.0, sy = 0.0;
+        /* p = M22 v over rows k+1 .. n-1, four threads per row */
+        double sx, sy;
+        int i, h;
 
-        if (i < n) {
-            int j = k + 1 + h;
-            int idx = j * (2 * n - j + 1) / 2 + (i - j);
-            double ax = 0.0, bx = 0.0, ay = 0.0, by = 0.0;
-
-            for (; j < i; j += R) {
-                const double2 m = w.T[idx], v = w.v[j];
-
-                ax = fma(m.x, v.x, ax);
-                bx = fma(m.y, v.y, bx);
-                ay = fma(m.x, v.y, ay);
-                by = fma(m.y, v.x, by);
-                idx += R * (2 * n - 2 * j - R + 1) / 2 - R;
-            }
-            sx = ax + bx;
-            sy = ay - by;
-            ax = bx = ay = by = 0.0;
-            for (idx = i * (2 * n - i + 1) / 2 + (j - i); j < n; j += R, idx += R) {
-                const double2 m = w.T[idx], v = w.v[j];
-
-                ax = fma(m.x, v.x, ax);
-                bx = fma(m.y, v.y, bx);
-                ay = fma(m.x, v.y, ay);
-                by = fma(m.y, v.x, by);
-            }
-            sx += ax - bx;
-            sy += ay + by;
-        }
-        for (int o = 1; o < R; o <<= 1) {
-            sx += __shfl_xor_sync(FULL, sx, o);
-            sy += __shfl_xor_sync(FULL, sy, o);
-        }
+        ex_matvec_rows<4>(n, k, w, t, i, h, sx, sy);
         const double2 wl = make_double2(tr * sx - ti * sy, tr * sy + ti * sx);
         double pr = 0.0, pi = 0.0;
 
@@ -1789,6 +1870,121 @@ __device__ void ex_householder(int n, int npu, const ExWs &w)
     if (t == 0)
         w.d[n - 1] = w.T[tc_pidx(n, n - 1, n - 1)].x;
     __syncthreads();
+}
+
+__device__ void ex_householder_lean(int n, int npu, const ExWs &w)
+{
+    const int t = threadIdx.x;
+
+    for (int k = 0; k < n - 1; k++) {
+        /* column k below the diagonal: x_r = conj(M_k,r); every warp
+           reduces it itself (no CTA barrier) */
+        const int lane = t & 31;
+        double xn2 = 0.0;
+
+        for (int r = lane; r < n - k - 2; r += 32) {
+            const double2 a = w.T[tc_pidx(n, k, k + 2 + r)];
+
+            xn2 = fma(a.x, a.x, fma(a.y, a.y, xn2));
+        }
+        xn2 = wsum<double>(xn2);
+        const double2 am = w.T[tc_pidx(n, k, k + 1)];
+        const double ax = am.x, ay = -am.y; /* alpha = x_k+1 */
+        double beta, tr = 0.0, ti = 0.0, sr = 0.0, si = 0.0;
+
+        if (xn2 == 0.0 && ay == 0.0)
+            beta = ax;
+        else {
+            beta = -copysign(sqrt(ax * ax + ay * ay + xn2), ax);
+            const double rb = ex_rcp_any(beta);
+
+            tr = (beta - ax) * rb;
+            ti = -ay * rb;
+            const double dr = ax - beta, di = ay, rden = ex_rcp_any(dr * dr + di * di);
+
+            sr = dr * rden;
+            si = -di * rden;
+        }
+        const bool reflect = tr != 0.0 || ti != 0.0;
+        /* v, into w.v now and into column k of T (which keeps the
+           reflectors) after the barrier: other warps may still be reading
+           the column */
+        double2 vk = make_double2(0.0, 0.0);
+
+        if (t < n) {
+            if (t == k + 1)
+                vk = make_double2(1.0, 0.0);
+            else if (t > k + 1 && reflect) {
+                const double2 a = w.T[tc_pidx(n, k, t)];
+                const double xr = a.x, xi = -a.y;
+
+                vk = make_double2(xr * sr - xi * si, xr * si + xi * sr);
+            }
+            w.v[t] = vk;
+        }
+        if (t == 0) {
+            w.d[k] = w.T[tc_pidx(n, k, k)].x;
+            w.e[k] = beta;
+            w.tau[k] = make_double2(tr, ti);
+        }
+        __syncthreads();
+        if (!reflect)
+            continue;
+        if (t > k + 1 && t < n)
+            w.T[tc_pidx(n, k, t)] = vk;
+        /* p = M22 v over rows k+1 .. n-1, two threads per row */
+        double sx, sy;
+        int i, h;
+
+        ex_matvec_rows<2>(n, k, w, t, i, h, sx, sy);
+        const double2 wl = make_double2(tr * sx - ti * sy, tr * sy + ti * sx);
+        double pr = 0.0, pi = 0.0;
+
+        if (i < n && h == 0) {
+            const double2 v = w.v[i];
+
+            pr = wl.x * v.x + wl.y * v.y;
+            pi = wl.x * v.y - wl.y * v.x;
+            /* w = wl + h v, the correction h known after the barrier */
+            w.w[i] = wl;
+        }
+        pr = wsum<double>(pr);
+        pi = wsum<double>(pi);
+        if (lane == 0) {
+            w.red[t >> 5] = pr;
+            w.red[4 + (t >> 5)] = pi;
+        }
+        __syncthreads();
+        const double ppx = w.red[0] + w.red[1] + w.red[2] + w.red[3];
+        const double ppy = w.red[4] + w.red[5] + w.red[6] + w.red[7];
+        const double hr = -0.5 * (tr * ppx - ti * ppy), hi = -0.5 * (tr * ppy + ti * ppx);
+
+        /* M22 -= v w^H + w v^H over the trailing triangle (contiguous) */
+        for (int q = tc_pidx(n, k + 1, k + 1) + t; q < npu; q += EX_THREADS) {
+            const int r = w.tab[q] >> 8, j = w.tab[q] & 255;
+            const double2 vr = w.v[r], vj = w.v[j], lr = w.w[r], lj = w.w[j];
+            const double2 wr = make_double2(lr.x + hr * vr.x - hi * vr.y, lr.y + hr * vr.y + hi * vr.x);
+            const double2 wj = make_double2(lj.x + hr * vj.x - hi * vj.y, lj.y + hr * vj.y + hi * vj.x);
+            double2 a = w.T[q];
+
+            a.x -= vr.x * wj.x + vr.y * wj.y + wr.x * vj.x + wr.y * vj.y;
+            a.y -= vr.y * wj.x - vr.x * wj.y + wr.y * vj.x - wr.x * vj.y;
+            w.T[q] = a;
+        }
+        __syncthreads();
+    }
+    if (t == 0)
+        w.d[n - 1] = w.T[tc_pidx(n, n - 1, n - 1)].x;
+    __syncthreads();
+}
+
+template <bool LEAN>
+__device__ void ex_householder(int n, int npu, const ExWs &w)
+{
+    if constexpr (LEAN)
+        ex_householder_lean(n, npu, w);
+    else
+        ex_householder_cta(n, npu, w);
 }
 
 /* Eigenvalue of rank `index` of (w.d, w.e) (0: the smallest, for EMI;
@@ -2222,7 +2418,7 @@ tc_link_exact_kernel(TcStrip s, TcChunk c, TcLinkConst k, ExLayout L,
         unsigned st = TC_STATUS_FP64;
 
         if (k.emi) {
-            st |= ex_inverse(n, npu, ld, w, W);
+            st |= ex_inverse<(NB > 1)>(n, npu, ld, w, W);
             /* M = |T|^-1 o T in place of T; T in float in place of |T|^-1 */
             for (int q = t; q < npu; q += EX_THREADS) {
                 const double g = w.G[q];
@@ -2240,7 +2436,7 @@ tc_link_exact_kernel(TcStrip s, TcChunk c, TcLinkConst k, ExLayout L,
                 w.Tf[q] = make_float2((float)v.x, (float)v.y);
             }
         __syncthreads();
-        ex_householder(n, npu, w);
+        ex_householder<(NB > 1)>(n, npu, w);
         st |= ex_eigvec(n, k.emi ? 0 : n - 1, w);
         const float gamma = ex_gamma(n, npu, w);
 
