@@ -60,9 +60,9 @@ def metric_name(w):
 # constant, from the ncu capture of profiles/
 # tc_link_half_kernel_emi_bias_n30_256x4096.md (dram__bytes_read.sum +
 # dram__bytes_write.sum of one 65,536-pixel chunk at N=30, AD / EMI / bias
-# correction: 237.7 MB read, the packed Gram, 465 x 8 B per pixel, read at
-# most once, + 9.6 MB written), not a measurement of the run that reports it.
-LINK_DRAM_BYTES_PER_PIXEL = 247.3e6 / 65536
+# correction: 245.2 MB read, the packed Gram, 465 x 8 B per pixel, read at
+# most once, + 7.3 MB written), not a measurement of the run that reports it.
+LINK_DRAM_BYTES_PER_PIXEL = 252.5e6 / 65536
 
 
 def parse():
