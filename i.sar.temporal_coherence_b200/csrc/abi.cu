@@ -673,7 +673,7 @@ static int run_device(struct ocl *o, const float *slc, const float *amp,
         q.buf = (int *)o->exact_list.p;
         q.stride = 1 + s.mask_words;
         q.capacity = cap;
-        CK(cudaMemsetAsync(q.buf, 0, sizeof(int), st));
+        CK(cudaMemsetAsync(q.buf, 0, sizeof(int) * TC_QUEUE_HEAD, st));
     }
     if (o->opt.gram == TC_GRAM_FP32)
         CK(ensure(o->soa, sizeof(float2) * s.planes * s.npad));

@@ -1112,7 +1112,7 @@ struct ExWs {
     double2 *v, *w, *tau, *z;
     float2 *zs;
     unsigned long long *adj;
-    int *ints;        /* [0] candidates, [1] flags */
+    int *ints;        /* [0] candidates, [1] flags, [2..5] per warp, [6] next queue entry */
 };
 
 __host__ __device__ inline ExLayout ex_layout(int n, int area)
@@ -2340,7 +2340,7 @@ template <int NB, int BC>
 __global__ void __launch_bounds__(EX_THREADS, ex_ctas(NB))
 tc_link_exact_kernel(TcStrip s, TcChunk c, TcLinkConst k, ExLayout L,
                      const float2 *__restrict__ slc, const uint32_t *__restrict__ mask,
-                     const int *__restrict__ count, const int *__restrict__ queue, int qstride,
+                     const int *__restrict__ count, int *queue, int qstride,
                      const unsigned short *__restrict__ upper_tab,
                      const unsigned short *__restrict__ pair_tab, double *__restrict__ scratch,
                      float *__restrict__ coh, float *__restrict__ pairs,
@@ -2364,9 +2364,24 @@ tc_link_exact_kernel(TcStrip s, TcChunk c, TcLinkConst k, ExLayout L,
     }
     __syncthreads();
     const int total = queue ? queue[0] : c.npix;
+    /* A chunk's pixels go to the CTAs in turn. Queued pixels vary more in
+       cost (pivoted inverses, unlinked dates, several chunks' worth of
+       flagged pixels of every kind): after its first, each CTA takes the
+       next untaken entry from the queue's counter buf[1]. The barriers
+       order thread 0's write of the index after every thread's read of the
+       previous one. */
+    auto next_item = [&](int it) -> int {
+        if (!queue)
+            return it + gridDim.x;
+        __syncthreads();
+        if (t == 0)
+            w.ints[6] = gridDim.x + atomicAdd(queue + 1, 1);
+        __syncthreads();
+        return w.ints[6];
+    };
 
-    for (int it = blockIdx.x; it < total; it += gridDim.x) {
-        const int *entry = queue ? queue + 1 + (long long)it * qstride : nullptr;
+    for (int it = blockIdx.x; it < total; it = next_item(it)) {
+        const int *entry = queue ? queue + TC_QUEUE_HEAD + (long long)it * qstride : nullptr;
         int y, x;
 
         if (entry) {
@@ -2539,7 +2554,7 @@ bool tc_link_queues(int n, const TcLinkConst &k)
 
 size_t tc_exact_queue_bytes(int mask_words, long long capacity)
 {
-    return sizeof(int) * (1 + (size_t)capacity * (1 + mask_words));
+    return sizeof(int) * (TC_QUEUE_HEAD + (size_t)capacity * (1 + mask_words));
 }
 
 cudaError_t tc_flush_exact(const TcStrip &s, const TcLinkConst &k, TcExactQueue *q,
@@ -2555,7 +2570,7 @@ cudaError_t tc_flush_exact(const TcStrip &s, const TcLinkConst &k, TcExactQueue 
 
         if ((e = launch_exact(s, none, k, slc, nullptr, count, q, upper_tab, pair_tab, scratch,
                               coh, pairs, phases, status, sms, st)) == cudaSuccess)
-            e = cudaMemsetAsync(q->buf, 0, sizeof(int), st);
+            e = cudaMemsetAsync(q->buf, 0, sizeof(int) * TC_QUEUE_HEAD, st);
     }
     q->pending = 0;
     return e;

@@ -224,7 +224,7 @@ TC_API int tc_run_device_static(const struct settings *s, int padded_cols, const
             eq.buf = (int *)q;
             eq.stride = 1 + ss.mask_words;
             eq.capacity = c.npix;
-            if ((e = cudaMemsetAsync(eq.buf, 0, sizeof(int), st)) != cudaSuccess)
+            if ((e = cudaMemsetAsync(eq.buf, 0, sizeof(int) * TC_QUEUE_HEAD, st)) != cudaSuccess)
                 return tc_error(TC_ERR_CUDA, "exact-tier queue: %s", cudaGetErrorString(e));
         }
 

@@ -83,12 +83,16 @@ __host__ __device__ inline void tc_pixel_yx(const TcChunk &c, int p, int &y, int
 
 /* The pixels handed to the exact tier, queued across the chunks of a strip
    so that one launch of the exact kernel takes many chunks' pixels: buf[0]
-   counts the entries; entry e (buf + 1 + e * stride, stride = 1 +
-   mask_words) holds the pixel's output index y * cols + x and its SHP-mask
+   counts the entries, buf[1] the entries that the exact kernel's CTAs have
+   taken beyond their first (each CTA takes its next pixel from it, so that
+   pixels of unequal cost spread evenly); entry e (buf + TC_QUEUE_HEAD + e *
+   stride, stride = 1 + mask_words) holds the pixel's output index y * cols + x and its SHP-mask
    words, copied from the chunk's mask (which the next chunk overwrites).
    The float link kernels append to it; the host flushes it
    (tc_flush_exact) before a chunk could overflow it and at the end of the
    strip, and counts in `pending` an upper bound on the entries queued. */
+constexpr int TC_QUEUE_HEAD = 2; /* ints before the first entry, zeroed per flush */
+
 struct TcExactQueue {
     int *buf;
     int stride;
@@ -101,7 +105,7 @@ struct TcExactQueue {
 __device__ __forceinline__ void tc_exact_push(int *q, int stride, long long out,
                                               const uint32_t *mask, long long npix, int p)
 {
-    int *e = q + 1 + (long long)atomicAdd(q, 1) * stride;
+    int *e = q + TC_QUEUE_HEAD + (long long)atomicAdd(q, 1) * stride;
 
     e[0] = (int)out;
     for (int w = 1; w < stride; w++)
