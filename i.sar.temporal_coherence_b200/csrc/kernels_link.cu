@@ -1452,47 +1452,12 @@ __device__ bool ex_linked(int n, const ExWs &w)
    a_ik, a_kj -> a_ik / a_kk, a_kk -> -1 / a_kk, and all pivots leave
    -A^-1, negated back at the end. It takes indefinite matrices. False when
    a pivot's magnitude is not above floor_ (A is then undefined).
-   Two forms: up to 32 dates the scaled pivot row goes to w.rrow behind its
-   own barrier (ex_sweep_rows); above, each step copies the next pivot row
-   as it updates it, one barrier a pivot (ex_sweep_lean), which pays where
-   the pivots are many. */
-__device__ bool ex_sweep_rows(int n, int npu, const ExWs &w, double *A, double floor_)
-{
-    const int t = threadIdx.x;
-
-    for (int kp = 0; kp < n; kp++) {
-        const double d = A[tc_pidx(n, kp, kp)];
-
-        if (!(fabs(d) > floor_)) {
-            __syncthreads();
-            return false;
-        }
-        const double id = ex_rcp_any(d);
-
-        for (int j = t; j < n; j += EX_THREADS)
-            w.rrow[j] = A[ex_sym(n, kp, j)] * id;
-        __syncthreads();
-        for (int q = t; q < npu; q += EX_THREADS) {
-            const int i = w.tab[q] >> 8, j = w.tab[q] & 255;
-
-            if (i == kp && j == kp)
-                A[q] = -id;
-            else if (i == kp)
-                A[q] = w.rrow[j];
-            else if (j == kp)
-                A[q] = w.rrow[i];
-            else
-                A[q] = fma(-w.rrow[i] * d, w.rrow[j], A[q]);
-        }
-        __syncthreads();
-    }
-    for (int q = t; q < npu; q += EX_THREADS)
-        A[q] = -A[q];
-    __syncthreads();
-    return true;
-}
-
-__device__ bool ex_sweep_lean(int n, int npu, const ExWs &w, double *A, double floor_)
+   Each step copies the next pivot row as it updates it (into one of two
+   buffers), so that one barrier a pivot suffices; against a form that
+   scaled the pivot row into its own buffer behind a second barrier, this
+   one is the faster at every size (30-date AD/EMI/-b exact tier 83.7 ->
+   82.0 ms per 4096 x 4096 step). */
+__device__ bool ex_sweep(int n, int npu, const ExWs &w, double *A, double floor_)
 {
     const int t = threadIdx.x;
     /* the pivot row as it stands before its step, in one of two buffers
@@ -1540,18 +1505,6 @@ __device__ bool ex_sweep_lean(int n, int npu, const ExWs &w, double *A, double f
         A[q] = -A[q];
     __syncthreads();
     return true;
-}
-
-/* LEAN: the form above 32 dates, chosen at compile time so that each
-   kernel holds only the code it runs (the chains here are latency-bound
-   and sensitive to instruction-cache misses). */
-template <bool LEAN>
-__device__ bool ex_sweep(int n, int npu, const ExWs &w, double *A, double floor_)
-{
-    if constexpr (LEAN)
-        return ex_sweep_lean(n, npu, w, A, floor_);
-    else
-        return ex_sweep_rows(n, npu, w, A, floor_);
 }
 
 /* Whether the packed inverse is finite and moderate: n max|inv_ij| < 1e8,
@@ -1671,12 +1624,11 @@ __device__ bool ex_gauss_jordan(int n, const ExWs &w, double *A)
    dates; in the CTA's global scratch W above); else, or when the inverse is
    not moderate, the Jacobi eigen-pseudo-inverse with the absolute floor
    1e-9 (tests/reference.py:151-156) on warp 0. Returns status bits. */
-template <bool LEAN>
 __device__ unsigned ex_inverse(int n, int npu, int ld, const ExWs &w, double *W)
 {
     const int t = threadIdx.x;
 
-    if (ex_sweep<LEAN>(n, npu, w, w.G, 1.0e-5) && ex_moderate(n, npu, w, w.G))
+    if (ex_sweep(n, npu, w, w.G, 1.0e-5) && ex_moderate(n, npu, w, w.G))
         return 0;
     double *A = n <= 32 ? (double *)w.stage : W;
 
@@ -1978,6 +1930,9 @@ __device__ void ex_householder_lean(int n, int npu, const ExWs &w)
     __syncthreads();
 }
 
+/* LEAN (above 32 dates) or not, chosen at compile time so that each kernel
+   holds only the code it runs: the chains here are latency-bound and
+   sensitive to instruction-cache misses. */
 template <bool LEAN>
 __device__ void ex_householder(int n, int npu, const ExWs &w)
 {
@@ -2433,7 +2388,7 @@ tc_link_exact_kernel(TcStrip s, TcChunk c, TcLinkConst k, ExLayout L,
         unsigned st = TC_STATUS_FP64;
 
         if (k.emi) {
-            st |= ex_inverse<(NB > 1)>(n, npu, ld, w, W);
+            st |= ex_inverse(n, npu, ld, w, W);
             /* M = |T|^-1 o T in place of T; T in float in place of |T|^-1 */
             for (int q = t; q < npu; q += EX_THREADS) {
                 const double g = w.G[q];
